@@ -1,0 +1,216 @@
+/* ve.h — C ABI of the B200-native voxel ray pipeline (drop-in for the
+ * RayPass / bounce-shade / AccumPass / AvgPass passes of
+ * AnghelusAndrei/VoxelEngine3.0).
+ *
+ * Plain pointers and sizes only.  Every function returns an int status
+ * (VE_OK = 0, negative = error); ve_last_error() gives the message of the
+ * calling thread's last failure.  The caller owns every host array; the
+ * library owns all device memory.  A context serialises its work on one CUDA
+ * stream and is used from one host thread at a time.
+ *
+ * Each declaration names the reference interface it replaces
+ * (paths relative to the reference repository).
+ */
+#ifndef VE_H
+#define VE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define VE_OK 0
+#define VE_ERR_INVALID (-1)  /* bad argument */
+#define VE_ERR_CUDA (-2)     /* CUDA runtime error (message in ve_last_error) */
+#define VE_ERR_NOMEM (-3)    /* allocation failed */
+#define VE_ERR_CAPACITY (-4) /* a fixed capacity would be exceeded */
+#define VE_ERR_NOT_FOUND (-5)
+#define VE_ERR_TIMEOUT (-6) /* a bounded device wait gave up */
+#define VE_ERR_STATE (-7)   /* call not valid in the current state */
+
+/* ---- render types (src/renderer/core.hpp:71-78) ----------------------- */
+#define VE_RENDER_DEFAULT 0
+#define VE_RENDER_STRUCTURE 1
+#define VE_RENDER_ALBEDO 2
+#define VE_RENDER_NORMAL 3
+#define VE_RENDER_VOXELID 4
+#define VE_RENDER_VARIANCE 5
+
+/* ---- flags ------------------------------------------------------------ */
+#define VE_SCENE_KEEP_NORMALS 1u  /* upload words as given (no device normal pass) */
+#define VE_FRAME_TIMING 1u        /* per-pass CUDA-event times into ve_frame_stats */
+#define VE_FRAME_COUNT_FETCH 2u   /* count node-word fetches on the device */
+#define VE_FRAME_PATH_RGB 4u      /* keep every path's deposit value (debug) */
+
+/* RendererConfig (src/renderer/core.hpp:30-42) plus device sizing.  The
+ * radiance cache replaces the lBuffer hash image (renderer.cpp:27-40):
+ * 2^hash_log2 entries per scene, linear probing up to hash_probes. */
+typedef struct ve_renderer_config {
+    int32_t device;
+    uint32_t hash_log2;   /* 22 -> 4,194,304 entries (32 B each) */
+    uint32_t hash_probes; /* 64 */
+    uint32_t flags;
+} ve_renderer_config;
+
+/* FrameConfig (src/renderer/core.hpp:83-158): the knobs the plain method
+ * reads, plus the benchmark lighting (directional sun + constant sky). */
+typedef struct ve_frame_config {
+    uint32_t width, height;
+    uint32_t spp;                   /* paths per hit pixel */
+    uint32_t bounces;               /* secondary bounces; MAX_BOUNCES = bounces + 1 */
+    uint32_t primary_controlchecks; /* core.hpp:85 */
+    uint32_t bounce_controlchecks;  /* core.hpp:86 */
+    uint32_t reconstruction_radius; /* core.hpp:87 */
+    uint32_t render_type;           /* VE_RENDER_* */
+    uint32_t frame_index;           /* emit.comp frameIdx */
+    float sun_dir[3];               /* unit vector toward the sun */
+    float sun_intensity;
+    float sky[3];                   /* constant sky radiance */
+    float decay;                    /* temporal decay of the cache per frame */
+    float variance_norm;            /* core.hpp:109 (VARIANCE view scale) */
+    uint32_t flags;                 /* VE_FRAME_* */
+} ve_frame_config;
+
+/* One render request: scene, Camera::UBO (camera.hpp:24-29: position,
+ * cameraPlane, cameraPlaneRight, cameraPlaneUp as 4 x vec4) and frame knobs. */
+typedef struct ve_view {
+    int32_t scene_id;
+    float camera[16];
+    ve_frame_config frame;
+} ve_view;
+
+/* Outputs of one view (host pointers; NULL = not requested).  gbuffer is the
+ * GBuffer image (generate_primary.comp:68-82) with the hit-node index in the
+ * reserved .z lane; rgb is the AvgPass output (avgPass.texture); mapped is
+ * the RenderPass ACES output (final.frag:11-18). */
+typedef struct ve_frame_outputs {
+    uint32_t* gbuffer;  /* 4 x u32 per pixel {checks, material, hit node, vid} */
+    uint32_t* voxel_id; /* 1 x u32 per pixel: voxelKey + 1, 0 on miss */
+    uint32_t* hit_node; /* 1 x u32 per pixel: node slot of the hit leaf, 0 on miss */
+    float* rgb;         /* 3 x f32 per pixel */
+    float* mapped;      /* 3 x f32 per pixel */
+    float* path_rgb;    /* 3 x f32 per path (pixel * spp + sample); VE_FRAME_PATH_RGB */
+} ve_frame_outputs;
+
+/* FrameStats (src/renderer/core.hpp:164-185) and the profiler's stage
+ * timings (src/renderer/profiler.hpp:43-70), from device counters and CUDA
+ * events of the last ve_render / ve_render_batch call. */
+typedef struct ve_frame_stats {
+    uint64_t rays_primary, rays_bounce, rays_shadow;
+    uint64_t fetch_nodes; /* node words read (VE_FRAME_COUNT_FETCH) */
+    uint64_t paths, deposits, deposits_dropped;
+    uint64_t dda_steps;   /* DDA outer iterations (VE_FRAME_COUNT_FETCH) */
+    float ms_total, ms_primary, ms_trace, ms_shade, ms_resolve, ms_decay;
+    uint32_t trace_launches, kernel_launches;
+    uint64_t cache_capacity;
+} ve_frame_stats;
+
+typedef struct ve_ctx ve_ctx;
+typedef struct ve_octree_cpu ve_octree_cpu;
+typedef struct ve_octree ve_octree;
+typedef struct ve_words ve_words;
+
+const char* ve_version(void);
+const char* ve_last_error(void);
+
+/* ======================================================================
+ * Host scene layer
+ * ==================================================================== */
+
+/* OctreeCPU (src/octree_cpu.hpp:27-37): ctor, insert, remove, lookup,
+ * insertBox, insertSphere, raycast. */
+int ve_octree_cpu_create(uint32_t depth, ve_octree_cpu** out);
+int ve_octree_cpu_destroy(ve_octree_cpu* t);
+int ve_octree_cpu_insert(ve_octree_cpu* t, uint32_t x, uint32_t y, uint32_t z, uint32_t material);
+int ve_octree_cpu_insert_many(ve_octree_cpu* t, const uint32_t* xyzm, uint64_t n);
+int ve_octree_cpu_remove(ve_octree_cpu* t, uint32_t x, uint32_t y, uint32_t z);
+/* material of the leaf at (x,y,z), or -1 when absent (OctreeCPU::lookup) */
+int ve_octree_cpu_lookup(const ve_octree_cpu* t, uint32_t x, uint32_t y, uint32_t z, int64_t* material);
+int ve_octree_cpu_insert_box(ve_octree_cpu* t, const uint32_t mn[3], const uint32_t mx[3], uint32_t material);
+int ve_octree_cpu_insert_sphere(ve_octree_cpu* t, const float centre[3], float radius, uint32_t material);
+int ve_octree_cpu_raycast(const ve_octree_cpu* t, const float origin[3], const float dir[3], uint32_t max_steps,
+                          int* hit, uint32_t pos[3]);
+
+/* Octree (src/renderer/octree.hpp:45-59): the node array in the reference
+ * layout.  ve_octree_words returns `capacity` words (valid until the next
+ * set / apply_edits). */
+int ve_octree_create(uint32_t depth, ve_octree** out);
+int ve_octree_destroy(ve_octree* o);
+int ve_octree_set(ve_octree* o, ve_octree_cpu* cpu);                     /* Octree::set */
+int ve_octree_apply_edits(ve_octree* o, ve_octree_cpu* cpu, uint32_t* changed_slots, uint64_t cap,
+                          uint64_t* n_changed);                           /* Octree::applyEdits */
+/* the changed slots of the last ve_octree_apply_edits (valid until the next call) */
+int ve_octree_last_changed(const ve_octree* o, const uint32_t** slots, uint64_t* n);
+int ve_octree_find_gpu_slot(const ve_octree* o, ve_octree_cpu* cpu, uint32_t x, uint32_t y, uint32_t z,
+                            uint32_t* slot);                              /* Octree::findGpuSlot */
+int ve_octree_info(const ve_octree* o, uint32_t* size, uint32_t* capacity, uint32_t* num_voxels);
+int ve_octree_words(const ve_octree* o, const uint32_t** words, uint64_t* n);
+
+/* Seeded value-noise terrain scenes (benchmark inputs; no reference
+ * counterpart: the reference's demo scene is built in voxelengine.cpp:129-144).
+ * ve_terrain_build emits the words of OctreeCPU::insert + Octree::set in
+ * parallel without pointer nodes. */
+int ve_terrain_build(uint32_t depth, uint32_t variant, uint64_t seed, uint32_t threads, ve_words** out,
+                     uint64_t* n_voxels);
+int ve_words_data(const ve_words* w, const uint32_t** data, uint64_t* n);
+int ve_words_free(ve_words* w);
+int ve_terrain_voxels(uint32_t depth, uint32_t variant, uint64_t seed, uint32_t* xyzm, uint64_t cap, uint64_t* n);
+int ve_terrain_materials(uint64_t seed, void* out_128_std140_entries);
+
+/* Camera::UpdateUBO (src/renderer/camera.cpp:39-50) */
+int ve_camera_ubo(const float pos[3], const float dir[3], float fov_deg, float aspect, float ubo[16]);
+
+/* ======================================================================
+ * Device renderer
+ * ==================================================================== */
+
+/* Renderer::Renderer (src/renderer/renderer.hpp:11-12) / ~Renderer */
+int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out);
+int ve_ctx_destroy(ve_ctx* ctx);
+/* the context's cudaStream_t, for callers that time or order work on it */
+int ve_ctx_stream(ve_ctx* ctx, void** stream);
+int ve_ctx_synchronize(ve_ctx* ctx);
+
+/* Octree::set upload (octree.cpp:157-159 glBufferData of Octree::data):
+ * `words` verbatim in the reference layout.  Unless VE_SCENE_KEEP_NORMALS,
+ * a device pass fills every leaf's normal field (3x3x3 occupancy gradient). */
+int ve_scene_upload(ve_ctx* ctx, const uint32_t* words, uint64_t n_words, uint32_t depth, uint32_t flags,
+                    int32_t* scene_id);
+int ve_scene_release(ve_ctx* ctx, int32_t scene_id);
+/* Octree::applyEdits upload (octree.cpp:228-314 UpdateNode): scatter
+ * words[i] to slots[i]; normals of affected leaves are recomputed unless
+ * VE_SCENE_KEEP_NORMALS.  The scene's radiance cache is kept. */
+int ve_scene_apply_edits(ve_ctx* ctx, int32_t scene_id, const uint32_t* slots, const uint32_t* words, uint64_t n,
+                         uint32_t flags);
+int ve_scene_download(ve_ctx* ctx, int32_t scene_id, uint32_t* out, uint64_t cap, uint64_t* n_words);
+/* device bytes held by a scene (node array + radiance cache) */
+int ve_scene_footprint(ve_ctx* ctx, int32_t scene_id, uint64_t* bytes);
+
+/* MaterialPool UBO (src/renderer/material.cpp:17-49): n entries of 64 B
+ * (std140 Material), index 0 reserved. */
+int ve_set_materials(ve_ctx* ctx, const void* entries, uint32_t n);
+
+/* Radiance cache of a scene (the lBuffer replacement): clear, and dump of
+ * occupied entries: vids, exact deposit counts, and 5 floats per entry
+ * {decayed weight, r, g, b, luma^2} sums. */
+int ve_cache_reset(ve_ctx* ctx, int32_t scene_id);
+int ve_cache_dump(ve_ctx* ctx, int32_t scene_id, uint32_t* vids, uint32_t* counts, float* values, uint64_t cap,
+                  uint64_t* n);
+
+/* Renderer::run (src/renderer/renderer.hpp:13, renderer.cpp:282-712): one
+ * frame of one view.  Returns after the host outputs are written; with all
+ * output pointers NULL it only enqueues the work on the context stream. */
+int ve_render(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
+/* Several views (any scenes, resolutions, spp, bounces) as one wavefront
+ * batch: one primary pass over all views, one trace and one shade pass per
+ * bounce depth for all their paths, one resolve pass. `outs` may be NULL. */
+int ve_render_batch(ve_ctx* ctx, const ve_view* views, uint32_t n_views, ve_frame_outputs* outs);
+/* stats of the last render call (synchronises the context stream) */
+int ve_get_stats(ve_ctx* ctx, ve_frame_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VE_H */

@@ -1,0 +1,996 @@
+// ve_oracle.cpp — TEST INFRASTRUCTURE ONLY: the CPU oracle for the ray
+// pipeline of AnghelusAndrei/VoxelEngine3.0.  It is the checker for the
+// product's CUDA kernels and the timed CPU baseline; nothing in the product
+// links or calls it.
+//
+// Every function cites the reference file:line it restates.  The GLSL passes
+// cannot execute here (no graphics stack), so this file restates them in
+// scalar C++ with a pinned floating-point policy:
+//   * compiled with -O2 -ffp-contract=off (no fused multiply-add unless an
+//     explicit fmaf is written), IEEE division and sqrt;
+//   * GLSL min/max are pinned to glm's expressions: min(a,b) = (b<a)?b:a,
+//     max(a,b) = (a<b)?b:a (NaN-propagation is therefore defined);
+//   * the Box-Muller RandomDirection (internal.glsl:101-112) uses log/cos,
+//     whose last bits differ between libm and CUDA; it is replaced here AND
+//     in the kernels by an exact-operation uniform-sphere map whose sin/cos
+//     are a project-written Taylor polynomial (Horner form, explicit fmaf)
+//     after quadrant reduction.  Deliberate, named deviation.
+// Parity pins: the tree build/linearisation and OctreeCPU::raycast are checked
+// against the reference's own compiled code (oracle/_ref, see build_ref.sh);
+// the GLSL restatements have no reference-side golden vectors.
+#include "ve_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stack>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// small float helpers (GLSL semantics pinned as documented above)
+// ---------------------------------------------------------------------------
+struct f3 {
+    float x, y, z;
+};
+inline f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+inline f3 add(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline f3 sub(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline f3 mul(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline f3 muls(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+inline f3 divs(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+inline float gmin(float a, float b) { return (b < a) ? b : a; }
+inline float gmax(float a, float b) { return (a < b) ? b : a; }
+inline float gclamp(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
+inline float dot(f3 a, f3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline f3 normalize(f3 v) { return divs(v, std::sqrt(dot(v, v))); }
+inline f3 cross(f3 a, f3 b) {
+    return mk(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+
+// ---------------------------------------------------------------------------
+// Node words (src/renderer/octree.hpp:16-37, internal.glsl:1, 18)
+// ---------------------------------------------------------------------------
+inline bool node_is_node(uint32_t raw) { return raw & 1u; }
+inline uint32_t node_next(uint32_t raw) { return (raw & 0xFFFFFFF0u) >> 4; }
+inline uint32_t node_material(uint32_t raw) { return (raw & 254u) >> 1; }
+
+struct Scene {
+    const uint32_t* words;
+    uint64_t n;
+    uint32_t depth;
+    // texelFetch on a buffer texture: out-of-range reads return 0.
+    uint32_t fetch(uint64_t off) const { return off < n ? words[off] : 0u; }
+};
+
+// locate (internal.glsl:30)
+inline uint32_t locate(uint32_t x, uint32_t y, uint32_t z, uint32_t p2) {
+    return (uint32_t(bool(x & p2)) << 2) | (uint32_t(bool(y & p2)) << 1) | uint32_t(bool(z & p2));
+}
+
+// inBounds (internal.glsl:29)
+inline bool in_bounds(f3 v, float n) {
+    return 0.0f <= v.x && v.x <= n && 0.0f <= v.y && v.y <= n && 0.0f <= v.z && v.z <= n;
+}
+
+enum { ST_HIT = 0, ST_ESCAPED = 1, ST_TIMEOUT = 2 };
+
+struct Hit {
+    int status;
+    uint32_t id, material;
+    uint32_t pos[3];
+    uint32_t size;
+    uint32_t checks;
+};
+
+struct RayCounters {
+    uint64_t fetch_restart = 0, fetch_min = 0, steps = 0;
+};
+
+// Raycast / RaycastCounted (internal.glsl:297-400) with intersect
+// (:245-253) and intersect_inside (:255-261).  Returns the termination status
+// as well (hit / left the volume / ran out of controlchecks); the reference
+// reports only hit-or-not.  `fetch_min` counts a node word only when it
+// differs from the word last read at the same descent level (the distinct
+// nodes along the ray's monotone DDA walk).
+Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc) {
+    const uint32_t D = s.depth;
+    const uint32_t L = 1u << D;
+    const float Lf = float(L);
+    uint32_t p2c[17];
+    for (uint32_t i = 0; i <= D; i++) p2c[i] = L >> i;
+    uint32_t last_off[17];
+    for (uint32_t i = 0; i <= D; i++) last_off[i] = 0xFFFFFFFFu;
+
+    Hit h{};
+    h.status = ST_ESCAPED;
+    const f3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    o = add(o, muls(d, 4.0f));  // ray.origin += ray.direction * 4  (:361)
+    uint32_t q = 0;
+    f3 r;
+    if (in_bounds(o, Lf)) {
+        r = o;
+    } else {
+        // intersect(ray, vec3(0), vec3(L))  (:245-253)
+        f3 t1 = mul(mk((0.0f - o.x) + 0.001f, (0.0f - o.y) + 0.001f, (0.0f - o.z) + 0.001f), inv);
+        f3 t2 = mul(mk((Lf - o.x) - 0.001f, (Lf - o.y) - 0.001f, (Lf - o.z) - 0.001f), inv);
+        f3 tmn = mk(gmin(t1.x, t2.x), gmin(t1.y, t2.y), gmin(t1.z, t2.z));
+        f3 tmx = mk(gmax(t1.x, t2.x), gmax(t1.y, t2.y), gmax(t1.z, t2.z));
+        float t_enter = gmax(gmax(tmn.x, tmn.y), tmn.z);
+        float t_exit = gmin(gmin(tmx.x, tmx.y), tmx.z);
+        q++;
+        if (t_exit < t_enter || t_exit < 0.0f) {
+            h.checks = q;
+            return h;
+        }
+        r = add(muls(d, t_enter), o);
+    }
+    while (in_bounds(r, Lf) && q++ <= controlchecks) {
+        if (rc) rc->steps++;
+        const uint32_t ux = uint32_t(r.x), uy = uint32_t(r.y), uz = uint32_t(r.z);
+        uint32_t off = 0, depth = 0, size = 0;
+        bool found = false;
+        for (; depth < D; depth++) {
+            off += locate(ux, uy, uz, p2c[depth]);
+            const uint32_t raw = s.fetch(off);
+            if (rc) {
+                rc->fetch_restart++;
+                if (last_off[depth] != off) { rc->fetch_min++; last_off[depth] = off; }
+            }
+            if (!node_is_node(raw)) {
+                size = p2c[depth];
+                found = true;
+                break;
+            }
+            off = node_next(raw);
+        }
+        uint32_t px, py, pz;
+        if (!found) {
+            off += locate(ux, uy, uz, p2c[depth]);
+            const uint32_t raw = s.fetch(off);
+            if (rc) {
+                rc->fetch_restart++;
+                if (last_off[depth] != off) { rc->fetch_min++; last_off[depth] = off; }
+            }
+            size = p2c[depth];
+            px = ux & ~(size - 1u); py = uy & ~(size - 1u); pz = uz & ~(size - 1u);
+            if (node_material(raw) != 0u) {
+                h.status = ST_HIT;
+                h.id = off;
+                h.material = node_material(raw);
+                h.pos[0] = px; h.pos[1] = py; h.pos[2] = pz;
+                h.size = size;
+                h.checks = q;
+                return h;
+            }
+        } else {
+            px = ux & ~(size - 1u); py = uy & ~(size - 1u); pz = uz & ~(size - 1u);
+        }
+        // intersect_inside(ray, pos, pos + size)  (:255-261)
+        const f3 bmin = mk(float(px), float(py), float(pz));
+        const float fs = float(size);
+        const f3 bmax = mk(bmin.x + fs, bmin.y + fs, bmin.z + fs);
+        f3 t1 = mul(mk((bmin.x - o.x) - 0.001f, (bmin.y - o.y) - 0.001f, (bmin.z - o.z) - 0.001f), inv);
+        f3 t2 = mul(mk((bmax.x - o.x) + 0.001f, (bmax.y - o.y) + 0.001f, (bmax.z - o.z) + 0.001f), inv);
+        f3 tmx = mk(gmax(t1.x, t2.x), gmax(t1.y, t2.y), gmax(t1.z, t2.z));
+        float t_exit = gmin(gmin(tmx.x, tmx.y), tmx.z);
+        r = add(muls(d, t_exit), o);
+    }
+    h.status = in_bounds(r, Lf) ? ST_TIMEOUT : ST_ESCAPED;
+    h.checks = q;
+    return h;
+}
+
+// hash + voxelKey (internal.glsl:263-291)
+inline uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+inline uint32_t voxel_key(const uint32_t pos[3]) {
+    uint32_t p = pos[0] | (pos[1] << 10) | (pos[2] << 20);
+    return hash32(p) & 0x7FFFFFFFu;
+}
+
+// halton + rand (internal.glsl:57-89)
+const uint32_t kHaltonBases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+inline float halton(uint32_t i, uint32_t b) {
+    float f = 1.0f, r = 0.0f;
+    for (int k = 0; k < 24 && i > 0u; k++) {
+        f /= float(b);
+        uint32_t q = i / b;
+        r += f * float(i - q * b);
+        i = q;
+    }
+    return r;
+}
+inline float rand01(uint32_t& state) {
+    uint32_t dim = state & 0xFFu;
+    uint32_t sample_idx = state >> 8;
+    state = (sample_idx << 8) | ((dim + 1u) & 0xFFu);
+    uint32_t base = kHaltonBases[dim & 15u];
+    uint32_t effective = sample_idx ^ ((dim >> 4) * 0x9E3779B9u);
+    return halton(effective, base);
+}
+
+// Project-written sin/cos of 2*pi*u for u in [0,1]: quadrant reduction
+// (exact: x = 4u, q = floor(x), f = x - q) then Taylor polynomials of
+// sin/cos on [0, pi/2) in Horner form with explicit fmaf (degree 11 / 12;
+// truncation error < 6e-8).  Replaces the reference's cos/log sampling.
+inline void sincos_turn(float u, float* s_out, float* c_out) {
+    const float x = u * 4.0f;
+    const float qf = std::floor(x);
+    const int q = int(qf) & 3;
+    const float t = (x - qf) * 0x1.921fb6p+0f;
+    const float t2 = t * t;
+    float ps = std::fmaf(t2, -0x1.ae6456p-26f, 0x1.71de3ap-19f);
+    ps = std::fmaf(t2, ps, -0x1.a01a02p-13f);
+    ps = std::fmaf(t2, ps, 0x1.111112p-7f);
+    ps = std::fmaf(t2, ps, -0x1.555556p-3f);
+    const float s = std::fmaf(t * t2, ps, t);
+    float pc = std::fmaf(t2, 0x1.1eed8ep-29f, -0x1.27e4fcp-22f);
+    pc = std::fmaf(t2, pc, 0x1.a01a02p-16f);
+    pc = std::fmaf(t2, pc, -0x1.6c16c2p-10f);
+    pc = std::fmaf(t2, pc, 0x1.555556p-5f);
+    pc = std::fmaf(t2, pc, -0x1p-1f);
+    const float c = std::fmaf(t2, pc, 1.0f);
+    switch (q) {
+        case 0: *s_out = s; *c_out = c; break;
+        case 1: *s_out = c; *c_out = -s; break;
+        case 2: *s_out = -s; *c_out = -c; break;
+        default: *s_out = -c; *c_out = s; break;
+    }
+}
+
+// Uniform direction on the unit sphere from two rand() draws; stands in for
+// RandomDirection (internal.glsl:107-112).
+inline f3 uniform_sphere(uint32_t& rng) {
+    const float u1 = rand01(rng);
+    const float u2 = rand01(rng);
+    const float z = 1.0f - 2.0f * u1;
+    const float rr = std::sqrt(gmax(1.0f - z * z, 0.0f));
+    float sn, cs;
+    sincos_turn(u2, &sn, &cs);
+    return mk(rr * cs, rr * sn, z);
+}
+
+// normalize(N + RandomDirection) (shade.comp:869) with a zero-length guard.
+inline f3 cosine_direction(f3 n, uint32_t& rng) {
+    const f3 v = add(n, uniform_sphere(rng));
+    const float d2 = dot(v, v);
+    if (!(d2 > 1e-12f)) return n;
+    return divs(v, std::sqrt(d2));
+}
+
+// Material (src/renderer/material.hpp:17-25; std140 64-B stride)
+struct Material {
+    float color[4];
+    float specular_color[4];
+    float roughness, specular, metallic;
+    int32_t emissive;
+    float emissive_intensity;
+    float pad[3];
+};
+static_assert(sizeof(Material) == 64, "material stride");
+
+// EvaluateBRDF (internal.glsl:120-149)
+inline f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float roughness, float metallic,
+                        float specular_intensity) {
+    const float NdotL = gmax(dot(N, L), 0.001f);
+    if (NdotL < 0.001f) return mk(0, 0, 0);
+    const float rc = gmax(roughness, 0.01f);
+    const float spec_exp = 2.0f / (rc * rc);
+    const f3 H = normalize(sub(L, V));
+    const float NdotH = gmax(dot(N, H), 0.001f);
+    const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
+    const float specular = spec_norm * std::pow(NdotH, spec_exp);
+    const float kS = specular_intensity * metallic;
+    const float kD = 1.0f - kS * 0.5f;
+    const f3 diffuse = muls(muls(albedo, kD), 0.31831f);
+    const float sp = specular * kS;
+    return muls(mk(diffuse.x + sp, diffuse.y + sp, diffuse.z + sp), NdotL);
+}
+
+// smithG1GGX / sampleGGXVNDF / ggxThroughput (internal.glsl:165-239);
+// pow(x, 5.0) is evaluated as x*x*x*x*x, sin/cos via sincos_turn.
+inline float smith_g1(float NdotX, float a) {
+    const float a2 = a * a;
+    return 2.0f * NdotX / (NdotX + std::sqrt(a2 + (1.0f - a2) * NdotX * NdotX));
+}
+inline f3 sample_ggx_vndf(f3 N, f3 V, float roughness, uint32_t& rng) {
+    const float a = gmax(roughness * roughness, 0.001f);
+    const f3 up = std::fabs(N.z) < 0.999f ? mk(0, 0, 1) : mk(1, 0, 0);
+    const f3 T = normalize(cross(up, N));
+    const f3 B = cross(N, T);
+    const f3 Vl = mk(dot(V, T), dot(V, B), dot(V, N));
+    const f3 Vh = normalize(mk(a * Vl.x, a * Vl.y, Vl.z));
+    const float lensq = Vh.x * Vh.x + Vh.y * Vh.y;
+    f3 T1;
+    if (lensq > 0.0f) {
+        const float is = 1.0f / std::sqrt(lensq);
+        T1 = mk(-Vh.y * is, Vh.x * is, 0.0f);
+    } else {
+        T1 = mk(1, 0, 0);
+    }
+    const f3 T2 = cross(Vh, T1);
+    const float r1 = rand01(rng);
+    const float r2 = rand01(rng);
+    const float r = std::sqrt(r1);
+    float sn, cs;
+    sincos_turn(r2, &sn, &cs);
+    const float t1 = r * cs;
+    float t2 = r * sn;
+    const float s = 0.5f * (1.0f + Vh.z);
+    t2 = (1.0f - s) * std::sqrt(gmax(1.0f - t1 * t1, 0.0f)) + s * t2;
+    const float w = std::sqrt(gmax(0.0f, 1.0f - t1 * t1 - t2 * t2));
+    const f3 Nh = add(add(muls(T1, t1), muls(T2, t2)), muls(Vh, w));
+    const f3 Hl = normalize(mk(a * Nh.x, a * Nh.y, gmax(0.0f, Nh.z)));
+    return add(add(muls(T, Hl.x), muls(B, Hl.y)), muls(N, Hl.z));
+}
+inline f3 ggx_throughput(f3 N, f3 V, f3 L, f3 H, float roughness, f3 F0) {
+    const float NdotL = gmax(dot(N, L), 0.001f);
+    const float VdotH = gmax(dot(V, H), 0.001f);
+    const float a = roughness * roughness;
+    const float x = 1.0f - VdotH;
+    const float x2 = x * x;
+    const float x5 = x2 * x2 * x;
+    const f3 F = mk(F0.x + (1.0f - F0.x) * x5, F0.y + (1.0f - F0.y) * x5, F0.z + (1.0f - F0.z) * x5);
+    return muls(F, smith_g1(NdotL, a));
+}
+// reflect(I, N) = I - 2*dot(N,I)*N (GLSL spec)
+inline f3 reflect(f3 I, f3 N) { return sub(I, muls(N, 2.0f * dot(N, I))); }
+
+// ---------------------------------------------------------------------------
+// Normals.  The reference computes per-voxel normals in normal.comp
+// (:55-95) as normalize(sum of offsets of EMPTY neighbours) with an L2-ball
+// neighbourhood and caches them 10-10-10 packed; the benchmark method uses the
+// full 3x3x3 neighbourhood and keeps the integer sum in the leaf word's unused
+// 24-bit `normal` field (octree.hpp:29): bits 8-12 x, 13-17 y, 18-22 z (5-bit
+// two's complement, each in [-9, 9]), bit 31 = "normal present".
+// ---------------------------------------------------------------------------
+// lookupOccupied (normal.comp:55-70)
+bool lookup_occupied(const Scene& s, int64_t x, int64_t y, int64_t z) {
+    const uint32_t L = 1u << s.depth;
+    if (x < 0 || y < 0 || z < 0 || x >= L || y >= L || z >= L) return false;
+    uint32_t off = 0, raw;
+    for (uint32_t d = 0; d < s.depth; d++) {
+        off += locate(uint32_t(x), uint32_t(y), uint32_t(z), L >> d);
+        raw = s.fetch(off);
+        if (!(raw & 1u)) return bool((raw >> 1) & 0x7Fu);
+        off = (raw >> 4) & 0x0FFFFFFFu;
+    }
+    off += locate(uint32_t(x), uint32_t(y), uint32_t(z), L >> s.depth);
+    raw = s.fetch(off);
+    return bool((raw >> 1) & 0x7Fu);
+}
+
+uint32_t encode_normal_field(int ix, int iy, int iz) {
+    return ((uint32_t(ix) & 31u) << 8) | ((uint32_t(iy) & 31u) << 13) | ((uint32_t(iz) & 31u) << 18) |
+           (1u << 31);
+}
+inline int sext5(uint32_t v) { return (v & 16u) ? int(v) - 32 : int(v); }
+
+// Shading normal for a hit: decode the gradient sum, then normalize ->
+// packNormalAccum (normal.comp:90-95) -> UnpackNormal (internal.glsl:22-28)
+// -> normalize, as shade.comp:267 reads it.  Leaves without a stored normal
+// use the face-normal fallback of lookupNormal (shade.comp:271-274).
+f3 shading_normal(uint32_t leaf_word, f3 ray_dir) {
+    if (!(leaf_word >> 31)) {
+        const f3 a = mk(std::fabs(ray_dir.x), std::fabs(ray_dir.y), std::fabs(ray_dir.z));
+        auto sgn = [](float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); };
+        if (a.x > a.y && a.x > a.z) return mk(-sgn(ray_dir.x), 0.0f, 0.0f);
+        if (a.y > a.z) return mk(0.0f, -sgn(ray_dir.y), 0.0f);
+        return mk(0.0f, 0.0f, -sgn(ray_dir.z));
+    }
+    const f3 acc = mk(float(sext5((leaf_word >> 8) & 31u)), float(sext5((leaf_word >> 13) & 31u)),
+                      float(sext5((leaf_word >> 18) & 31u)));
+    const float len = std::sqrt(dot(acc, acc));
+    const f3 n = len > 0.001f ? divs(acc, len) : mk(0.0f, 1.0f, 0.0f);
+    auto pack = [](float c) {
+        int v = int(std::round((c + 1.0f) * 511.0f));
+        v = v < 0 ? 0 : (v > 1022 ? 1022 : v);
+        return uint32_t(v);
+    };
+    const uint32_t px = pack(n.x), py = pack(n.y), pz = pack(n.z);
+    const f3 u = mk(float(px) / 511.0f - 1.0f, float(py) / 511.0f - 1.0f, float(pz) / 511.0f - 1.0f);
+    return normalize(u);
+}
+
+// ---------------------------------------------------------------------------
+// Pointer octree restated from src/octree_cpu.cpp (insert/insertR :33-64,
+// remove/removeR :66-98, lookup :100-112) and src/renderer/octree.cpp
+// (set :127-166, linearizeNode :170-217).
+// ---------------------------------------------------------------------------
+struct PNode {
+    PNode* child[8] = {};
+    uint8_t count = 0;
+    uint32_t material = 0;
+};
+struct PTree {
+    PNode* root = nullptr;
+    uint32_t depth;
+    uint32_t p2r[18];
+    std::vector<std::unique_ptr<PNode>> pool;
+    explicit PTree(uint32_t d) : depth(d) {
+        uint32_t p = 1;
+        for (int i = int(d); i >= 1; i--) { p2r[i] = p; p <<= 1; }
+        p2r[0] = p;
+    }
+    PNode* alloc() { pool.emplace_back(new PNode()); return pool.back().get(); }
+    void insert(uint32_t x, uint32_t y, uint32_t z, uint32_t m) {
+        const uint32_t b = 1u << depth;
+        if (x >= b || y >= b || z >= b) return;
+        if (!root) root = alloc();
+        PNode* n = root;
+        for (uint32_t level = 1; level <= depth; level++) {
+            const uint32_t idx = locate(x, y, z, p2r[level]);
+            if (!n->child[idx]) { n->child[idx] = alloc(); n->count++; }
+            n = n->child[idx];
+        }
+        n->material = m;
+        n->count = 0;
+    }
+    // Octree::set slot order: slot 0 root, 1-8 root children (processed in
+    // order 0..7), each internal node gets an 8-slot block at `size` in
+    // iterative-DFS LIFO order (children pushed 0..7, popped 7..0).
+    std::vector<uint32_t> linearize(uint32_t* size_out, uint32_t* nvox) const {
+        std::vector<uint32_t> data(9, 0u);
+        uint32_t size = 9, nv = 0;
+        if (!root) { *size_out = 9; *nvox = 0; return data; }
+        data[0] = 1u | ((uint32_t(root->count) & 7u) << 1) | (1u << 4);
+        for (int i = 0; i < 8; i++) {
+            std::stack<std::tuple<PNode*, uint32_t, uint32_t>> st;
+            st.push({root->child[i], uint32_t(i + 1), 2u});
+            while (!st.empty()) {
+                auto [cn, off, lv] = st.top();
+                st.pop();
+                if (!cn) continue;
+                if (lv > depth || (cn->material != 0 && cn->count == 0)) {
+                    if (cn->material == 0) continue;
+                    if (data.size() <= off) data.resize(off + 1, 0u);
+                    data[off] = ((cn->material & 0x7Fu) << 1);
+                    nv++;
+                } else {
+                    const uint32_t block = size;
+                    size += 8;
+                    if (data.size() < size) data.resize(size, 0u);
+                    data[off] = 1u | ((uint32_t(cn->count) & 7u) << 1) | (block << 4);
+                    for (int k = 0; k < 8; k++) st.push({cn->child[k], block + uint32_t(k), lv + 1});
+                }
+            }
+        }
+        data.resize(size, 0u);
+        *size_out = size;
+        *nvox = nv;
+        return data;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// FP64 radiance cache: the re-accumulation reference for the product's FP32
+// hash cache.  Keyed by voxel id (voxelKey + 1).
+// ---------------------------------------------------------------------------
+struct CacheEntry {
+    uint64_t count = 0;
+    double weight = 0, r = 0, g = 0, b = 0, l2 = 0;
+};
+struct Cache {
+    std::unordered_map<uint32_t, CacheEntry> map;
+};
+
+struct Deposit {
+    uint32_t vid;
+    float rgb[3];
+};
+
+struct PathOut {
+    f3 direct{0, 0, 0}, indirect{0, 0, 0};
+};
+
+// The per-pixel plain method: one path of the bounce/shade loop
+// (shade.comp:543-575, 838-908) from a known primary hit, with the sun
+// next-event estimate in the place of the emissive NEE (shade.comp:631-836 is
+// dormant in scenes without emissive voxels).
+void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_frame_params& P,
+                const Hit& primary, f3 primary_dir, uint32_t pix_index, uint32_t sample, PathOut* out,
+                ov_stats* st, RayCounters* rc) {
+    const uint32_t max_bounces = P.bounces + 1u;  // MAX_BOUNCES (wavefront.glsl:23)
+    const uint32_t list_idx = pix_index * P.spp + sample;
+    // emit.comp:171-174
+    const uint32_t sample_idx = P.frame_index + pix_index * 2654435761u + list_idx * 1442695040u;
+    uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+    f3 tp = mk(1, 1, 1);
+    f3 dir = primary_dir;
+    f3 direct = mk(0, 0, 0), indirect = mk(0, 0, 0);
+    Hit hit = primary;
+    const f3 sun = mk(P.sun_dir[0], P.sun_dir[1], P.sun_dir[2]);
+    const f3 sky = mk(P.sky[0], P.sky[1], P.sky[2]);
+    uint32_t b = 0;
+    for (;;) {
+        if (hit.status != ST_HIT) {  // shade.comp:558-564 (sky in place of the cubemap)
+            indirect = add(indirect, mul(sky, tp));
+            break;
+        }
+        const uint32_t mi = hit.material < n_mats ? hit.material : 0u;
+        const Material& m = mats[mi];
+        const f3 albedo = mk(m.color[0], m.color[1], m.color[2]);
+        const f3 N = shading_normal(s.fetch(hit.id), dir);
+        if (m.emissive) {  // shade.comp:576-583
+            const float k = m.emissive_intensity;
+            f3 e = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
+            e = mk(gmin(e.x, 20.0f), gmin(e.y, 20.0f), gmin(e.z, 20.0f));
+            if (b == 0) direct = add(direct, e); else indirect = add(indirect, e);
+        }
+        const f3 hit_pos = mk(float(hit.pos[0]), float(hit.pos[1]), float(hit.pos[2]));
+        const f3 shading_point = add(add(hit_pos, mk(0.5f, 0.5f, 0.5f)), N);  // shade.comp:635, 892
+        // NEE gate of shade.comp:631 (non-emissive surface, bounce < 2), with
+        // the sun's cosine test of shade.comp:811-815.
+        if (!m.emissive && b < 2u && dot(N, sun) > 0.0f) {
+            const Hit sh = raycast(s, shading_point, sun, P.bounce_controlchecks, rc);
+            st->rays_shadow++;
+            if (sh.status == ST_ESCAPED) {
+                const f3 brdf = evaluate_brdf(dir, sun, N, albedo, m.roughness, m.metallic, m.specular);
+                f3 c = muls(brdf, P.sun_intensity);
+                c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
+                const f3 w = mul(tp, c);
+                if (b == 0) direct = add(direct, w); else indirect = add(indirect, w);
+            }
+        }
+        if (b + 1u >= max_bounces) break;  // shade.comp:840-845
+        // BRDF sample (shade.comp:850-873)
+        const bool use_ggx = m.metallic * (1.0f - m.roughness) > 0.5f;
+        f3 sdir, bt;
+        if (use_ggx) {
+            const f3 V = mk(-dir.x, -dir.y, -dir.z);
+            const f3 H = sample_ggx_vndf(N, V, m.roughness, rng);
+            sdir = reflect(dir, H);
+            if (dot(sdir, N) <= 0.0f) {
+                sdir = cosine_direction(N, rng);
+                bt = evaluate_brdf(dir, sdir, N, albedo, m.roughness, m.metallic, m.specular);
+            } else {
+                const f3 F0 = mk(0.04f * (1.0f - m.metallic) + albedo.x * m.metallic,
+                                 0.04f * (1.0f - m.metallic) + albedo.y * m.metallic,
+                                 0.04f * (1.0f - m.metallic) + albedo.z * m.metallic);
+                bt = ggx_throughput(N, V, sdir, H, m.roughness, F0);
+            }
+        } else {
+            sdir = cosine_direction(N, rng);
+            bt = evaluate_brdf(dir, sdir, N, albedo, m.roughness, m.metallic, m.specular);
+        }
+        f3 ntp = mul(tp, bt);
+        // Russian roulette (shade.comp:879-889), RR_START_BOUNCE = 2
+        if (b + 1u >= 2u) {
+            const float p = gclamp(gmax(ntp.x, gmax(ntp.y, ntp.z)), 0.05f, 0.95f);
+            const float xi = rand01(rng);
+            if (xi > p) break;
+            ntp = divs(ntp, p);
+        }
+        // survivor (shade.comp:892-895) + trace.comp
+        tp = ntp;
+        dir = sdir;
+        b++;
+        hit = raycast(s, shading_point, sdir, P.bounce_controlchecks, rc);
+        st->rays_bounce++;
+    }
+    out->direct = direct;
+    out->indirect = indirect;
+}
+
+// Deposit value: the reference quantises each channel with
+// clamp(rgb, 0, 1024) (packRgbL2, shade.comp:154-160); the FP cache keeps the
+// clamped channels as floats, direct + indirect summed.
+inline void deposit_value(const PathOut& p, float out[3]) {
+    const float dv[3] = {p.direct.x, p.direct.y, p.direct.z};
+    const float iv[3] = {p.indirect.x, p.indirect.y, p.indirect.z};
+    for (int c = 0; c < 3; c++) {
+        float a = dv[c], b = iv[c];
+        if (!(a == a)) a = 0.0f;
+        if (!(b == b)) b = 0.0f;
+        out[c] = gclamp(a, 0.0f, 1024.0f) + gclamp(b, 0.0f, 1024.0f);
+    }
+}
+
+// lookupVoxelAvg (resolve.comp:109-148) over the FP64 cache.
+struct Avg {
+    double rgb[3];
+    uint64_t count;
+    double var;
+};
+Avg lookup_avg(const Cache& c, uint32_t vid) {
+    Avg a{{0, 0, 0}, 0, 0};
+    if (vid == 0) return a;
+    auto it = c.map.find(vid);
+    if (it == c.map.end()) return a;
+    const CacheEntry& e = it->second;
+    a.count = e.count;
+    if (e.count == 0 || e.weight <= 0.0) return a;
+    const double inv = 1.0 / e.weight;
+    a.rgb[0] = e.r * inv; a.rgb[1] = e.g * inv; a.rgb[2] = e.b * inv;
+    const double meanL = (e.r + e.g + e.b) * inv / 3.0;
+    a.var = std::max(e.l2 * inv - meanL * meanL, 0.0);
+    return a;
+}
+
+inline double aces(double x) {  // final.frag:11-18
+    double v = (x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14);
+    return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+}
+
+struct Renderer {
+    Cache cache;
+};
+
+}  // namespace
+
+// ===========================================================================
+// C API (ctypes)
+// ===========================================================================
+extern "C" {
+
+uint32_t oracle_version() { return 3u; }
+
+// Builds the reference layout from a voxel list (x, y, z, material) by
+// OctreeCPU::insert order then Octree::set.  Returns the word count
+// (== size) and writes up to `cap` words.
+uint64_t oracle_build(uint32_t depth, const uint32_t* xyzm, uint64_t n, uint32_t* out, uint64_t cap,
+                      uint32_t* nvox) {
+    PTree t(depth);
+    for (uint64_t i = 0; i < n; i++) t.insert(xyzm[4 * i], xyzm[4 * i + 1], xyzm[4 * i + 2], xyzm[4 * i + 3]);
+    uint32_t size = 0, nv = 0;
+    std::vector<uint32_t> d = t.linearize(&size, &nv);
+    const uint64_t m = std::min<uint64_t>(d.size(), cap);
+    if (out) std::memcpy(out, d.data(), m * 4);
+    if (nvox) *nvox = nv;
+    return d.size();
+}
+
+// normal.comp restated over the 3x3x3 neighbourhood; writes the normal field
+// into every leaf word of `words` (in place).  Leaves are found by walking
+// the tree from the root.
+void oracle_fill_normals(uint32_t* words, uint64_t n, uint32_t depth) {
+    std::vector<uint32_t> copy(words, words + n);
+    Scene s{copy.data(), n, depth};
+    const uint32_t L = 1u << depth;
+    struct E { uint32_t off, level, x, y, z; };
+    std::vector<E> st;
+    // root block: slots 1..8 are the root's children at CPU level 2
+    for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t half = L >> 1;
+        st.push_back({1u + i, 1u, (i & 4) ? half : 0u, (i & 2) ? half : 0u, (i & 1) ? half : 0u});
+    }
+    while (!st.empty()) {
+        E e = st.back();
+        st.pop_back();
+        const uint32_t raw = s.fetch(e.off);
+        if (raw & 1u) {
+            const uint32_t next = node_next(raw);
+            const uint32_t half = L >> (e.level + 1);
+            for (uint32_t i = 0; i < 8; i++)
+                st.push_back({next + i, e.level + 1, e.x + ((i & 4) ? half : 0u), e.y + ((i & 2) ? half : 0u),
+                              e.z + ((i & 1) ? half : 0u)});
+        } else if (node_material(raw) != 0u && e.level == depth) {
+            int ax = 0, ay = 0, az = 0;
+            for (int dx = -1; dx <= 1; dx++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dz = -1; dz <= 1; dz++) {
+                        if (dx == 0 && dy == 0 && dz == 0) continue;
+                        if (!lookup_occupied(s, int64_t(e.x) + dx, int64_t(e.y) + dy, int64_t(e.z) + dz)) {
+                            ax += dx; ay += dy; az += dz;
+                        }
+                    }
+            words[e.off] = (raw & 0xFFu) | encode_normal_field(ax, ay, az);
+        }
+    }
+}
+
+int oracle_lookup_occupied(const uint32_t* words, uint64_t n, uint32_t depth, int64_t x, int64_t y, int64_t z) {
+    Scene s{words, n, depth};
+    return lookup_occupied(s, x, y, z) ? 1 : 0;
+}
+
+// Camera::UpdateUBO (src/renderer/camera.cpp:39-50): ubo = {position,
+// cameraPlane = direction, right, up} as 4 x vec4.
+void oracle_camera_ubo(const float pos[3], const float dir[3], float fov_deg, float aspect, float ubo[16]) {
+    // glm (host) semantics: normalize(v) = v * inversesqrt(dot(v, v))
+    auto gnorm = [](f3 v) { return muls(v, 1.0f / std::sqrt(dot(v, v))); };
+    const f3 d = mk(dir[0], dir[1], dir[2]);
+    const float tn = std::tan((fov_deg / 2.0f) * 0.01745329251994329576923690768489f);
+    const f3 right = muls(muls(gnorm(cross(mk(0, 1, 0), d)), tn), aspect);
+    const f3 up = muls(gnorm(cross(right, d)), tn);
+    const float v[16] = {pos[0], pos[1], pos[2], 0, d.x, d.y, d.z, 0, right.x, right.y, right.z, 0,
+                         up.x, up.y, up.z, 0};
+    std::memcpy(ubo, v, sizeof(v));
+}
+
+// Single ray through the restated DDA.  out = {status, id, material, x, y,
+// z, size, checks}; fetch counters accumulate into fetch[2] when non-null.
+void oracle_raycast(const uint32_t* words, uint64_t n, uint32_t depth, const float o[3], const float d[3],
+                    uint32_t controlchecks, uint32_t out[8], uint64_t fetch[2]) {
+    Scene s{words, n, depth};
+    RayCounters rc;
+    Hit h = raycast(s, mk(o[0], o[1], o[2]), mk(d[0], d[1], d[2]), controlchecks, &rc);
+    out[0] = uint32_t(h.status); out[1] = h.id; out[2] = h.material;
+    out[3] = h.pos[0]; out[4] = h.pos[1]; out[5] = h.pos[2];
+    out[6] = h.size; out[7] = h.checks;
+    if (fetch) { fetch[0] += rc.fetch_restart; fetch[1] += rc.fetch_min; }
+}
+
+uint32_t oracle_voxel_key(uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t p[3] = {x, y, z};
+    return voxel_key(p);
+}
+
+// Draws `n` values of rand() from `state` (golden RNG vectors).
+uint32_t oracle_rand_seq(uint32_t state, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; i++) out[i] = rand01(state);
+    return state;
+}
+
+void oracle_sincos_turn(const float* u, uint64_t n, float* s, float* c) {
+    for (uint64_t i = 0; i < n; i++) sincos_turn(u[i], &s[i], &c[i]);
+}
+
+void oracle_shading_normal(uint32_t leaf_word, const float dir[3], float out[3]) {
+    f3 v = shading_normal(leaf_word, mk(dir[0], dir[1], dir[2]));
+    out[0] = v.x; out[1] = v.y; out[2] = v.z;
+}
+
+void* oracle_renderer_new() { return new Renderer(); }
+void oracle_renderer_free(void* r) { delete static_cast<Renderer*>(r); }
+
+// Number of cache entries and a dump: vids[i], counts[i], and
+// values[5*i..] = {weight, r, g, b, l2} (FP64).
+uint64_t oracle_cache_dump(void* rp, uint32_t* vids, uint64_t* counts, double* values, uint64_t cap) {
+    Renderer* r = static_cast<Renderer*>(rp);
+    uint64_t i = 0;
+    std::vector<uint32_t> keys;
+    keys.reserve(r->cache.map.size());
+    for (auto& kv : r->cache.map) keys.push_back(kv.first);
+    std::sort(keys.begin(), keys.end());
+    for (uint32_t k : keys) {
+        if (i >= cap) break;
+        const CacheEntry& e = r->cache.map[k];
+        if (vids) vids[i] = k;
+        if (counts) counts[i] = e.count;
+        if (values) {
+            values[5 * i] = e.weight; values[5 * i + 1] = e.r; values[5 * i + 2] = e.g;
+            values[5 * i + 3] = e.b; values[5 * i + 4] = e.l2;
+        }
+        i++;
+    }
+    return keys.size();
+}
+
+// One frame of the plain method (the four passes of
+// Renderer::runWavefrontFrame, renderer.cpp:282-649, in per-pixel form):
+//   1 primary DDA per pixel -> GBuffer {checks, material, hit node, vid}
+//     (generate_primary.comp:38-85; .z carries the hit-node index)
+//   2 spp paths per hit pixel through the bounce/shade loop (trace_path)
+//   3 AccumPass: decay then deposit into the FP64 cache (fixed merge order)
+//   4 AvgPass + tonemap per pixel (resolve.comp:362-382, final.frag:11-18)
+// Rows [row_begin, row_end) are rendered (all rows when row_end == 0) with
+// `threads` std::threads, one contiguous row band each.  gbuf: 4 u32 per
+// pixel; rgb, mapped: 3 f32 per pixel (null to skip).  Paths' per-sample
+// values are written to `path_rgb` (3 f32 per path, index pix*spp+s) when
+// non-null.
+int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint32_t depth, const void* materials,
+                        uint32_t n_mats, const float cam[16], const ov_frame_params* P, uint32_t threads,
+                        uint32_t row_begin, uint32_t row_end, uint32_t* gbuf, float* rgb, float* mapped,
+                        float* path_rgb, ov_stats* stats_out) {
+    Renderer* R = static_cast<Renderer*>(rp);
+    Scene s{words, n_words, depth};
+    const Material* mats = static_cast<const Material*>(materials);
+    const uint32_t W = P->width, H = P->height;
+    if (row_end == 0 || row_end > H) row_end = H;
+    if (row_begin > row_end) row_begin = row_end;
+    if (threads == 0) threads = 1;
+
+    // temporal decay of the cache before this frame's deposits
+    for (auto& kv : R->cache.map) {
+        CacheEntry& e = kv.second;
+        const double k = P->decay;
+        e.weight *= k; e.r *= k; e.g *= k; e.b *= k; e.l2 *= k;
+    }
+
+    const f3 cpos = mk(cam[0], cam[1], cam[2]);
+    const f3 plane = mk(cam[4], cam[5], cam[6]);
+    const f3 right = mk(cam[8], cam[9], cam[10]);
+    const f3 up = mk(cam[12], cam[13], cam[14]);
+
+    std::vector<std::vector<Deposit>> deps(threads);
+    std::vector<ov_stats> tstats(threads);
+    std::vector<RayCounters> trc(threads);
+    const uint32_t rows = row_end - row_begin;
+    auto work = [&](uint32_t t) {
+        const uint32_t r0 = row_begin + uint32_t(uint64_t(rows) * t / threads);
+        const uint32_t r1 = row_begin + uint32_t(uint64_t(rows) * (t + 1) / threads);
+        ov_stats& st = tstats[t];
+        std::memset(&st, 0, sizeof(st));
+        for (uint32_t py = r0; py < r1; py++) {
+            for (uint32_t px = 0; px < W; px++) {
+                // pixel -> ray (generate_primary.comp:44-52)
+                const float ndx = (float(px) + 0.5f) / float(W) * 2.0f - 1.0f;
+                const float ndy = (float(py) + 0.5f) / float(H) * 2.0f - 1.0f;
+                const f3 dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
+                const Hit h = raycast(s, cpos, dir, P->primary_controlchecks, &trc[t]);
+                st.rays_primary++;
+                const uint32_t pix = py * W + px;
+                uint32_t vid = 0;
+                if (h.status == ST_HIT) vid = voxel_key(h.pos) + 1u;
+                if (gbuf) {
+                    gbuf[4 * uint64_t(pix) + 0] = h.checks;
+                    gbuf[4 * uint64_t(pix) + 1] = h.status == ST_HIT ? h.material : 0u;
+                    gbuf[4 * uint64_t(pix) + 2] = h.status == ST_HIT ? h.id : 0u;
+                    gbuf[4 * uint64_t(pix) + 3] = vid;
+                }
+                if (vid == 0) continue;
+                for (uint32_t smp = 0; smp < P->spp; smp++) {
+                    PathOut po;
+                    trace_path(s, mats, n_mats, *P, h, dir, pix, smp, &po, &st, &trc[t]);
+                    st.paths++;
+                    Deposit dp;
+                    dp.vid = vid;
+                    deposit_value(po, dp.rgb);
+                    if (path_rgb) {
+                        float* o = path_rgb + 3 * (uint64_t(pix) * P->spp + smp);
+                        o[0] = dp.rgb[0]; o[1] = dp.rgb[1]; o[2] = dp.rgb[2];
+                    }
+                    deps[t].push_back(dp);
+                }
+            }
+        }
+    };
+    if (threads == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < threads; t++) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+    ov_stats total{};
+    for (uint32_t t = 0; t < threads; t++) {
+        total.rays_primary += tstats[t].rays_primary;
+        total.rays_bounce += tstats[t].rays_bounce;
+        total.rays_shadow += tstats[t].rays_shadow;
+        total.paths += tstats[t].paths;
+        total.fetch_restart += trc[t].fetch_restart;
+        total.fetch_min += trc[t].fetch_min;
+        total.steps += trc[t].steps;
+        for (const Deposit& d : deps[t]) {
+            CacheEntry& e = R->cache.map[d.vid];
+            const double r = d.rgb[0], g = d.rgb[1], b = d.rgb[2];
+            const float Lf = ((d.rgb[0] + d.rgb[1]) + d.rgb[2]) / 3.0f;
+            e.count += 1;
+            e.weight += 1.0;
+            e.r += r; e.g += g; e.b += b;
+            e.l2 += double(Lf * Lf);
+            total.deposits++;
+        }
+    }
+
+    // AvgPass (resolve.comp main :362-382 with resolveDefault :224-261,
+    // reconstructTimeout :193-219, and the visualisation modes :266-359)
+    if (rgb || mapped) {
+        const double sky[3] = {P->sky[0], P->sky[1], P->sky[2]};
+        auto gb = [&](int64_t x, int64_t y, int k) -> uint32_t {
+            if (y < int64_t(row_begin) || y >= int64_t(row_end)) return 0u;
+            return gbuf[4 * uint64_t(y * W + x) + k];
+        };
+        const int dxs[4] = {1, -1, 0, 0}, dys[4] = {0, 0, 1, -1};
+        for (uint32_t py = row_begin; py < row_end; py++) {
+            for (uint32_t px = 0; px < W; px++) {
+                const uint32_t pix = py * W + px;
+                const uint32_t checks = gb(px, py, 0), mat = gb(px, py, 1), node = gb(px, py, 2),
+                               vid = gb(px, py, 3);
+                double col[3] = {0, 0, 0};
+                auto reconstruct = [&]() {
+                    double sum[3] = {0, 0, 0}, ws = 0;
+                    const int R_ = int(P->reconstruction_radius);
+                    for (int dy = -R_; dy <= R_; dy++)
+                        for (int dx = -R_; dx <= R_; dx++) {
+                            if (dx == 0 && dy == 0) continue;
+                            const int64_t qx = int64_t(px) + dx, qy = int64_t(py) + dy;
+                            if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+                            const uint32_t nv = gb(qx, qy, 3), nc = gb(qx, qy, 0);
+                            if (nv == 0 || nc >= P->primary_controlchecks) continue;
+                            Avg a = lookup_avg(R->cache, nv);
+                            if (a.count == 0) continue;
+                            const double dist = double(dx * dx + dy * dy);
+                            const double w = double(std::min<uint64_t>(a.count, 32)) / (1.0 + dist * 0.15);
+                            for (int c = 0; c < 3; c++) sum[c] += a.rgb[c] * w;
+                            ws += w;
+                        }
+                    if (ws > 0.0001) { for (int c = 0; c < 3; c++) col[c] = sum[c] / ws; }
+                    else { for (int c = 0; c < 3; c++) col[c] = sky[c]; }
+                };
+                auto miss = [&]() {
+                    if (checks >= P->primary_controlchecks) reconstruct();
+                    else { for (int c = 0; c < 3; c++) col[c] = sky[c]; }
+                };
+                switch (P->render_type) {
+                    case 1:  // STRUCTURE
+                        for (int c = 0; c < 3; c++) col[c] = double(float(checks) / 65.0f);
+                        break;
+                    case 2:  // ALBEDO
+                        if (vid == 0) miss();
+                        else if (mat != 0 && mat < 127 && mat < n_mats)
+                            for (int c = 0; c < 3; c++) col[c] = mats[mat].color[c];
+                        break;
+                    case 3:  // NORMAL (from the leaf word's normal field)
+                        if (vid == 0) miss();
+                        else {
+                            const uint32_t w = s.fetch(node);
+                            if (w >> 31) {
+                                const f3 nd = mk(0, 0, 1);
+                                f3 nn = shading_normal(w, nd);
+                                col[0] = nn.x * 0.5 + 0.5; col[1] = nn.y * 0.5 + 0.5; col[2] = nn.z * 0.5 + 0.5;
+                            }
+                        }
+                        break;
+                    case 4:  // VOXELID
+                        if (vid == 0) miss();
+                        else {
+                            const uint32_t hid = vid - 1u;
+                            col[0] = double(float((hid + 1u) % 255u) / 255.0f);
+                            col[1] = double(float(((hid + 1u) / 255u) % 255u) / 255.0f);
+                            col[2] = double(float(((hid + 1u) / (255u * 255u)) % 255u) / 255.0f);
+                        }
+                        break;
+                    case 5:  // VARIANCE
+                        if (vid == 0) miss();
+                        else {
+                            Avg a = lookup_avg(R->cache, vid);
+                            double v = a.count >= 2 ? a.var : 0.0;
+                            double sc = v * (255.0 * 255.0) / std::max<double>(P->variance_norm, 1.0);
+                            sc = sc < 0 ? 0 : (sc > 1 ? 1 : sc);
+                            for (int c = 0; c < 3; c++) col[c] = sc;
+                        }
+                        break;
+                    default: {  // DEFAULT
+                        if (vid == 0) { miss(); break; }
+                        Avg a = lookup_avg(R->cache, vid);
+                        if (a.count >= 128 && a.var < 0.02) {
+                            for (int c = 0; c < 3; c++) col[c] = a.rgb[c];
+                            break;
+                        }
+                        double sum[3], ws = double(a.count);
+                        for (int c = 0; c < 3; c++) sum[c] = a.rgb[c] * double(a.count);
+                        for (int k = 0; k < 4; k++) {
+                            const int64_t qx = int64_t(px) + dxs[k], qy = int64_t(py) + dys[k];
+                            if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
+                            const uint32_t nv = gb(qx, qy, 3);
+                            if (nv == 0 || nv == vid) continue;
+                            Avg na = lookup_avg(R->cache, nv);
+                            if (na.count == 0) continue;
+                            const double d0 = na.rgb[0] - a.rgb[0], d1 = na.rgb[1] - a.rgb[1],
+                                         d2 = na.rgb[2] - a.rgb[2];
+                            const double dc = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                            const double wc = std::exp(-dc * 6.0);
+                            const double wv = 1.0 / (1.0 + na.var * 32.0);
+                            const double w = wc * wv * double(std::min<uint64_t>(na.count, 32));
+                            for (int c = 0; c < 3; c++) sum[c] += na.rgb[c] * w;
+                            ws += w;
+                        }
+                        if (ws > 0.0001) for (int c = 0; c < 3; c++) col[c] = sum[c] / ws;
+                        break;
+                    }
+                }
+                if (rgb) for (int c = 0; c < 3; c++) rgb[3 * uint64_t(pix) + c] = float(col[c]);
+                if (mapped) for (int c = 0; c < 3; c++) mapped[3 * uint64_t(pix) + c] = float(aces(col[c]));
+            }
+        }
+    }
+    if (stats_out) *stats_out = total;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,535 @@
+"""voxelengine3.0_b200 — B200-native voxel ray pipeline (RayPass, bounce/shade
+loop, AccumPass, AvgPass of AnghelusAndrei/VoxelEngine3.0).
+
+This module binds the native library ``libve.so`` (C ABI: include/ve.h) with
+ctypes and mirrors the reference's host interface:
+
+* ``OctreeCPU``   — src/octree_cpu.hpp:9-57 (insert / remove / lookup /
+  insertBox / insertSphere / raycast)
+* ``Octree``      — src/renderer/octree.hpp:14-98 (set / applyEdits /
+  findGpuSlot, node words in the reference layout)
+* ``camera_ubo``  — Camera::UpdateUBO, src/renderer/camera.cpp:39-50
+* ``FrameConfig`` — core::FrameConfig, src/renderer/core.hpp:83-158
+* ``Renderer``    — src/renderer/renderer.hpp:9-129 (``run`` renders one frame)
+
+There is no CPU fallback: every render call runs the CUDA kernels of
+libve.so, and loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+import os
+from typing import Dict, Iterable, List, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libve.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "ve.h")
+
+VE_OK = 0
+VE_ERR_INVALID = -1
+VE_ERR_CUDA = -2
+VE_ERR_NOMEM = -3
+VE_ERR_CAPACITY = -4
+VE_ERR_NOT_FOUND = -5
+VE_ERR_TIMEOUT = -6
+VE_ERR_STATE = -7
+
+RENDER_DEFAULT, RENDER_STRUCTURE, RENDER_ALBEDO, RENDER_NORMAL, RENDER_VOXELID, RENDER_VARIANCE = range(6)
+SCENE_KEEP_NORMALS = 1
+FRAME_TIMING = 1
+FRAME_COUNT_FETCH = 2
+FRAME_PATH_RGB = 4
+
+
+class VeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ve error {code}: {msg}")
+        self.code = code
+
+
+# ---------------------------------------------------------------------------
+# ctypes structures (include/ve.h)
+# ---------------------------------------------------------------------------
+class RendererConfigC(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("hash_log2", ctypes.c_uint32), ("hash_probes", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class FrameConfigC(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("bounces", ctypes.c_uint32), ("primary_controlchecks", ctypes.c_uint32),
+                ("bounce_controlchecks", ctypes.c_uint32), ("reconstruction_radius", ctypes.c_uint32),
+                ("render_type", ctypes.c_uint32), ("frame_index", ctypes.c_uint32),
+                ("sun_dir", ctypes.c_float * 3), ("sun_intensity", ctypes.c_float), ("sky", ctypes.c_float * 3),
+                ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", ctypes.c_uint32)]
+
+
+class ViewC(ctypes.Structure):
+    _fields_ = [("scene_id", ctypes.c_int32), ("camera", ctypes.c_float * 16), ("frame", FrameConfigC)]
+
+
+class FrameOutputsC(ctypes.Structure):
+    _fields_ = [("gbuffer", ctypes.c_void_p), ("voxel_id", ctypes.c_void_p), ("hit_node", ctypes.c_void_p),
+                ("rgb", ctypes.c_void_p), ("mapped", ctypes.c_void_p), ("path_rgb", ctypes.c_void_p)]
+
+
+class FrameStatsC(ctypes.Structure):
+    _fields_ = [("rays_primary", ctypes.c_uint64), ("rays_bounce", ctypes.c_uint64),
+                ("rays_shadow", ctypes.c_uint64), ("fetch_nodes", ctypes.c_uint64), ("paths", ctypes.c_uint64),
+                ("deposits", ctypes.c_uint64), ("deposits_dropped", ctypes.c_uint64), ("dda_steps", ctypes.c_uint64),
+                ("ms_total", ctypes.c_float), ("ms_primary", ctypes.c_float), ("ms_trace", ctypes.c_float),
+                ("ms_shade", ctypes.c_float), ("ms_resolve", ctypes.c_float), ("ms_decay", ctypes.c_float),
+                ("trace_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+                ("cache_capacity", ctypes.c_uint64)]
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_I32 = ctypes.c_int32
+_F = ctypes.c_float
+_PTR = ctypes.POINTER
+
+_SIGNATURES = {
+    "ve_version": ([], ctypes.c_char_p),
+    "ve_last_error": ([], ctypes.c_char_p),
+    "ve_octree_cpu_create": ([_U32, _PTR(_P)], ctypes.c_int),
+    "ve_octree_cpu_destroy": ([_P], ctypes.c_int),
+    "ve_octree_cpu_insert": ([_P, _U32, _U32, _U32, _U32], ctypes.c_int),
+    "ve_octree_cpu_insert_many": ([_P, _P, _U64], ctypes.c_int),
+    "ve_octree_cpu_remove": ([_P, _U32, _U32, _U32], ctypes.c_int),
+    "ve_octree_cpu_lookup": ([_P, _U32, _U32, _U32, _PTR(ctypes.c_int64)], ctypes.c_int),
+    "ve_octree_cpu_insert_box": ([_P, _P, _P, _U32], ctypes.c_int),
+    "ve_octree_cpu_insert_sphere": ([_P, _P, _F, _U32], ctypes.c_int),
+    "ve_octree_cpu_raycast": ([_P, _P, _P, _U32, _PTR(ctypes.c_int), _P], ctypes.c_int),
+    "ve_octree_create": ([_U32, _PTR(_P)], ctypes.c_int),
+    "ve_octree_destroy": ([_P], ctypes.c_int),
+    "ve_octree_set": ([_P, _P], ctypes.c_int),
+    "ve_octree_apply_edits": ([_P, _P, _P, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_octree_last_changed": ([_P, _PTR(_P), _PTR(_U64)], ctypes.c_int),
+    "ve_octree_find_gpu_slot": ([_P, _P, _U32, _U32, _U32, _PTR(_U32)], ctypes.c_int),
+    "ve_octree_info": ([_P, _PTR(_U32), _PTR(_U32), _PTR(_U32)], ctypes.c_int),
+    "ve_octree_words": ([_P, _PTR(_P), _PTR(_U64)], ctypes.c_int),
+    "ve_terrain_build": ([_U32, _U32, _U64, _U32, _PTR(_P), _PTR(_U64)], ctypes.c_int),
+    "ve_words_data": ([_P, _PTR(_P), _PTR(_U64)], ctypes.c_int),
+    "ve_words_free": ([_P], ctypes.c_int),
+    "ve_terrain_voxels": ([_U32, _U32, _U64, _P, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_terrain_materials": ([_U64, _P], ctypes.c_int),
+    "ve_camera_ubo": ([_P, _P, _F, _F, _P], ctypes.c_int),
+    "ve_ctx_create": ([_PTR(RendererConfigC), _PTR(_P)], ctypes.c_int),
+    "ve_ctx_destroy": ([_P], ctypes.c_int),
+    "ve_ctx_stream": ([_P, _PTR(_P)], ctypes.c_int),
+    "ve_ctx_synchronize": ([_P], ctypes.c_int),
+    "ve_scene_upload": ([_P, _P, _U64, _U32, _U32, _PTR(_I32)], ctypes.c_int),
+    "ve_scene_release": ([_P, _I32], ctypes.c_int),
+    "ve_scene_apply_edits": ([_P, _I32, _P, _P, _U64, _U32], ctypes.c_int),
+    "ve_scene_download": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_scene_footprint": ([_P, _I32, _PTR(_U64)], ctypes.c_int),
+    "ve_set_materials": ([_P, _P, _U32], ctypes.c_int),
+    "ve_cache_reset": ([_P, _I32], ctypes.c_int),
+    "ve_cache_dump": ([_P, _I32, _P, _P, _P, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_render": ([_P, _PTR(ViewC), _PTR(FrameOutputsC)], ctypes.c_int),
+    "ve_render_batch": ([_P, _PTR(ViewC), _U32, _P], ctypes.c_int),
+    "ve_get_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libve.so (raises when it has not been built: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libve.so not found at {path}; build it with `python voxelengine3.0_b200/build.py` "
+                          "or __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != VE_OK:
+        raise VeError(rc, load_library().ve_last_error().decode(errors="replace"))
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+# ---------------------------------------------------------------------------
+# host scene layer
+# ---------------------------------------------------------------------------
+class OctreeCPU:
+    """Pointer sparse voxel octree with the reference's build API."""
+
+    def __init__(self, depth: int):
+        self._lib = load_library()
+        self.depth = int(depth)
+        h = _P()
+        _check(self._lib.ve_octree_cpu_create(self.depth, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ve_octree_cpu_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def insert(self, x: int, y: int, z: int, material: int) -> None:
+        _check(self._lib.ve_octree_cpu_insert(self._h, x, y, z, material))
+
+    def insert_many(self, xyzm: np.ndarray) -> None:
+        a = np.ascontiguousarray(xyzm, dtype=np.uint32).reshape(-1, 4)
+        _check(self._lib.ve_octree_cpu_insert_many(self._h, _ptr(a), a.shape[0]))
+
+    def remove(self, x: int, y: int, z: int) -> None:
+        _check(self._lib.ve_octree_cpu_remove(self._h, x, y, z))
+
+    def lookup(self, x: int, y: int, z: int) -> int:
+        m = ctypes.c_int64()
+        _check(self._lib.ve_octree_cpu_lookup(self._h, x, y, z, ctypes.byref(m)))
+        return m.value
+
+    def insert_box(self, mn: Sequence[int], mx: Sequence[int], material: int) -> None:
+        a = np.asarray(mn, np.uint32)
+        b = np.asarray(mx, np.uint32)
+        _check(self._lib.ve_octree_cpu_insert_box(self._h, _ptr(a), _ptr(b), material))
+
+    def insert_sphere(self, centre: Sequence[float], radius: float, material: int) -> None:
+        c = np.asarray(centre, np.float32)
+        _check(self._lib.ve_octree_cpu_insert_sphere(self._h, _ptr(c), float(radius), material))
+
+    def raycast(self, origin: Sequence[float], direction: Sequence[float], max_steps: int = 300):
+        o = np.asarray(origin, np.float32)
+        d = np.asarray(direction, np.float32)
+        hit = ctypes.c_int()
+        pos = np.zeros(3, np.uint32)
+        _check(self._lib.ve_octree_cpu_raycast(self._h, _ptr(o), _ptr(d), max_steps, ctypes.byref(hit), _ptr(pos)))
+        return (True, tuple(int(v) for v in pos)) if hit.value else (False, None)
+
+    # reference-style names
+    insertBox = insert_box
+    insertSphere = insert_sphere
+
+
+class Octree:
+    """Node array in the reference layout (Octree::data)."""
+
+    def __init__(self, depth: int):
+        self._lib = load_library()
+        self.depth = int(depth)
+        h = _P()
+        _check(self._lib.ve_octree_create(self.depth, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ve_octree_destroy(self._h)
+            self._h = None
+
+    def set(self, cpu: OctreeCPU) -> None:
+        _check(self._lib.ve_octree_set(self._h, cpu.handle))
+
+    def apply_edits(self, cpu: OctreeCPU) -> np.ndarray:
+        """Octree::applyEdits; returns the slots whose words changed."""
+        n = _U64()
+        _check(self._lib.ve_octree_apply_edits(self._h, cpu.handle, None, 0, ctypes.byref(n)))
+        p = _P()
+        _check(self._lib.ve_octree_last_changed(self._h, ctypes.byref(p), ctypes.byref(n)))
+        if n.value == 0:
+            return np.zeros(0, np.uint32)
+        return np.frombuffer((ctypes.c_uint32 * n.value).from_address(p.value), dtype=np.uint32).copy()
+
+    def find_gpu_slot(self, cpu: OctreeCPU, pos: Sequence[int]) -> int:
+        s = _U32()
+        _check(self._lib.ve_octree_find_gpu_slot(self._h, cpu.handle, pos[0], pos[1], pos[2], ctypes.byref(s)))
+        return s.value
+
+    def info(self):
+        size, cap, nv = _U32(), _U32(), _U32()
+        _check(self._lib.ve_octree_info(self._h, ctypes.byref(size), ctypes.byref(cap), ctypes.byref(nv)))
+        return size.value, cap.value, nv.value
+
+    @property
+    def size(self) -> int:
+        return self.info()[0]
+
+    @property
+    def capacity(self) -> int:
+        return self.info()[1]
+
+    @property
+    def num_voxels(self) -> int:
+        return self.info()[2]
+
+    def words(self) -> np.ndarray:
+        """Copy of all `capacity` words (Octree::data)."""
+        p = _P()
+        n = _U64()
+        _check(self._lib.ve_octree_words(self._h, ctypes.byref(p), ctypes.byref(n)))
+        if n.value == 0:
+            return np.zeros(0, np.uint32)
+        buf = (ctypes.c_uint32 * n.value).from_address(p.value)
+        return np.frombuffer(buf, dtype=np.uint32).copy()
+
+    findGpuSlot = find_gpu_slot
+    applyEdits = apply_edits
+
+
+def terrain_words(depth: int, variant: int = 0, seed: int = 1, threads: int = 0):
+    """Bulk-built node words of a seeded terrain scene; returns (words, n_voxels)."""
+    lib = load_library()
+    h = _P()
+    nv = _U64()
+    _check(lib.ve_terrain_build(depth, variant, seed, threads, ctypes.byref(h), ctypes.byref(nv)))
+    try:
+        p = _P()
+        n = _U64()
+        _check(lib.ve_words_data(h, ctypes.byref(p), ctypes.byref(n)))
+        buf = (ctypes.c_uint32 * n.value).from_address(p.value)
+        words = np.frombuffer(buf, dtype=np.uint32).copy()
+    finally:
+        lib.ve_words_free(h)
+    return words, nv.value
+
+
+def terrain_voxels(depth: int, variant: int = 0, seed: int = 1) -> np.ndarray:
+    lib = load_library()
+    n = _U64()
+    _check(lib.ve_terrain_voxels(depth, variant, seed, None, 0, ctypes.byref(n)))
+    out = np.zeros((n.value, 4), np.uint32)
+    _check(lib.ve_terrain_voxels(depth, variant, seed, _ptr(out), n.value, ctypes.byref(n)))
+    return out
+
+
+def terrain_materials(seed: int = 1) -> np.ndarray:
+    """128 std140 Material entries (64 B each) as a (128, 16) float32 view."""
+    out = np.zeros((128, 16), np.float32)
+    _check(load_library().ve_terrain_materials(seed, _ptr(out)))
+    return out
+
+
+def camera_ubo(position: Sequence[float], direction: Sequence[float], fov_deg: float, aspect: float) -> np.ndarray:
+    p = np.asarray(position, np.float32)
+    d = np.asarray(direction, np.float32)
+    out = np.zeros(16, np.float32)
+    _check(load_library().ve_camera_ubo(_ptr(p), _ptr(d), float(fov_deg), float(aspect), _ptr(out)))
+    return out
+
+
+def look_at(eye: Sequence[float], target: Sequence[float]) -> np.ndarray:
+    """Unit view direction from eye toward target (float32, normalised in float64)."""
+    d = np.asarray(target, np.float64) - np.asarray(eye, np.float64)
+    return (d / np.linalg.norm(d)).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# frame configuration
+# ---------------------------------------------------------------------------
+SUN_DIR = tuple(float(v) for v in (np.array([0.3, 1.0, 0.2]) / np.linalg.norm([0.3, 1.0, 0.2])).astype(np.float32))
+
+
+@dataclasses.dataclass
+class FrameConfig:
+    """core::FrameConfig subset read by the plain method + benchmark lighting."""
+    width: int = 256
+    height: int = 256
+    spp: int = 1
+    bounces: int = 1
+    primary_controlchecks: int = 70
+    bounce_controlchecks: int = 100
+    reconstruction_radius: int = 10
+    render_type: int = RENDER_DEFAULT
+    frame_index: int = 0
+    sun_dir: Sequence[float] = SUN_DIR
+    sun_intensity: float = math.pi
+    sky: Sequence[float] = (0.4, 0.4, 0.4)
+    decay: float = 0.95
+    variance_norm: float = 10000.0
+    flags: int = 0
+
+    def to_c(self) -> FrameConfigC:
+        c = FrameConfigC()
+        for f in ("width", "height", "spp", "bounces", "primary_controlchecks", "bounce_controlchecks",
+                  "reconstruction_radius", "render_type", "frame_index", "flags"):
+            setattr(c, f, int(getattr(self, f)))
+        for i in range(3):
+            c.sun_dir[i] = float(self.sun_dir[i])
+            c.sky[i] = float(self.sky[i])
+        c.sun_intensity = float(self.sun_intensity)
+        c.decay = float(self.decay)
+        c.variance_norm = float(self.variance_norm)
+        return c
+
+
+OUTPUT_KINDS = ("gbuffer", "voxel_id", "hit_node", "rgb", "mapped", "path_rgb")
+
+
+def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
+    npx = fc.width * fc.height
+    arrays: Dict[str, np.ndarray] = {}
+    for k in want:
+        if k == "gbuffer":
+            arrays[k] = np.zeros((fc.height, fc.width, 4), np.uint32)
+        elif k in ("voxel_id", "hit_node"):
+            arrays[k] = np.zeros((fc.height, fc.width), np.uint32)
+        elif k in ("rgb", "mapped"):
+            arrays[k] = np.zeros((fc.height, fc.width, 3), np.float32)
+        elif k == "path_rgb":
+            arrays[k] = np.zeros((npx * fc.spp, 3), np.float32)
+        else:
+            raise ValueError(f"unknown output {k!r}")
+    o = FrameOutputsC()
+    for k, a in arrays.items():
+        setattr(o, k, a.ctypes.data)
+    return o, arrays
+
+
+class Renderer:
+    """The device renderer (one CUDA context stream, owned device memory)."""
+
+    def __init__(self, device: int = 0, hash_log2: int = 22, hash_probes: int = 64):
+        self._lib = load_library()
+        cfg = RendererConfigC(device, hash_log2, hash_probes, 0)
+        h = _P()
+        _check(self._lib.ve_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.hash_log2 = hash_log2
+        self.scene: Optional[int] = None
+        self.camera: Optional[np.ndarray] = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ve_ctx_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        s = _P()
+        _check(self._lib.ve_ctx_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        _check(self._lib.ve_ctx_synchronize(self._h))
+
+    def upload_scene(self, words: np.ndarray, depth: int, keep_normals: bool = False) -> int:
+        w = np.ascontiguousarray(words, np.uint32)
+        sid = _I32()
+        _check(self._lib.ve_scene_upload(self._h, _ptr(w), w.size, depth, SCENE_KEEP_NORMALS if keep_normals else 0,
+                                         ctypes.byref(sid)))
+        return sid.value
+
+    def release_scene(self, scene_id: int) -> None:
+        _check(self._lib.ve_scene_release(self._h, scene_id))
+
+    def apply_edits(self, scene_id: int, slots: np.ndarray, words: np.ndarray, keep_normals: bool = False) -> None:
+        s = np.ascontiguousarray(slots, np.uint32)
+        w = np.ascontiguousarray(words, np.uint32)
+        _check(self._lib.ve_scene_apply_edits(self._h, scene_id, _ptr(s), _ptr(w), s.size,
+                                              SCENE_KEEP_NORMALS if keep_normals else 0))
+
+    def download_scene(self, scene_id: int) -> np.ndarray:
+        n = _U64()
+        _check(self._lib.ve_scene_download(self._h, scene_id, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.uint32)
+        _check(self._lib.ve_scene_download(self._h, scene_id, _ptr(out), n.value, ctypes.byref(n)))
+        return out
+
+    def scene_footprint(self, scene_id: int) -> int:
+        b = _U64()
+        _check(self._lib.ve_scene_footprint(self._h, scene_id, ctypes.byref(b)))
+        return b.value
+
+    def set_materials(self, materials: np.ndarray) -> None:
+        m = np.ascontiguousarray(materials, np.float32).reshape(-1, 16)
+        _check(self._lib.ve_set_materials(self._h, _ptr(m), m.shape[0]))
+
+    def cache_reset(self, scene_id: int) -> None:
+        _check(self._lib.ve_cache_reset(self._h, scene_id))
+
+    def cache_dump(self, scene_id: int):
+        n = _U64()
+        _check(self._lib.ve_cache_dump(self._h, scene_id, None, None, None, 0, ctypes.byref(n)))
+        vids = np.zeros(n.value, np.uint32)
+        counts = np.zeros(n.value, np.uint32)
+        vals = np.zeros((n.value, 5), np.float32)
+        _check(self._lib.ve_cache_dump(self._h, scene_id, _ptr(vids), _ptr(counts), _ptr(vals), n.value,
+                                       ctypes.byref(n)))
+        return vids, counts, vals
+
+    @staticmethod
+    def make_view(scene_id: int, camera: np.ndarray, fc: FrameConfig) -> ViewC:
+        v = ViewC()
+        v.scene_id = scene_id
+        cam = np.asarray(camera, np.float32).reshape(16)
+        for i in range(16):
+            v.camera[i] = float(cam[i])
+        v.frame = fc.to_c()
+        return v
+
+    def render(self, scene_id: int, camera: np.ndarray, fc: FrameConfig,
+               outputs: Iterable[str] = ("voxel_id", "rgb")) -> Dict[str, np.ndarray]:
+        """One frame of one view; returns the requested host outputs."""
+        view = self.make_view(scene_id, camera, fc)
+        want = list(outputs)
+        o, arrays = _alloc_outputs(fc, want)
+        _check(self._lib.ve_render(self._h, ctypes.byref(view), ctypes.byref(o) if want else None))
+        return arrays
+
+    def render_batch(self, views: Sequence[tuple], outputs: Iterable[str] = ("voxel_id", "rgb")):
+        """views: sequence of (scene_id, camera, FrameConfig)."""
+        arr = (ViewC * len(views))()
+        want = list(outputs)
+        outs = (FrameOutputsC * len(views))()
+        results: List[Dict[str, np.ndarray]] = []
+        for i, (sid, cam, fc) in enumerate(views):
+            arr[i] = self.make_view(sid, cam, fc)
+            o, arrays = _alloc_outputs(fc, want)
+            outs[i] = o
+            results.append(arrays)
+        _check(self._lib.ve_render_batch(self._h, arr, len(views), outs if want else None))
+        return results
+
+    def stats(self) -> Dict[str, float]:
+        s = FrameStatsC()
+        _check(self._lib.ve_get_stats(self._h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in FrameStatsC._fields_}
+
+    # Renderer::run (reference-shaped): renders the bound scene from the bound camera
+    def set_scene(self, scene_id: int) -> None:
+        self.scene = scene_id
+
+    def set_camera(self, ubo: np.ndarray) -> None:
+        self.camera = np.asarray(ubo, np.float32).reshape(16)
+
+    def run(self, fc: FrameConfig, outputs: Iterable[str] = ("rgb",)) -> Dict[str, np.ndarray]:
+        if self.scene is None or self.camera is None:
+            raise VeError(VE_ERR_STATE, "run: bind a scene (set_scene) and a camera (set_camera) first")
+        return self.render(self.scene, self.camera, fc, outputs)
+
+
+__all__ = [
+    "OctreeCPU", "Octree", "Renderer", "FrameConfig", "VeError", "camera_ubo", "look_at", "terrain_words",
+    "terrain_voxels", "terrain_materials", "load_library", "SUN_DIR",
+]

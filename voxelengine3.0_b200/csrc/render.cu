@@ -1,0 +1,1325 @@
+// render.cu — B200 wavefront renderer for the voxel ray pipeline and its
+// C ABI (include/ve.h).
+//
+// Frame structure (the four passes of Renderer::runWavefrontFrame,
+// reference src/renderer/renderer.cpp:282-649, in per-pixel form, with every
+// host readback removed):
+//   decay      radiance-cache temporal decay (once per scene per frame)
+//   primary    one thread per pixel: camera ray + counted DDA -> GBuffer;
+//              spp path states per hit pixel, appended to the live queue
+//   shade/trace  bounce loop; shade consumes the live queue, adds the
+//              pending sun-shadow result, shades the hit, emits the
+//              extension ray and the sun shadow ray into one ray queue
+//              (warp-ballot compaction) and deposits finished paths into the
+//              radiance cache with warp-aggregated atomics (AccumPass);
+//              trace runs the DDA for every queued ray
+//   resolve    AvgPass + visualisation modes + ACES tonemap per pixel
+// All queue sizes live in device counters: kernels size their loops from
+// them, so a frame needs no host synchronisation.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ve.h"
+#include "raycast.cuh"
+#include "ve_device.cuh"
+
+namespace ve {
+using namespace dev;
+
+// ---------------------------------------------------------------------------
+// device data
+// ---------------------------------------------------------------------------
+struct alignas(16) CacheEntry {
+    uint32_t key;    // vid (voxelKey + 1); 0 = empty
+    uint32_t count;  // exact number of deposits
+    float l2;        // sum of luma^2 (decayed)
+    uint32_t pad;
+    float4 rgbw;     // sums of r, g, b and the decayed weight
+};
+static_assert(sizeof(CacheEntry) == 32, "cache entry is one 32-byte sector");
+
+struct DevScene {
+    const uint32_t* nodes;
+    uint64_t n_words;
+    CacheEntry* cache;
+    uint32_t depth;
+    uint32_t cache_log2;
+    uint32_t probes;
+    uint32_t pad;
+};
+
+struct DevMaterial {
+    float4 albedo_rough;  // albedo rgb, roughness
+    float4 params;        // metallic, specular, emissive (0/1), emissive intensity
+};
+
+struct DevView {
+    float cam[16];
+    uint32_t scene, W, H, spp;
+    uint32_t bounces, cc_primary, cc_bounce, recon_radius;
+    uint32_t render_type, frame_index, flags, tiles_x;
+    float sun[3], sun_intensity;
+    float sky[3], decay;
+    float variance_norm;
+    uint32_t pix_base;
+    uint32_t tile_base;
+    uint32_t pad0;
+    unsigned long long path_base;
+};
+
+enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
+enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_TOTAL = 64 };
+enum : uint32_t {
+    ST_RAYS_PRIMARY = 0,
+    ST_RAYS_BOUNCE,
+    ST_RAYS_SHADOW,
+    ST_FETCH,
+    ST_PATHS,
+    ST_DEPOSITS,
+    ST_DROPPED,
+    ST_STEPS,
+    ST_TOTAL = 16
+};
+enum : uint32_t { F_PENDING = 1u, F_TERM = 2u };
+
+struct FrameArgs {
+    const DevView* views;
+    uint32_t n_views;
+    uint32_t total_tiles;
+    const DevScene* scenes;
+    const DevMaterial* mats;
+    // path state (structure of arrays, index = global path id)
+    float4* p_ray_o;     // next ray origin (shading point)
+    float4* p_ray_d;     // direction of the ray that produced the current hit / next extension ray
+    float4* p_tp;        // throughput
+    float4* p_direct;    // direct radiance (sun at bounce 0, bounce-0 emission)
+    float4* p_indirect;  // indirect radiance
+    float4* p_pend;      // pending sun contribution, w = channel (0 direct, 1 indirect)
+    uint4* p_hit;        // {status, node slot, x | y<<16, z | material<<16}
+    uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
+    uint8_t* p_vis;      // sun visibility from the shadow trace
+    uint32_t* live[2];
+    uint32_t* rayq;
+    uint32_t* counters;
+    unsigned long long* stats;
+    uint4* gbuf;
+    uint32_t* out_vid;
+    uint32_t* out_node;
+    float* out_rgb;
+    float* out_mapped;
+    float* path_rgb;
+};
+
+// ---------------------------------------------------------------------------
+// warp helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated queue append: one atomicAdd per warp; returns this lane's
+// slot.  Must be called by all 32 lanes.
+__device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* counter, uint32_t per_lane = 1u) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (m == 0u) return 0u;
+    const uint32_t lane = lane_id();
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(counter, uint32_t(__popc(m)) * per_lane);
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + uint32_t(__popc(m & ((1u << lane) - 1u))) * per_lane;
+}
+
+__device__ __forceinline__ void warp_add_stat(unsigned long long* stat, uint32_t v) {
+    uint32_t s = v;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane_id() == 0 && s) atomicAdd(stat, (unsigned long long)s);
+}
+
+// Radiance cache: power-of-two table, Fibonacci hash of the vid, linear
+// probing, claim by CAS on the key.
+__device__ __forceinline__ uint32_t cache_home(uint32_t vid, uint32_t log2n) {
+    return (vid * 0x9E3779B1u) >> (32u - log2n);
+}
+__device__ __forceinline__ int cache_claim(CacheEntry* c, uint32_t log2n, uint32_t probes, uint32_t vid) {
+    const uint32_t mask = (1u << log2n) - 1u;
+    const uint32_t h = cache_home(vid, log2n);
+    for (uint32_t i = 0; i < probes; i++) {
+        const uint32_t s = (h + i) & mask;
+        uint32_t k = *((volatile uint32_t*)&c[s].key);
+        if (k == vid) return int(s);
+        if (k == 0u) {
+            k = atomicCAS(&c[s].key, 0u, vid);
+            if (k == 0u || k == vid) return int(s);
+        }
+    }
+    return -1;
+}
+__device__ __forceinline__ int cache_find(const CacheEntry* c, uint32_t log2n, uint32_t probes, uint32_t vid) {
+    const uint32_t mask = (1u << log2n) - 1u;
+    const uint32_t h = cache_home(vid, log2n);
+    for (uint32_t i = 0; i < probes; i++) {
+        const uint32_t s = (h + i) & mask;
+        const uint32_t k = c[s].key;
+        if (k == vid) return int(s);
+        if (k == 0u) return -1;
+    }
+    return -1;
+}
+
+struct DepSlot {
+    float r, g, b, l2;
+};
+
+// AccumPass deposit, warp-aggregated: lanes depositing into the same
+// (scene, vid) are merged in shared memory and one leader lane issues the
+// atomics (count, luma^2, and one vector add of {r, g, b, weight}).
+__device__ __forceinline__ void warp_deposit(bool active, uint32_t scene, uint32_t vid, float r, float g, float b,
+                                             float l2, DepSlot* sh, const DevScene* scenes,
+                                             unsigned long long* stats) {
+    const unsigned am = __ballot_sync(0xffffffffu, active);
+    if (am == 0u) return;
+    const uint32_t lane = lane_id();
+    if (active) sh[lane] = DepSlot{r, g, b, l2};
+    __syncwarp();
+    if (active) {
+        const unsigned long long key = (static_cast<unsigned long long>(scene) << 32) | vid;
+        const unsigned peers = __match_any_sync(am, key);
+        if (int(lane) == __ffs(peers) - 1) {
+            float sr = 0.0f, sg = 0.0f, sb = 0.0f, sl = 0.0f;
+            for (unsigned m = peers; m; m &= m - 1u) {
+                const int j = __ffs(m) - 1;
+                sr += sh[j].r;
+                sg += sh[j].g;
+                sb += sh[j].b;
+                sl += sh[j].l2;
+            }
+            const uint32_t n = uint32_t(__popc(peers));
+            const DevScene& S = scenes[scene];
+            const int s = cache_claim(S.cache, S.cache_log2, S.probes, vid);
+            if (s >= 0) {
+                CacheEntry* e = S.cache + s;
+                atomicAdd(&e->count, n);
+                atomicAdd(&e->l2, sl);
+                atomicAdd(&e->rgbw, make_float4(sr, sg, sb, float(n)));
+                atomicAdd(&stats[ST_DEPOSITS], (unsigned long long)n);
+            } else {
+                atomicAdd(&stats[ST_DROPPED], (unsigned long long)n);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ uint32_t find_view(const DevView* views, uint32_t n, uint32_t tile) {
+    uint32_t lo = 0, hi = n;  // last view with tile_base <= tile
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (views[mid].tile_base <= tile) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// 16x16 pixel tile per 256-thread block; each warp covers an 8x4 sub-tile.
+__device__ __forceinline__ void tile_pixel(uint32_t local_tile, uint32_t tiles_x, uint32_t* px, uint32_t* py) {
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
+    *px = (local_tile % tiles_x) * 16u + (w & 1u) * 8u + (l & 7u);
+    *py = (local_tile / tiles_x) * 16u + (w >> 1) * 4u + (l >> 3);
+}
+
+__device__ __forceinline__ f3 ld3(const float4& v) { return mk(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 st3(f3 v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Radiance-cache temporal decay: sums and weight *= decay (counts exact).
+__global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, float decay) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (cache[i].key == 0u) continue;
+        float4 v = cache[i].rgbw;
+        v.x = v.x * decay; v.y = v.y * decay; v.z = v.z * decay; v.w = v.w * decay;
+        cache[i].rgbw = v;
+        cache[i].l2 = cache[i].l2 * decay;
+    }
+}
+
+// RayPass primary (generate_primary.comp:38-85) + path seeding (emit.comp:39-101)
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
+    const uint32_t tile = blockIdx.x;
+    const uint32_t vi = find_view(a.views, a.n_views, tile);
+    const DevView& v = a.views[vi];
+    uint32_t px, py;
+    tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
+    const bool inside = px < v.W && py < v.H;
+    const DevScene S = a.scenes[v.scene];
+    Hit h;
+    h.status = kEscaped;
+    h.checks = 0;
+    f3 dir = mk(0.0f, 0.0f, 0.0f);
+    RayCount rc;
+    uint32_t vid = 0;
+    if (inside) {
+        const float ndx = (float(px) + 0.5f) / float(v.W) * 2.0f - 1.0f;
+        const float ndy = (float(py) + 0.5f) / float(v.H) * 2.0f - 1.0f;
+        const f3 plane = mk(v.cam[4], v.cam[5], v.cam[6]);
+        const f3 right = mk(v.cam[8], v.cam[9], v.cam[10]);
+        const f3 up = mk(v.cam[12], v.cam[13], v.cam[14]);
+        dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
+        h = raycast<COUNT>(S.nodes, S.n_words, S.depth, mk(v.cam[0], v.cam[1], v.cam[2]), dir, v.cc_primary, rc);
+        if (h.status == kHit) vid = voxel_key(h.x, h.y, h.z) + 1u;
+        const uint32_t pix = py * v.W + px;
+        a.gbuf[v.pix_base + pix] = make_uint4(h.checks, h.status == kHit ? h.material : 0u,
+                                              h.status == kHit ? h.id : 0u, vid);
+    }
+    const bool spawn = inside && vid != 0u;
+    const uint32_t q = warp_append(spawn, &a.counters[CNT_LIVE + 0], v.spp);
+    if (spawn) {
+        const uint32_t pix = py * v.W + px;
+        for (uint32_t s = 0; s < v.spp; s++) {
+            const unsigned long long p = v.path_base + (unsigned long long)pix * v.spp + s;
+            const uint32_t list_idx = pix * v.spp + s;
+            // emit.comp:171-174
+            const uint32_t sample_idx = v.frame_index + pix * 2654435761u + list_idx * 1442695040u;
+            const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+            a.p_ray_d[p] = st3(dir);
+            a.p_tp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.p_hit[p] = make_uint4(kHit, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+            a.p_meta[p] = make_uint4(vid, rng, vi, pix);
+            a.live[0][q + s] = uint32_t(p);
+        }
+    }
+    warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside ? 1u : 0u);
+    warp_add_stat(&a.stats[ST_PATHS], spawn ? v.spp : 0u);
+    if (COUNT) {
+        warp_add_stat(&a.stats[ST_FETCH], rc.fetch);
+        warp_add_stat(&a.stats[ST_STEPS], rc.steps);
+    }
+}
+
+// trace.comp:25-70 for extension rays; shadow rays test escape toward the sun.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
+    const uint32_t n = a.counters[CNT_RAY + pass];
+    uint32_t fetch = 0, steps = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = a.rayq[i];
+        const uint32_t p = e & 0x7FFFFFFFu;
+        const bool shadow = (e >> 31) != 0u;
+        const uint4 meta = a.p_meta[p];
+        const DevView& v = a.views[meta.z & 0xFFFFu];
+        const DevScene S = a.scenes[v.scene];
+        const f3 o = ld3(a.p_ray_o[p]);
+        const f3 d = shadow ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
+        RayCount rc;
+        const Hit h = raycast<COUNT>(S.nodes, S.n_words, S.depth, o, d, v.cc_bounce, rc);
+        if (shadow) {
+            a.p_vis[p] = h.status == kEscaped ? 1u : 0u;
+        } else {
+            a.p_hit[p] = make_uint4(h.status, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+        }
+        if (COUNT) {
+            fetch += rc.fetch;
+            steps += rc.steps;
+        }
+    }
+    if (COUNT) {
+        atomicAdd(&a.stats[ST_FETCH], (unsigned long long)fetch);
+        atomicAdd(&a.stats[ST_STEPS], (unsigned long long)steps);
+    }
+}
+
+// shade.comp:543-575, 838-908 (bounce/shade loop) with the sun next-event
+// estimate in the place of the dormant emissive NEE, and the AccumPass deposit.
+__global__ void __launch_bounds__(256) k_shade(FrameArgs a, uint32_t pass) {
+    __shared__ DepSlot dep[256];
+    const uint32_t n = a.counters[CNT_LIVE + pass];
+    const uint32_t* live_in = a.live[pass & 1u];
+    uint32_t* live_out = a.live[(pass + 1u) & 1u];
+    uint32_t* live_cnt = &a.counters[CNT_LIVE + pass + 1u];
+    uint32_t* ray_cnt = &a.counters[CNT_RAY + pass];
+    uint32_t n_ext = 0, n_sh = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t p = valid ? live_in[i] : 0u;
+        bool do_dep = false, app_live = false, app_ext = false, app_sh = false;
+        float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
+        uint32_t dvid = 0, dscene = 0;
+        if (valid) {
+            uint4 meta = a.p_meta[p];
+            const uint32_t vi = meta.z & 0xFFFFu;
+            uint32_t b = (meta.z >> 16) & 0xFFu;
+            const uint32_t flags = meta.z >> 24;
+            const DevView& v = a.views[vi];
+            f3 tp = ld3(a.p_tp[p]);
+            f3 direct = ld3(a.p_direct[p]);
+            f3 indirect = ld3(a.p_indirect[p]);
+            f3 dir = ld3(a.p_ray_d[p]);
+            if (flags & F_PENDING) {
+                if (a.p_vis[p]) {
+                    const float4 pe = a.p_pend[p];
+                    if (pe.w == 0.0f) direct = add(direct, ld3(pe));
+                    else indirect = add(indirect, ld3(pe));
+                }
+            }
+            if (flags & F_TERM) {
+                do_dep = true;
+            } else {
+                const uint4 hit = a.p_hit[p];
+                if (hit.x != kHit) {  // miss (shade.comp:558-564): constant sky
+                    indirect = add(indirect, mul(mk(v.sky[0], v.sky[1], v.sky[2]), tp));
+                    do_dep = true;
+                } else {
+                    const DevScene S = a.scenes[v.scene];
+                    const uint32_t mi = hit.w >> 16;
+                    const DevMaterial m = a.mats[mi & 127u];
+                    const f3 albedo = mk(m.albedo_rough.x, m.albedo_rough.y, m.albedo_rough.z);
+                    const float roughness = m.albedo_rough.w, metallic = m.params.x, spec = m.params.y;
+                    const bool emissive = m.params.z != 0.0f;
+                    const f3 N = shading_normal(fetch_node(S.nodes, S.n_words, hit.y), dir);
+                    if (emissive) {  // shade.comp:576-583
+                        const float k = m.params.w;
+                        f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
+                        em = mk(gmin(em.x, 20.0f), gmin(em.y, 20.0f), gmin(em.z, 20.0f));
+                        if (b == 0u) direct = add(direct, em); else indirect = add(indirect, em);
+                    }
+                    const f3 hp = mk(float(hit.z & 0xFFFFu), float(hit.z >> 16), float(hit.w & 0xFFFFu));
+                    const f3 sp = add(add(hp, mk(0.5f, 0.5f, 0.5f)), N);
+                    const f3 sun = mk(v.sun[0], v.sun[1], v.sun[2]);
+                    uint32_t nf = 0;
+                    if (!emissive && b < 2u && dot(N, sun) > 0.0f) {
+                        const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
+                        f3 c = muls(brdf, v.sun_intensity);
+                        c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
+                        a.p_pend[p] = st3(mul(tp, c), b == 0u ? 0.0f : 1.0f);
+                        nf |= F_PENDING;
+                        app_sh = true;
+                    }
+                    bool term = false;
+                    uint32_t rng = meta.y;
+                    if (b + 1u >= v.bounces + 1u) {
+                        term = true;
+                    } else {
+                        const bool use_ggx = metallic * (1.0f - roughness) > 0.5f;
+                        f3 sdir, bt;
+                        if (use_ggx) {
+                            const f3 V = mk(-dir.x, -dir.y, -dir.z);
+                            const f3 H = sample_ggx_vndf(N, V, roughness, rng);
+                            sdir = reflect(dir, H);
+                            if (dot(sdir, N) <= 0.0f) {
+                                sdir = cosine_direction(N, rng);
+                                bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
+                            } else {
+                                const f3 F0 = mk(0.04f * (1.0f - metallic) + albedo.x * metallic,
+                                                 0.04f * (1.0f - metallic) + albedo.y * metallic,
+                                                 0.04f * (1.0f - metallic) + albedo.z * metallic);
+                                bt = ggx_throughput(N, V, sdir, H, roughness, F0);
+                            }
+                        } else {
+                            sdir = cosine_direction(N, rng);
+                            bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
+                        }
+                        f3 ntp = mul(tp, bt);
+                        if (b + 1u >= 2u) {  // Russian roulette, RR_START_BOUNCE = 2
+                            const float pr = gclamp(gmax(ntp.x, gmax(ntp.y, ntp.z)), 0.05f, 0.95f);
+                            const float xi = rand01(rng);
+                            if (xi > pr) term = true;
+                            else ntp = divs(ntp, pr);
+                        }
+                        if (!term) {
+                            tp = ntp;
+                            dir = sdir;
+                            b++;
+                            app_ext = true;
+                        }
+                    }
+                    if (term) {
+                        if (nf & F_PENDING) nf |= F_TERM;
+                        else do_dep = true;
+                    }
+                    if (app_ext || (nf & F_PENDING)) {
+                        app_live = true;
+                        a.p_ray_o[p] = st3(sp);
+                        a.p_ray_d[p] = st3(dir);
+                        a.p_tp[p] = st3(tp);
+                        a.p_direct[p] = st3(direct);
+                        a.p_indirect[p] = st3(indirect);
+                        meta.y = rng;
+                        meta.z = vi | (b << 16) | (nf << 24);
+                        a.p_meta[p] = meta;
+                    }
+                }
+            }
+            if (do_dep) {
+                // packRgbL2 clamp (shade.comp:154-160), direct + indirect
+                float dv[3] = {direct.x, direct.y, direct.z};
+                const float iv[3] = {indirect.x, indirect.y, indirect.z};
+                float outv[3];
+                for (int c = 0; c < 3; c++) {
+                    float x = dv[c], y = iv[c];
+                    if (!(x == x)) x = 0.0f;
+                    if (!(y == y)) y = 0.0f;
+                    outv[c] = gclamp(x, 0.0f, 1024.0f) + gclamp(y, 0.0f, 1024.0f);
+                }
+                dr = outv[0]; dg = outv[1]; db = outv[2];
+                const float Lf = ((dr + dg) + db) / 3.0f;
+                dl2 = Lf * Lf;
+                dvid = meta.x;
+                dscene = v.scene;
+                if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
+                    a.path_rgb[3ull * p + 0] = dr;
+                    a.path_rgb[3ull * p + 1] = dg;
+                    a.path_rgb[3ull * p + 2] = db;
+                }
+            }
+        }
+        const uint32_t sl = warp_append(app_live, live_cnt);
+        if (app_live) live_out[sl] = p;
+        const uint32_t se = warp_append(app_ext, ray_cnt);
+        if (app_ext) a.rayq[se] = p;
+        const uint32_t ss = warp_append(app_sh, ray_cnt);
+        if (app_sh) a.rayq[ss] = p | 0x80000000u;
+        n_ext += app_ext ? 1u : 0u;
+        n_sh += app_sh ? 1u : 0u;
+        warp_deposit(do_dep, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
+    }
+    warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
+    warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+}
+
+struct Avg {
+    f3 rgb;
+    uint32_t count;
+    float var;
+};
+// lookupVoxelAvg (resolve.comp:109-148) over the FP32 cache
+__device__ __forceinline__ Avg lookup_avg(const DevScene& S, uint32_t vid) {
+    Avg r{mk(0.0f, 0.0f, 0.0f), 0u, 0.0f};
+    if (vid == 0u) return r;
+    const int s = cache_find(S.cache, S.cache_log2, S.probes, vid);
+    if (s < 0) return r;
+    const CacheEntry& e = S.cache[s];
+    r.count = e.count;
+    const float4 v = e.rgbw;
+    if (r.count == 0u || !(v.w > 0.0f)) return r;
+    const float inv = 1.0f / v.w;
+    r.rgb = mk(v.x * inv, v.y * inv, v.z * inv);
+    const float meanL = ((v.x + v.y) + v.z) * inv / 3.0f;
+    r.var = gmax(e.l2 * inv - meanL * meanL, 0.0f);
+    return r;
+}
+
+__device__ __forceinline__ float aces(float x) {  // final.frag:11-18
+    const float v = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+    return gclamp(v, 0.0f, 1.0f);
+}
+
+// AvgPass (resolve.comp:362-382 with resolveDefault :224-261,
+// reconstructTimeout :193-219 and the visualisation modes) + tonemap.
+__global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
+    const uint32_t tile = blockIdx.x;
+    const uint32_t vi = find_view(a.views, a.n_views, tile);
+    const DevView& v = a.views[vi];
+    uint32_t px, py;
+    tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
+    if (px >= v.W || py >= v.H) return;
+    const DevScene S = a.scenes[v.scene];
+    const uint32_t W = v.W, H = v.H;
+    const uint32_t gp = v.pix_base + py * W + px;
+    const uint4 g = a.gbuf[gp];
+    const uint32_t checks = g.x, mat = g.y, node = g.z, vid = g.w;
+    const f3 sky = mk(v.sky[0], v.sky[1], v.sky[2]);
+    f3 col = mk(0.0f, 0.0f, 0.0f);
+    auto reconstruct = [&]() {
+        f3 sum = mk(0.0f, 0.0f, 0.0f);
+        float ws = 0.0f;
+        const int R = int(v.recon_radius);
+        for (int dy = -R; dy <= R; dy++)
+            for (int dx = -R; dx <= R; dx++) {
+                if (dx == 0 && dy == 0) continue;
+                const int qx = int(px) + dx, qy = int(py) + dy;
+                if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
+                const uint4 nd = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)];
+                if (nd.w == 0u || nd.x >= v.cc_primary) continue;
+                const Avg na = lookup_avg(S, nd.w);
+                if (na.count == 0u) continue;
+                const float dist = float(dx * dx + dy * dy);
+                const float w = float(na.count < 32u ? na.count : 32u) / (1.0f + dist * 0.15f);
+                sum = add(sum, muls(na.rgb, w));
+                ws += w;
+            }
+        return ws > 0.0001f ? divs(sum, ws) : sky;
+    };
+    auto miss = [&]() { return checks >= v.cc_primary ? reconstruct() : sky; };
+    switch (v.render_type) {
+        case VE_RENDER_STRUCTURE: {
+            const float s = float(checks) / 65.0f;
+            col = mk(s, s, s);
+            break;
+        }
+        case VE_RENDER_ALBEDO:
+            if (vid == 0u) col = miss();
+            else if (mat != 0u && mat < 127u) {
+                const float4 m = a.mats[mat].albedo_rough;
+                col = mk(m.x, m.y, m.z);
+            }
+            break;
+        case VE_RENDER_NORMAL:
+            if (vid == 0u) col = miss();
+            else {
+                const uint32_t w = fetch_node(S.nodes, S.n_words, node);
+                if (w >> 31) {
+                    const f3 nn = shading_normal(w, mk(0.0f, 0.0f, 1.0f));
+                    col = mk(nn.x * 0.5f + 0.5f, nn.y * 0.5f + 0.5f, nn.z * 0.5f + 0.5f);
+                }
+            }
+            break;
+        case VE_RENDER_VOXELID:
+            if (vid == 0u) col = miss();
+            else {
+                const uint32_t hid = vid - 1u;
+                col = mk(float((hid + 1u) % 255u) / 255.0f, float(((hid + 1u) / 255u) % 255u) / 255.0f,
+                         float(((hid + 1u) / (255u * 255u)) % 255u) / 255.0f);
+            }
+            break;
+        case VE_RENDER_VARIANCE:
+            if (vid == 0u) col = miss();
+            else {
+                const Avg c = lookup_avg(S, vid);
+                const float var = c.count >= 2u ? c.var : 0.0f;
+                const float sc = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
+                col = mk(sc, sc, sc);
+            }
+            break;
+        default: {
+            if (vid == 0u) {
+                col = miss();
+                break;
+            }
+            const Avg c = lookup_avg(S, vid);
+            if (c.count >= 128u && c.var < 0.02f) {
+                col = c.rgb;
+                break;
+            }
+            f3 sum = muls(c.rgb, float(c.count));
+            float ws = float(c.count);
+            const int dxs[4] = {1, -1, 0, 0}, dys[4] = {0, 0, 1, -1};
+            for (int k = 0; k < 4; k++) {
+                const int qx = int(px) + dxs[k], qy = int(py) + dys[k];
+                if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
+                const uint32_t nv = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)].w;
+                if (nv == 0u || nv == vid) continue;
+                const Avg na = lookup_avg(S, nv);
+                if (na.count == 0u) continue;
+                const f3 dd = sub(na.rgb, c.rgb);
+                const float dc = sqrtf(dot(dd, dd));
+                const float wc = expf(-dc * 6.0f);
+                const float wv = 1.0f / (1.0f + na.var * 32.0f);
+                const float w = wc * wv * float(na.count < 32u ? na.count : 32u);
+                sum = add(sum, muls(na.rgb, w));
+                ws += w;
+            }
+            if (ws > 0.0001f) col = divs(sum, ws);
+            break;
+        }
+    }
+    if (a.out_vid) a.out_vid[gp] = vid;
+    if (a.out_node) a.out_node[gp] = node;
+    if (a.out_rgb) {
+        a.out_rgb[3ull * gp + 0] = col.x;
+        a.out_rgb[3ull * gp + 1] = col.y;
+        a.out_rgb[3ull * gp + 2] = col.z;
+    }
+    if (a.out_mapped) {
+        a.out_mapped[3ull * gp + 0] = aces(col.x);
+        a.out_mapped[3ull * gp + 1] = aces(col.y);
+        a.out_mapped[3ull * gp + 2] = aces(col.z);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scene normals: 3x3x3 occupancy gradient of every leaf (normal.comp:73-95
+// over the full cube), written into the leaf words' normal field.
+// ---------------------------------------------------------------------------
+// frontier entry: slot (28 bits) | x << 28 | y << 39 | z << 50 (11 bits each)
+__device__ __forceinline__ unsigned long long pack_cell(uint32_t slot, uint32_t x, uint32_t y, uint32_t z) {
+    return (unsigned long long)slot | ((unsigned long long)x << 28) | ((unsigned long long)y << 39) |
+           ((unsigned long long)z << 50);
+}
+
+// Expands internal nodes of level k (cell size 2^(D-k)) into their internal
+// children (level k+1).
+__global__ void __launch_bounds__(256) k_expand(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                                uint32_t k, const unsigned long long* in, const uint32_t* in_cnt,
+                                                unsigned long long* out, uint32_t* out_cnt, uint32_t cap) {
+    const uint32_t n = min(*in_cnt, cap);
+    const uint32_t half = (1u << D) >> (k + 1u);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        unsigned long long e = 0;
+        uint32_t word = 0;
+        if (i < n) {
+            e = in[i];
+            word = fetch_node(nodes, n_words, uint32_t(e & 0xFFFFFFFull));
+        }
+        const uint32_t next = word >> 4;
+        const uint32_t x = uint32_t((e >> 28) & 2047u), y = uint32_t((e >> 39) & 2047u), z = uint32_t((e >> 50) & 2047u);
+        for (uint32_t c = 0; c < 8; c++) {
+            bool app = false;
+            if (i < n && (word & 1u)) app = (fetch_node(nodes, n_words, next + c) & 1u) != 0u;
+            const uint32_t slot = warp_append(app, out_cnt);
+            if (app && slot < cap)
+                out[slot] = pack_cell(next + c, x + ((c & 4u) ? half : 0u), y + ((c & 2u) ? half : 0u),
+                                      z + ((c & 1u) ? half : 0u));
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t occ_index(uint32_t x, uint32_t y, uint32_t z, uint32_t D) {
+    return (((uint64_t(z) << D) + y) << D) + x;
+}
+
+// phase 0: set occupancy bits of all leaves below level D-1 nodes
+// phase 1: compute and store the normal field of those leaves
+__global__ void __launch_bounds__(256) k_leaf_pass(uint32_t* nodes, uint64_t n_words, uint32_t D,
+                                                   const unsigned long long* in, const uint32_t* in_cnt,
+                                                   uint32_t* occ, int phase, uint32_t cap) {
+    const uint32_t n = min(*in_cnt, cap);
+    const int L = int(1u << D);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long e = in[i];
+        const uint32_t word = fetch_node(nodes, n_words, uint32_t(e & 0xFFFFFFFull));
+        if (!(word & 1u)) continue;
+        const uint32_t next = word >> 4;
+        const uint32_t x0 = uint32_t((e >> 28) & 2047u), y0 = uint32_t((e >> 39) & 2047u),
+                       z0 = uint32_t((e >> 50) & 2047u);
+        for (uint32_t c = 0; c < 8; c++) {
+            if (uint64_t(next) + c >= n_words) break;
+            const uint32_t lw = nodes[next + c];
+            if ((lw & 1u) || ((lw >> 1) & 0x7Fu) == 0u) continue;
+            const uint32_t x = x0 + ((c >> 2) & 1u), y = y0 + ((c >> 1) & 1u), z = z0 + (c & 1u);
+            if (phase == 0) {
+                const uint64_t bi = occ_index(x, y, z, D);
+                atomicOr(&occ[bi >> 5], 1u << (bi & 31u));
+            } else {
+                int ax = 0, ay = 0, az = 0;
+                for (int dx = -1; dx <= 1; dx++)
+                    for (int dy = -1; dy <= 1; dy++)
+                        for (int dz = -1; dz <= 1; dz++) {
+                            if (dx == 0 && dy == 0 && dz == 0) continue;
+                            const int nx = int(x) + dx, ny = int(y) + dy, nz = int(z) + dz;
+                            bool occd = false;
+                            if (nx >= 0 && ny >= 0 && nz >= 0 && nx < L && ny < L && nz < L) {
+                                const uint64_t bi = occ_index(uint32_t(nx), uint32_t(ny), uint32_t(nz), D);
+                                occd = (occ[bi >> 5] >> (bi & 31u)) & 1u;
+                            }
+                            if (!occd) { ax += dx; ay += dy; az += dz; }
+                        }
+                nodes[next + c] = (lw & 0xFFu) | encode_normal_field(ax, ay, az);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+void set_last_error(const char* msg) { g_err = msg; }
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define VE_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(VE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+struct SceneSlot {
+    void* alloc = nullptr;   // node array allocation (nodes start 7 words in)
+    uint32_t* nodes = nullptr;
+    uint64_t n_words = 0;
+    uint32_t depth = 0;
+    CacheEntry* cache = nullptr;
+    bool live = false;
+};
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t n) {
+        if (n <= cap) return VE_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(n, 1);
+        if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess)
+            return fail(VE_ERR_NOMEM, "device allocation failed (" + std::to_string(want * sizeof(T)) + " bytes)");
+        cap = want;
+        return VE_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace ve
+
+struct ve_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    ve_renderer_config cfg{};
+    std::vector<ve::SceneSlot> scenes;
+    ve::DevBuf<ve::DevScene> d_scenes;
+    bool scenes_dirty = true;
+    ve::DevBuf<ve::DevMaterial> d_mats;
+    ve::DevBuf<ve::DevView> d_views;
+    ve::DevView* h_views = nullptr;  // pinned staging
+    size_t h_views_cap = 0;
+    ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
+    ve::DevBuf<uint4> p_hit, p_meta;
+    ve::DevBuf<uint8_t> p_vis;
+    ve::DevBuf<uint32_t> live0, live1, rayq;
+    ve::DevBuf<uint32_t> counters;
+    ve::DevBuf<unsigned long long> stats;
+    unsigned long long* h_stats = nullptr;  // pinned
+    ve::DevBuf<uint4> gbuf;
+    ve::DevBuf<uint32_t> out_vid, out_node;
+    ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
+    int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
+    cudaEvent_t ev[48] = {};
+    ve_frame_stats last{};
+    bool last_timing = false;
+    uint32_t last_launches = 0, last_trace_launches = 0;
+};
+
+namespace ve {
+
+static int sync_scenes(ve_ctx* c) {
+    if (!c->scenes_dirty) return VE_OK;
+    std::vector<DevScene> h(std::max<size_t>(c->scenes.size(), 1));
+    for (size_t i = 0; i < c->scenes.size(); i++) {
+        const SceneSlot& s = c->scenes[i];
+        h[i] = DevScene{s.nodes, s.n_words, s.cache, s.depth, c->cfg.hash_log2, c->cfg.hash_probes, 0u};
+    }
+    int rc = c->d_scenes.ensure(h.size());
+    if (rc) return rc;
+    VE_CUDA(cudaMemcpyAsync(c->d_scenes.p, h.data(), h.size() * sizeof(DevScene), cudaMemcpyHostToDevice, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    c->scenes_dirty = false;
+    return VE_OK;
+}
+
+static int compute_normals(ve_ctx* c, SceneSlot& s) {
+    const uint32_t D = s.depth;
+    if (D < 1 || D > 11) return VE_OK;
+    const uint64_t cap = std::max<uint64_t>(s.n_words, 16);
+    unsigned long long *fa = nullptr, *fb = nullptr;
+    uint32_t* cnt = nullptr;
+    uint32_t* occ = nullptr;
+    const uint64_t occ_words = ((1ull << (3 * D)) + 31) / 32;
+    auto cleanup = [&]() {
+        if (fa) cudaFree(fa);
+        if (fb) cudaFree(fb);
+        if (cnt) cudaFree(cnt);
+        if (occ) cudaFree(occ);
+    };
+    if (cudaMalloc(&fa, cap * 8) != cudaSuccess || cudaMalloc(&fb, cap * 8) != cudaSuccess ||
+        cudaMalloc(&cnt, 64 * 4) != cudaSuccess || cudaMalloc(&occ, occ_words * 4) != cudaSuccess) {
+        cleanup();
+        return fail(VE_ERR_NOMEM, "normal pass: device allocation failed");
+    }
+    cudaMemsetAsync(cnt, 0, 64 * 4, c->stream);
+    cudaMemsetAsync(occ, 0, occ_words * 4, c->stream);
+    const unsigned long long root = 0ull;  // slot 0, origin (0,0,0), level 0
+    cudaMemcpyAsync(fa, &root, 8, cudaMemcpyHostToDevice, c->stream);
+    const uint32_t one = 1;
+    cudaMemcpyAsync(cnt, &one, 4, cudaMemcpyHostToDevice, c->stream);
+    const int grid = c->num_sms * 8;
+    unsigned long long* in = fa;
+    unsigned long long* out = fb;
+    for (uint32_t k = 0; k + 1 < D; k++) {
+        k_expand<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, k, in, cnt + k, out, cnt + k + 1,
+                                              uint32_t(cap));
+        std::swap(in, out);
+    }
+    const uint32_t* lc = cnt + (D - 1);
+    k_leaf_pass<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, 0, uint32_t(cap));
+    k_leaf_pass<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, 1, uint32_t(cap));
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cleanup();
+    if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("normal pass: ") + cudaGetErrorString(e));
+    return VE_OK;
+}
+
+static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_views) {
+    int rc = 0;
+    if ((rc = c->gbuf.ensure(pixels)) || (rc = c->out_vid.ensure(pixels)) || (rc = c->out_node.ensure(pixels)) ||
+        (rc = c->out_rgb.ensure(pixels * 3)) || (rc = c->out_mapped.ensure(pixels * 3)))
+        return rc;
+    if ((rc = c->p_ray_o.ensure(paths)) || (rc = c->p_ray_d.ensure(paths)) || (rc = c->p_tp.ensure(paths)) ||
+        (rc = c->p_direct.ensure(paths)) || (rc = c->p_indirect.ensure(paths)) || (rc = c->p_pend.ensure(paths)) ||
+        (rc = c->p_hit.ensure(paths)) || (rc = c->p_meta.ensure(paths)) || (rc = c->p_vis.ensure(paths)) ||
+        (rc = c->live0.ensure(paths)) || (rc = c->live1.ensure(paths)) || (rc = c->rayq.ensure(paths * 2)))
+        return rc;
+    if ((rc = c->d_views.ensure(n_views))) return rc;
+    if (c->h_views_cap < n_views) {
+        if (c->h_views) cudaFreeHost(c->h_views);
+        c->h_views = nullptr;
+        if (cudaMallocHost(&c->h_views, sizeof(DevView) * n_views) != cudaSuccess)
+            return fail(VE_ERR_NOMEM, "pinned view table allocation failed");
+        c->h_views_cap = n_views;
+    }
+    return VE_OK;
+}
+
+static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_outputs* outs) {
+    if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "render: no views");
+    if (nv > 65535u) return fail(VE_ERR_INVALID, "render: at most 65535 views per batch");
+    uint64_t pixels = 0, paths = 0;
+    uint32_t tiles = 0, max_b = 0, flags = 0;
+    for (uint32_t i = 0; i < nv; i++) {
+        const ve_view& v = views[i];
+        const ve_frame_config& f = v.frame;
+        if (v.scene_id < 0 || size_t(v.scene_id) >= c->scenes.size() || !c->scenes[v.scene_id].live)
+            return fail(VE_ERR_NOT_FOUND, "render: unknown scene id " + std::to_string(v.scene_id));
+        if (f.width == 0 || f.height == 0 || f.width > 16384 || f.height > 16384)
+            return fail(VE_ERR_INVALID, "render: width/height must be in [1, 16384]");
+        if (f.spp == 0 || f.spp > 1024) return fail(VE_ERR_INVALID, "render: spp must be in [1, 1024]");
+        if (f.bounces + 2 > kMaxPasses) return fail(VE_ERR_INVALID, "render: bounces must be <= 16");
+        if (f.render_type > VE_RENDER_VARIANCE) return fail(VE_ERR_INVALID, "render: unknown render type");
+        // every DDA loop is bounded by its controlchecks; keep the bound finite
+        if (f.primary_controlchecks > kMaxControlChecks || f.bounce_controlchecks > kMaxControlChecks)
+            return fail(VE_ERR_INVALID, "render: controlchecks must be <= 65536");
+        if (f.reconstruction_radius > 64) return fail(VE_ERR_INVALID, "render: reconstruction_radius must be <= 64");
+        const uint32_t tx = (f.width + 15) / 16, ty = (f.height + 15) / 16;
+        tiles += tx * ty;
+        pixels += uint64_t(f.width) * f.height;
+        paths += uint64_t(f.width) * f.height * f.spp;
+        max_b = std::max(max_b, f.bounces);
+        flags |= f.flags;
+    }
+    if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
+    int rc = ensure_frame(c, pixels, paths, nv);
+    if (rc) return rc;
+    if ((flags & VE_FRAME_PATH_RGB) && (rc = c->path_rgb.ensure(paths * 3))) return rc;
+    if ((rc = sync_scenes(c))) return rc;
+    // view table
+    uint32_t tile_base = 0;
+    uint64_t pix_base = 0, path_base = 0;
+    for (uint32_t i = 0; i < nv; i++) {
+        const ve_view& v = views[i];
+        const ve_frame_config& f = v.frame;
+        DevView& d = c->h_views[i];
+        std::memset(&d, 0, sizeof(d));
+        std::memcpy(d.cam, v.camera, sizeof(d.cam));
+        d.scene = uint32_t(v.scene_id);
+        d.W = f.width; d.H = f.height; d.spp = f.spp;
+        d.bounces = f.bounces; d.cc_primary = f.primary_controlchecks; d.cc_bounce = f.bounce_controlchecks;
+        d.recon_radius = f.reconstruction_radius; d.render_type = f.render_type; d.frame_index = f.frame_index;
+        d.flags = f.flags;
+        d.tiles_x = (f.width + 15) / 16;
+        for (int k = 0; k < 3; k++) { d.sun[k] = f.sun_dir[k]; d.sky[k] = f.sky[k]; }
+        d.sun_intensity = f.sun_intensity;
+        d.decay = f.decay;
+        d.variance_norm = f.variance_norm;
+        d.pix_base = uint32_t(pix_base);
+        d.tile_base = tile_base;
+        d.path_base = path_base;
+        tile_base += d.tiles_x * ((f.height + 15) / 16);
+        pix_base += uint64_t(f.width) * f.height;
+        path_base += uint64_t(f.width) * f.height * f.spp;
+    }
+    cudaStream_t st = c->stream;
+    const bool timing = (flags & VE_FRAME_TIMING) != 0;
+    const bool count = (flags & VE_FRAME_COUNT_FETCH) != 0;
+    uint32_t launches = 0, trace_launches = 0;
+    VE_CUDA(cudaMemcpyAsync(c->d_views.p, c->h_views, sizeof(DevView) * nv, cudaMemcpyHostToDevice, st));
+    VE_CUDA(cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st));
+    VE_CUDA(cudaMemsetAsync(c->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), st));
+    // events: 0 start, 1 after decay, 2 after primary, then per pass
+    // (shade, trace) pairs, last = after resolve
+    int ne = 0;
+    auto rec = [&]() {
+        if (timing) cudaEventRecord(c->ev[ne], st);
+        ne++;
+    };
+    rec();
+    // decay once per distinct scene (first view's decay factor)
+    {
+        std::vector<int> seen;
+        for (uint32_t i = 0; i < nv; i++) {
+            const int s = views[i].scene_id;
+            if (std::find(seen.begin(), seen.end(), s) != seen.end()) continue;
+            seen.push_back(s);
+            const float dk = views[i].frame.decay;
+            if (dk != 1.0f) {
+                const uint32_t n = 1u << c->cfg.hash_log2;
+                k_decay<<<c->num_sms * 8, 256, 0, st>>>(c->scenes[s].cache, n, dk);
+                launches++;
+            }
+        }
+    }
+    rec();
+    FrameArgs a{};
+    a.views = c->d_views.p;
+    a.n_views = nv;
+    a.total_tiles = tiles;
+    a.scenes = c->d_scenes.p;
+    a.mats = c->d_mats.p;
+    a.p_ray_o = c->p_ray_o.p; a.p_ray_d = c->p_ray_d.p; a.p_tp = c->p_tp.p;
+    a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
+    a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p; a.p_vis = c->p_vis.p;
+    a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p;
+    a.counters = c->counters.p; a.stats = c->stats.p;
+    a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
+    a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
+    a.path_rgb = (flags & VE_FRAME_PATH_RGB) ? c->path_rgb.p : nullptr;
+    if (count) k_primary<true><<<tiles, 256, 0, st>>>(a);
+    else k_primary<false><<<tiles, 256, 0, st>>>(a);
+    launches++;
+    rec();
+    for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
+        k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
+        launches++;
+        rec();
+        if (pass <= max_b) {
+            if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
+            else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
+            launches++;
+            trace_launches++;
+        }
+        rec();
+    }
+    k_resolve<<<tiles, 256, 0, st>>>(a);
+    launches++;
+    rec();
+    VE_CUDA(cudaGetLastError());
+    c->last_launches = launches;
+    c->last_trace_launches = trace_launches;
+    c->last_timing = timing;
+    std::memset(&c->last, 0, sizeof(c->last));
+    if (timing) {
+        cudaEventSynchronize(c->ev[ne - 1]);
+        float t = 0;
+        cudaEventElapsedTime(&t, c->ev[0], c->ev[1]); c->last.ms_decay = t;
+        cudaEventElapsedTime(&t, c->ev[1], c->ev[2]); c->last.ms_primary = t;
+        for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
+            const int e0 = 2 + 2 * int(pass);
+            cudaEventElapsedTime(&t, c->ev[e0], c->ev[e0 + 1]); c->last.ms_shade += t;
+            cudaEventElapsedTime(&t, c->ev[e0 + 1], c->ev[e0 + 2]); c->last.ms_trace += t;
+        }
+        cudaEventElapsedTime(&t, c->ev[ne - 2], c->ev[ne - 1]); c->last.ms_resolve = t;
+        cudaEventElapsedTime(&t, c->ev[0], c->ev[ne - 1]); c->last.ms_total = t;
+    }
+    VE_CUDA(cudaMemcpyAsync(c->h_stats, c->stats.p, ST_TOTAL * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    // host outputs
+    if (outs) {
+        uint64_t pb = 0, qb = 0;
+        for (uint32_t i = 0; i < nv; i++) {
+            const ve_frame_config& f = views[i].frame;
+            const uint64_t np = uint64_t(f.width) * f.height;
+            const uint64_t nq = np * f.spp;
+            ve_frame_outputs& o = outs[i];
+            if (o.gbuffer) VE_CUDA(cudaMemcpyAsync(o.gbuffer, c->gbuf.p + pb, np * 16, cudaMemcpyDeviceToHost, st));
+            if (o.voxel_id) VE_CUDA(cudaMemcpyAsync(o.voxel_id, c->out_vid.p + pb, np * 4, cudaMemcpyDeviceToHost, st));
+            if (o.hit_node) VE_CUDA(cudaMemcpyAsync(o.hit_node, c->out_node.p + pb, np * 4, cudaMemcpyDeviceToHost, st));
+            if (o.rgb) VE_CUDA(cudaMemcpyAsync(o.rgb, c->out_rgb.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st));
+            if (o.mapped) VE_CUDA(cudaMemcpyAsync(o.mapped, c->out_mapped.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st));
+            if (o.path_rgb && (f.flags & VE_FRAME_PATH_RGB))
+                VE_CUDA(cudaMemcpyAsync(o.path_rgb, c->path_rgb.p + 3 * qb, nq * 12, cudaMemcpyDeviceToHost, st));
+            pb += np;
+            qb += nq;
+        }
+        VE_CUDA(cudaStreamSynchronize(st));
+    }
+    return VE_OK;
+}
+
+}  // namespace ve
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace ve;
+
+extern "C" {
+
+const char* ve_last_error(void) { return g_err.c_str(); }
+
+int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
+    if (!out) return fail(VE_ERR_INVALID, "ctx_create: null output");
+    *out = nullptr;
+    ve_renderer_config c{};
+    c.device = 0;
+    c.hash_log2 = 22;
+    c.hash_probes = 64;
+    if (cfg) c = *cfg;
+    if (c.hash_log2 < 8 || c.hash_log2 > 28) return fail(VE_ERR_INVALID, "ctx_create: hash_log2 must be in [8, 28]");
+    if (c.hash_probes == 0) c.hash_probes = 64;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(VE_ERR_CUDA, "ctx_create: no CUDA device available");
+    if (c.device < 0 || c.device >= ndev) return fail(VE_ERR_INVALID, "ctx_create: bad device index");
+    VE_CUDA(cudaSetDevice(c.device));
+    ve_ctx* x = new ve_ctx();
+    x->device = c.device;
+    x->cfg = c;
+    cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, c.device);
+    if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete x;
+        return fail(VE_ERR_CUDA, "ctx_create: stream creation failed");
+    }
+    for (auto& e : x->ev) cudaEventCreate(&e);
+    int bt = 0, btc = 0, bs = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade, 256, 0);
+    x->grid_trace = x->num_sms * std::max(bt, 1);
+    x->grid_trace_count = x->num_sms * std::max(btc, 1);
+    x->grid_shade = x->num_sms * std::max(bs, 1);
+    int rc = 0;
+    if ((rc = x->counters.ensure(CNT_TOTAL)) || (rc = x->stats.ensure(ST_TOTAL)) || (rc = x->d_mats.ensure(128))) {
+        ve_ctx_destroy(x);
+        return rc;
+    }
+    cudaMallocHost(&x->h_stats, ST_TOTAL * sizeof(unsigned long long));
+    cudaMemset(x->d_mats.p, 0, 128 * sizeof(DevMaterial));
+    *out = x;
+    return VE_OK;
+}
+
+int ve_ctx_destroy(ve_ctx* c) {
+    if (!c) return VE_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& s : c->scenes) {
+        if (s.alloc) cudaFree(s.alloc);
+        if (s.cache) cudaFree(s.cache);
+    }
+    c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
+    c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
+    c->p_indirect.release(); c->p_pend.release(); c->p_hit.release(); c->p_meta.release(); c->p_vis.release();
+    c->live0.release(); c->live1.release(); c->rayq.release(); c->counters.release(); c->stats.release();
+    c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
+    c->out_mapped.release(); c->path_rgb.release();
+    if (c->h_views) cudaFreeHost(c->h_views);
+    if (c->h_stats) cudaFreeHost(c->h_stats);
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return VE_OK;
+}
+
+int ve_ctx_stream(ve_ctx* c, void** stream) {
+    if (!c || !stream) return fail(VE_ERR_INVALID, "ctx_stream: null argument");
+    *stream = c->stream;
+    return VE_OK;
+}
+
+int ve_ctx_synchronize(ve_ctx* c) {
+    if (!c) return fail(VE_ERR_INVALID, "ctx_synchronize: null context");
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t depth, uint32_t flags,
+                    int32_t* scene_id) {
+    if (!c || !words || !scene_id) return fail(VE_ERR_INVALID, "scene_upload: null argument");
+    if (n_words < 9) return fail(VE_ERR_INVALID, "scene_upload: a node array has at least 9 words");
+    if (depth < 1 || depth > 16) return fail(VE_ERR_INVALID, "scene_upload: depth must be in [1, 16]");
+    if (n_words >= (1ull << 32)) return fail(VE_ERR_CAPACITY, "scene_upload: more than 2^32 words");
+    cudaSetDevice(c->device);
+    SceneSlot s;
+    s.depth = depth;
+    s.n_words = n_words;
+    // nodes start 7 words into the allocation so every 8-child block
+    // (slots 1 + 8k) begins on a 32-byte boundary
+    if (cudaMalloc(&s.alloc, (n_words + 8) * 4) != cudaSuccess)
+        return fail(VE_ERR_NOMEM, "scene_upload: node array allocation failed");
+    s.nodes = reinterpret_cast<uint32_t*>(s.alloc) + 7;
+    const size_t cache_bytes = sizeof(CacheEntry) << c->cfg.hash_log2;
+    if (cudaMalloc(&s.cache, cache_bytes) != cudaSuccess) {
+        cudaFree(s.alloc);
+        return fail(VE_ERR_NOMEM, "scene_upload: radiance cache allocation failed");
+    }
+    VE_CUDA(cudaMemcpyAsync(s.nodes, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
+    VE_CUDA(cudaMemsetAsync(s.cache, 0, cache_bytes, c->stream));
+    s.live = true;
+    if (!(flags & VE_SCENE_KEEP_NORMALS)) {
+        int rc = compute_normals(c, s);
+        if (rc) {
+            cudaFree(s.alloc);
+            cudaFree(s.cache);
+            return rc;
+        }
+    }
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    int32_t id = -1;
+    for (size_t i = 0; i < c->scenes.size(); i++)
+        if (!c->scenes[i].live) { id = int32_t(i); break; }
+    if (id < 0) {
+        id = int32_t(c->scenes.size());
+        c->scenes.push_back(s);
+    } else {
+        c->scenes[id] = s;
+    }
+    c->scenes_dirty = true;
+    *scene_id = id;
+    return VE_OK;
+}
+
+int ve_scene_release(ve_ctx* c, int32_t id) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_release: unknown scene");
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    SceneSlot& s = c->scenes[id];
+    cudaFree(s.alloc);
+    cudaFree(s.cache);
+    s = SceneSlot();
+    c->scenes_dirty = true;
+    return VE_OK;
+}
+
+int ve_scene_apply_edits(ve_ctx* c, int32_t id, const uint32_t* slots, const uint32_t* words, uint64_t n,
+                         uint32_t flags) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_apply_edits: unknown scene");
+    if (n && (!slots || !words)) return fail(VE_ERR_INVALID, "scene_apply_edits: null arrays");
+    SceneSlot& s = c->scenes[id];
+    for (uint64_t i = 0; i < n; i++)
+        if (slots[i] >= s.n_words) return fail(VE_ERR_CAPACITY, "scene_apply_edits: slot beyond the uploaded array");
+    cudaSetDevice(c->device);
+    for (uint64_t i = 0; i < n; i++)
+        VE_CUDA(cudaMemcpyAsync(s.nodes + slots[i], words + i, 4, cudaMemcpyHostToDevice, c->stream));
+    if (!(flags & VE_SCENE_KEEP_NORMALS)) {
+        int rc = compute_normals(c, s);
+        if (rc) return rc;
+    }
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t* n_words) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_download: unknown scene");
+    SceneSlot& s = c->scenes[id];
+    if (n_words) *n_words = s.n_words;
+    if (out && cap) {
+        VE_CUDA(cudaMemcpyAsync(out, s.nodes, std::min<uint64_t>(cap, s.n_words) * 4, cudaMemcpyDeviceToHost, c->stream));
+        VE_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return VE_OK;
+}
+
+int ve_scene_footprint(ve_ctx* c, int32_t id, uint64_t* bytes) {
+    if (!c || !bytes || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_footprint: unknown scene");
+    *bytes = (c->scenes[id].n_words + 8) * 4 + (sizeof(CacheEntry) << c->cfg.hash_log2);
+    return VE_OK;
+}
+
+int ve_set_materials(ve_ctx* c, const void* entries, uint32_t n) {
+    if (!c || (!entries && n)) return fail(VE_ERR_INVALID, "set_materials: null argument");
+    if (n > 128) return fail(VE_ERR_CAPACITY, "set_materials: at most 128 materials");
+    std::vector<DevMaterial> m(128);
+    std::memset(m.data(), 0, m.size() * sizeof(DevMaterial));
+    const uint8_t* src = static_cast<const uint8_t*>(entries);
+    for (uint32_t i = 0; i < n; i++) {
+        float f[16];
+        std::memcpy(f, src + 64 * i, 64);
+        int32_t emissive;
+        std::memcpy(&emissive, src + 64 * i + 44, 4);
+        m[i].albedo_rough = make_float4(f[0], f[1], f[2], f[8]);
+        m[i].params = make_float4(f[10], f[9], emissive ? 1.0f : 0.0f, f[12]);
+    }
+    cudaSetDevice(c->device);
+    VE_CUDA(cudaMemcpyAsync(c->d_mats.p, m.data(), 128 * sizeof(DevMaterial), cudaMemcpyHostToDevice, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_cache_reset(ve_ctx* c, int32_t id) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "cache_reset: unknown scene");
+    VE_CUDA(cudaMemsetAsync(c->scenes[id].cache, 0, sizeof(CacheEntry) << c->cfg.hash_log2, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_cache_dump(ve_ctx* c, int32_t id, uint32_t* vids, uint32_t* counts, float* values, uint64_t cap, uint64_t* n) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "cache_dump: unknown scene");
+    const size_t N = size_t(1) << c->cfg.hash_log2;
+    std::vector<CacheEntry> h(N);
+    VE_CUDA(cudaMemcpyAsync(h.data(), c->scenes[id].cache, N * sizeof(CacheEntry), cudaMemcpyDeviceToHost, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < N; i++)
+        if (h[i].key) idx.push_back(i);
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return h[a].key < h[b].key; });
+    if (n) *n = idx.size();
+    for (size_t j = 0; j < idx.size() && j < cap; j++) {
+        const CacheEntry& e = h[idx[j]];
+        if (vids) vids[j] = e.key;
+        if (counts) counts[j] = e.count;
+        if (values) {
+            values[5 * j] = e.rgbw.w;
+            values[5 * j + 1] = e.rgbw.x;
+            values[5 * j + 2] = e.rgbw.y;
+            values[5 * j + 3] = e.rgbw.z;
+            values[5 * j + 4] = e.l2;
+        }
+    }
+    return VE_OK;
+}
+
+int ve_render(ve_ctx* c, const ve_view* view, ve_frame_outputs* out) {
+    if (!c || !view) return fail(VE_ERR_INVALID, "render: null argument");
+    cudaSetDevice(c->device);
+    return render_batch(c, view, 1, out);
+}
+
+int ve_render_batch(ve_ctx* c, const ve_view* views, uint32_t n, ve_frame_outputs* outs) {
+    if (!c) return fail(VE_ERR_INVALID, "render_batch: null context");
+    cudaSetDevice(c->device);
+    return render_batch(c, views, n, outs);
+}
+
+int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
+    if (!c || !s) return fail(VE_ERR_INVALID, "get_stats: null argument");
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    ve_frame_stats r = c->last;
+    const unsigned long long* h = c->h_stats;
+    r.rays_primary = h[ST_RAYS_PRIMARY];
+    r.rays_bounce = h[ST_RAYS_BOUNCE];
+    r.rays_shadow = h[ST_RAYS_SHADOW];
+    r.fetch_nodes = h[ST_FETCH];
+    r.paths = h[ST_PATHS];
+    r.deposits = h[ST_DEPOSITS];
+    r.deposits_dropped = h[ST_DROPPED];
+    r.dda_steps = h[ST_STEPS];
+    r.kernel_launches = c->last_launches;
+    r.trace_launches = c->last_trace_launches;
+    r.cache_capacity = 1ull << c->cfg.hash_log2;
+    *s = r;
+    return VE_OK;
+}
+
+}  // extern "C"
