@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the plain method: Mrays/s at 1080p on a depth-10 octree.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one frame of the large workload: depth-10 (1024^3) seeded terrain
+with overhangs (66.2M voxels, 77.6M node words), 1920x1080, 4 spp x 3 bounces,
+radiance cache 2^22 entries, decay 0.95, camera on the seeded 64-frame orbit of
+radius 600.  A ray is one DDA traversal (primary, bounce or sun shadow).
+
+* ``value``: device-resident frames back to back (no host outputs), CUDA
+  events on the renderer's stream around K frames, max over ranks.
+* ``e2e``: the same frames through the public API with host outputs (voxel-id
+  image + RGB into pinned host memory) and the per-frame view table uploaded;
+  events around all K steps, copies included.
+* ``roofline``: the trace kernel (bounce + shadow DDA): algorithmic bytes
+  (4 B per distinct node word read + 48 B ray state per traversal) over its
+  CUDA-event time inside the timed frames, against the measured HBM copy
+  bandwidth.
+* ``cpu_baseline``: the scalar C++ oracle on the host cores (all threads),
+  on a bounded band of rows of frame 0.
+
+Multi-GPU (torchrun, one process per GPU): replicas — rank r renders its own
+orbit frames; no collective on the data path ("scaling": "weak").
+``--impl reference`` times the reference's path on the host CPU (the oracle
+port of its GLSL passes; the reference has no runnable GPU path here).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def load_package():
+    import importlib.util
+
+    pkg = os.path.join(ROOT, "voxelengine3.0_b200")
+    if "ve_b200" in sys.modules:
+        return sys.modules["ve_b200"]
+    spec = importlib.util.spec_from_file_location("ve_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["ve_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+METRIC = "Mrays/s at 1080p depth-10 octree"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def frame_config(ve, W, f, flags=0):
+    return ve.FrameConfig(width=W.width, height=W.height, spp=W.spp, bounces=W.bounces, frame_index=f,
+                          primary_controlchecks=W.primary_controlchecks,
+                          bounce_controlchecks=W.bounce_controlchecks, flags=flags)
+
+
+def rays_of(st):
+    return st["rays_primary"] + st["rays_bounce"] + st["rays_shadow"]
+
+
+def cpu_baseline(ve, W, words, mats, budget_s):
+    """Oracle on all host cores over a bounded band of rows of frame 0."""
+    from oracle.oracle import Oracle, OracleRenderer, frame_params
+
+    orc = Oracle()
+    threads = os.cpu_count() or 1
+    eye, d = _orbit(W, 0)
+    cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+    fp = frame_params(frame_config(ve, W, 0))
+    mid = W.height // 2
+    rows = max(threads, 8)
+    total_rays = 0
+    total_t = 0.0
+    while True:
+        r0 = max(0, mid - rows // 2)
+        rr = OracleRenderer(orc)
+        t = time.perf_counter()
+        out = rr.render(words, W.depth, mats, cam, fp, threads=threads, rows=(r0, r0 + rows), want_rgb=False)
+        dt = time.perf_counter() - t
+        s = out["stats"]
+        total_rays, total_t = s["rays_primary"] + s["rays_bounce"] + s["rays_shadow"], dt
+        if dt * 2.5 > budget_s or rows >= W.height:
+            break
+        rows = min(W.height, int(rows * max(2.0, budget_s / max(dt, 1e-3) * 0.5)))
+    return {"value": total_rays / total_t / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"frame 0 rows {r0}-{r0 + rows - 1} of {W.width}x{W.height}, {W.spp} spp x {W.bounces} "
+                      f"bounces, {total_rays} rays in {total_t:.1f} s"}
+
+
+def _orbit(W, f):
+    import ve_b200.workloads as w
+
+    return w.orbit_camera(f, W.frames, W.seed)
+
+
+def run_reference(args, W, rank, world):
+    """The reference's path on the host CPU (oracle port, all threads)."""
+    if rank != 0:
+        return 0
+    ve = load_package()
+    import ve_b200.workloads  # noqa: F401
+    from oracle.oracle import Oracle, OracleRenderer, frame_params
+
+    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
+    mats = ve.terrain_materials(W.seed)
+    orc = Oracle()
+    # normals as the device pass computes them (3x3x3 occupancy gradient)
+    words = _words_with_normals(ve, words, W.depth)
+    threads = os.cpu_count() or 1
+    rr = OracleRenderer(orc)
+    rows_per_step = max(threads, 16)
+
+    def step(f):
+        eye, d = _orbit(W, f % W.frames)
+        cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+        r0 = (W.height // 2 - rows_per_step // 2)
+        t = time.perf_counter()
+        out = rr.render(words, W.depth, mats, cam, frame_params(frame_config(ve, W, f)), threads=threads,
+                        rows=(r0, r0 + rows_per_step), want_rgb=False)
+        return time.perf_counter() - t, rays_of_oracle(out["stats"])
+
+    for f in range(args.warmup):
+        step(f)
+    tt = 0.0
+    rays = 0
+    for f in range(args.steps):
+        dt, n = step(args.warmup + f)
+        tt += dt
+        rays += n
+    v = rays / tt / 1e6
+    sample = (f"{rows_per_step} rows x {W.width} px per frame (frames {args.warmup}..{args.warmup + args.steps - 1} "
+              f"of the orbit), {W.spp} spp x {W.bounces} bounces")
+    line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain)",
+            "impl": "reference",
+            "config": {"workload": "large: depth-10 terrain 1920x1080 4 spp x 3 bounces (row band per step)"},
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def rays_of_oracle(s):
+    return s["rays_primary"] + s["rays_bounce"] + s["rays_shadow"]
+
+
+def _words_with_normals(ve, words, depth):
+    with ve.Renderer(hash_log2=8) as r:
+        sid = r.upload_scene(words, depth)
+        return r.download_scene(sid)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    ve = load_package()
+    import ve_b200.workloads as wl
+
+    W = wl.LARGE
+    if args.impl == "reference":
+        return run_reference(args, W, rank, world)
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    torch.cuda.init()
+
+    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
+    mats = ve.terrain_materials(W.seed)
+    r = ve.Renderer(device=local, hash_log2=W.hash_log2)
+    r.set_materials(mats)
+    sid = r.upload_scene(words, W.depth)
+    stream = torch.cuda.ExternalStream(r.stream, device=local)
+
+    def frame(i):  # replicas: rank r takes every world-th orbit frame
+        return (rank + world * i) % W.frames
+
+    def cams(i):
+        eye, d = wl.orbit_camera(frame(i), W.frames, W.seed)
+        return ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+
+    K, Wm = args.steps, args.warmup
+    cam_list = [cams(Wm + i) for i in range(K)]
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        r.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # warm-up
+    for i in range(Wm):
+        r.render(sid, cams(i), frame_config(ve, W, frame(i)), outputs=())
+    r.synchronize()
+
+    # ---- timed region: device-resident frames, per-pass CUDA events --------
+    r.reset_total_stats()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for i in range(K):
+            r.render(sid, cam_list[i], frame_config(ve, W, frame(Wm + i), ve.FRAME_TIMING), outputs=())
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    tot = r.total_stats()
+    ms_max = max_over_ranks(ms)
+    rays_all = sum_over_ranks(rays_of(tot))
+    value = rays_all / (ms_max / 1e3) / 1e6
+
+    # ---- algorithmic bytes of the same frames (node-word fetch counts) -----
+    r.reset_total_stats()
+    for i in range(K):
+        r.render(sid, cam_list[i], frame_config(ve, W, frame(Wm + i), ve.FRAME_COUNT_FETCH), outputs=())
+    cnt = r.total_stats()
+    trace_rays = cnt["rays_bounce"] + cnt["rays_shadow"]
+    trace_bytes = 4.0 * cnt["fetch_nodes_trace"] + 48.0 * trace_rays
+    trace_ms = tot["ms_trace"]
+    launches = tot["trace_launches"]
+    achieved = trace_bytes / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
+    peak, peak_kind = peaks()
+
+    # ---- e2e: public API, host outputs, view upload each step --------------
+    hv = torch.empty((W.height, W.width), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hrgb = torch.empty((W.height, W.width, 3), dtype=torch.float32, pin_memory=True).numpy()
+    outs = ve.FrameOutputsC()
+    outs.voxel_id = hv.ctypes.data
+    outs.rgb = hrgb.ctypes.data
+    lib = ve.load_library()
+    import ctypes
+
+    views = [ve.Renderer.make_view(sid, cam_list[i], frame_config(ve, W, frame(Wm + i))) for i in range(K)]
+    r.reset_total_stats()
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i in range(K):
+        rc = lib.ve_render(r._h, ctypes.byref(views[i]), ctypes.byref(outs))
+        if rc != 0:
+            raise RuntimeError(lib.ve_last_error().decode())
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    etot = r.total_stats()
+    e2e_value = sum_over_ranks(rays_of(etot)) / (e2e_ms / 1e3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dev_words = r.download_scene(sid)
+        cpu = cpu_baseline(ve, W, dev_words, mats, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded value-noise terrain, seeded orbit camera)",
+            "config": {
+                "workload": "large: depth-10 (1024^3) terrain + overhangs, 66.2M voxels, 1920x1080, "
+                            "4 spp x 3 bounces, hash 2^22, decay 0.95, orbit r=600",
+                "voxels": int(nv), "node_words": int(words.size),
+                "controlchecks": [W.primary_controlchecks, W.bounce_controlchecks],
+                "l2": "inputs larger than L2 (310 MB node array, ~1 GB path state)",
+                "rays_per_step": rays_of(tot) / K,
+                "ray_mix_per_step": {k: tot[k] / K for k in ("rays_primary", "rays_bounce", "rays_shadow")},
+                "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": etot["h2d_bytes"] / K,
+                    "d2h_bytes_per_step": etot["d2h_bytes"] / K},
+            "roofline": {"bound": "hbm", "kernel": "k_trace (bounce + shadow DDA)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": trace_bytes / max(launches, 1),
+                         "ms_per_launch": trace_ms / max(launches, 1)},
+            "gpu_launches": int(tot["kernel_launches"]),
+            "stage_ms_per_step": {k: tot[k] / K for k in ("ms_primary", "ms_trace", "ms_shade", "ms_resolve",
+                                                           "ms_decay")},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

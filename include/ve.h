@@ -91,7 +91,8 @@ typedef struct ve_frame_outputs {
     uint32_t* hit_node; /* 1 x u32 per pixel: node slot of the hit leaf, 0 on miss */
     float* rgb;         /* 3 x f32 per pixel */
     float* mapped;      /* 3 x f32 per pixel */
-    float* path_rgb;    /* 3 x f32 per path (pixel * spp + sample); VE_FRAME_PATH_RGB */
+    float* path_rgb;    /* 3 x f32 per path (pixel * spp + sample); VE_FRAME_PATH_RGB;
+                           zero for pixels without a primary hit (no path) */
 } ve_frame_outputs;
 
 /* FrameStats (src/renderer/core.hpp:164-185) and the profiler's stage
@@ -99,10 +100,13 @@ typedef struct ve_frame_outputs {
  * events of the last ve_render / ve_render_batch call. */
 typedef struct ve_frame_stats {
     uint64_t rays_primary, rays_bounce, rays_shadow;
-    uint64_t fetch_nodes; /* node words read (VE_FRAME_COUNT_FETCH) */
+    uint64_t fetch_nodes; /* node words read by every DDA (VE_FRAME_COUNT_FETCH) */
     uint64_t paths, deposits, deposits_dropped;
     uint64_t dda_steps;   /* DDA outer iterations (VE_FRAME_COUNT_FETCH) */
-    float ms_total, ms_primary, ms_trace, ms_shade, ms_resolve, ms_decay;
+    uint64_t fetch_nodes_trace, dda_steps_trace; /* the bounce/shadow trace kernel alone */
+    uint64_t h2d_bytes, d2h_bytes;               /* bytes the call(s) copied host<->device */
+    uint64_t frames;                             /* render calls covered */
+    float ms_total, ms_primary, ms_trace, ms_shade, ms_resolve, ms_decay; /* VE_FRAME_TIMING */
     uint32_t trace_launches, kernel_launches;
     uint64_t cache_capacity;
 } ve_frame_stats;
@@ -209,6 +213,10 @@ int ve_render(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
 int ve_render_batch(ve_ctx* ctx, const ve_view* views, uint32_t n_views, ve_frame_outputs* outs);
 /* stats of the last render call (synchronises the context stream) */
 int ve_get_stats(ve_ctx* ctx, ve_frame_stats* stats);
+/* stats summed over every render call since ve_reset_total_stats (device
+ * counters accumulate on the stream: no host synchronisation per frame) */
+int ve_get_total_stats(ve_ctx* ctx, ve_frame_stats* stats);
+int ve_reset_total_stats(ve_ctx* ctx);
 
 #ifdef __cplusplus
 }

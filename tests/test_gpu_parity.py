@@ -124,7 +124,13 @@ def test_render_types(ve, renderer, oracle, small, rtype):
     _, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 3, want=("gbuffer", "rgb"))
     g, st, o = outs[-1]
     assert np.array_equal(g["gbuffer"], o["gbuffer"])
-    assert close_rel(g["rgb"], o["rgb"]).all()
+    if rtype == 5:
+        # VARIANCE view: E[L^2] - E[L]^2 cancels catastrophically, so the FP32
+        # cache cannot hold 1e-4 relative against FP64; the display value
+        # (in [0, 1]) is held to 1e-4 absolute instead.
+        assert (np.abs(g["rgb"].astype(np.float64) - o["rgb"]) <= 1e-4).all()
+    else:
+        assert close_rel(g["rgb"], o["rgb"]).all()
 
 
 def scene_from_voxels(ve, depth, voxels):
@@ -139,7 +145,10 @@ EDGE_CASES = {
     "single_voxel": (3, [(3, 4, 5, 2)], (4.5, 4.5, -10.0), (3.5, 4.5, 5.5)),
     "full_octant": (3, [(x, y, z, 1 + (x + y + z) % 8) for x in range(4) for y in range(4) for z in range(4)],
                     (12.0, 9.0, 13.0), (2.0, 2.0, 2.0)),
-    "axis_aligned": (4, [(x, 0, z, 3) for x in range(16) for z in range(16)], (8.0, 12.0, 8.0), (8.0, 0.0, 8.0)),
+    # camera along +z, odd resolution: the centre row/column rays have exact
+    # zero components (reciprocal +-inf in the slab tests)
+    "axis_aligned": (4, [(x, y, 10 + (x * y) % 3, 3) for x in range(16) for y in range(16)], (8.0, 8.0, -6.0),
+                     (8.0, 8.0, 10.0)),
     "inside_volume": (5, [(x, y, 0, 4) for x in range(32) for y in range(32)], (16.0, 16.0, 20.0),
                       (16.0, 16.0, 0.0)),
     "depth1": (1, [(0, 0, 0, 1), (1, 1, 1, 2)], (3.0, 3.0, -3.0), (1.0, 1.0, 1.0)),
@@ -158,10 +167,9 @@ def test_edge_cases(ve, renderer, oracle, case, cc):
         dev_words = renderer.download_scene(sid)
         assert np.array_equal(dev_words, oracle.fill_normals(words, depth))
         d = ve.look_at(eye, target)
-        if case == "axis_aligned":
-            d = np.array([0.0, -1.0, 0.0], np.float32)
-        cam = ve.camera_ubo(np.asarray(eye, np.float32), d, 70.0, 1.0)
-        fc = ve.FrameConfig(width=40, height=24, spp=3, bounces=2, primary_controlchecks=cc,
+        W, H = (41, 25) if case == "axis_aligned" else (40, 24)
+        cam = ve.camera_ubo(np.asarray(eye, np.float32), d, 70.0, W / H)
+        fc = ve.FrameConfig(width=W, height=H, spp=3, bounces=2, primary_controlchecks=cc,
                             bounce_controlchecks=cc, reconstruction_radius=3, flags=ve.FRAME_PATH_RGB)
         orc, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 2,
                              want=("gbuffer", "rgb", "path_rgb"))
@@ -198,6 +206,8 @@ def test_batch_matches_single_views(ve, renderer, oracle, small):
         for (s, c, f), b in zip(views, batch):
             single = renderer.render(s, c, f, outputs=("gbuffer", "path_rgb"))
             assert np.array_equal(b["gbuffer"], single["gbuffer"])
+            hit = np.repeat(single["gbuffer"][..., 3].reshape(-1) != 0, f.spp)
+            assert hit.any() and not b["path_rgb"][~hit].any()
             assert np.array_equal(b["path_rgb"].view(np.uint32), single["path_rgb"].view(np.uint32))
     finally:
         renderer.release_scene(sid6)

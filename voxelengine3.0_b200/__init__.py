@@ -81,6 +81,8 @@ class FrameStatsC(ctypes.Structure):
     _fields_ = [("rays_primary", ctypes.c_uint64), ("rays_bounce", ctypes.c_uint64),
                 ("rays_shadow", ctypes.c_uint64), ("fetch_nodes", ctypes.c_uint64), ("paths", ctypes.c_uint64),
                 ("deposits", ctypes.c_uint64), ("deposits_dropped", ctypes.c_uint64), ("dda_steps", ctypes.c_uint64),
+                ("fetch_nodes_trace", ctypes.c_uint64), ("dda_steps_trace", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("frames", ctypes.c_uint64),
                 ("ms_total", ctypes.c_float), ("ms_primary", ctypes.c_float), ("ms_trace", ctypes.c_float),
                 ("ms_shade", ctypes.c_float), ("ms_resolve", ctypes.c_float), ("ms_decay", ctypes.c_float),
                 ("trace_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
@@ -135,6 +137,8 @@ _SIGNATURES = {
     "ve_render": ([_P, _PTR(ViewC), _PTR(FrameOutputsC)], ctypes.c_int),
     "ve_render_batch": ([_P, _PTR(ViewC), _U32, _P], ctypes.c_int),
     "ve_get_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
+    "ve_get_total_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
+    "ve_reset_total_stats": ([_P], ctypes.c_int),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -512,9 +516,19 @@ class Renderer:
         return results
 
     def stats(self) -> Dict[str, float]:
+        """Counters and timings of the last render call."""
         s = FrameStatsC()
         _check(self._lib.ve_get_stats(self._h, ctypes.byref(s)))
         return {name: getattr(s, name) for name, _ in FrameStatsC._fields_}
+
+    def total_stats(self) -> Dict[str, float]:
+        """Counters summed over every render since reset_total_stats()."""
+        s = FrameStatsC()
+        _check(self._lib.ve_get_total_stats(self._h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in FrameStatsC._fields_}
+
+    def reset_total_stats(self) -> None:
+        _check(self._lib.ve_reset_total_stats(self._h))
 
     # Renderer::run (reference-shaped): renders the bound scene from the bound camera
     def set_scene(self, scene_id: int) -> None:

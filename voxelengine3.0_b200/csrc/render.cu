@@ -79,11 +79,13 @@ enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
     ST_RAYS_BOUNCE,
     ST_RAYS_SHADOW,
-    ST_FETCH,
+    ST_FETCH,        // node words read by k_primary + k_trace
     ST_PATHS,
     ST_DEPOSITS,
     ST_DROPPED,
-    ST_STEPS,
+    ST_STEPS,        // DDA iterations of k_primary + k_trace
+    ST_FETCH_TRACE,  // node words read by k_trace alone
+    ST_STEPS_TRACE,
     ST_TOTAL = 16
 };
 enum : uint32_t { F_PENDING = 1u, F_TERM = 2u };
@@ -332,9 +334,16 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
         }
     }
     if (COUNT) {
-        atomicAdd(&a.stats[ST_FETCH], (unsigned long long)fetch);
-        atomicAdd(&a.stats[ST_STEPS], (unsigned long long)steps);
+        warp_add_stat(&a.stats[ST_FETCH], fetch);
+        warp_add_stat(&a.stats[ST_STEPS], steps);
+        warp_add_stat(&a.stats[ST_FETCH_TRACE], fetch);
+        warp_add_stat(&a.stats[ST_STEPS_TRACE], steps);
     }
+}
+
+// Adds the frame's counters to the running totals (ve_get_total_stats).
+__global__ void k_accum_stats(const unsigned long long* frame, unsigned long long* total) {
+    if (threadIdx.x < ST_TOTAL) total[threadIdx.x] += frame[threadIdx.x];
 }
 
 // shade.comp:543-575, 838-908 (bounce/shade loop) with the sun next-event
@@ -789,15 +798,26 @@ struct ve_ctx {
     bool scenes_dirty = true;
     ve::DevBuf<ve::DevMaterial> d_mats;
     ve::DevBuf<ve::DevView> d_views;
-    ve::DevView* h_views = nullptr;  // pinned staging
+    // pinned staging ring for the per-frame view table: a slot is rewritten
+    // only after the copy that last read it has executed
+    static constexpr int kStaging = 8;
+    ve::DevView* h_views[kStaging] = {};
     size_t h_views_cap = 0;
+    cudaEvent_t staging_ev[kStaging] = {};
+    int staging_next = 0;
     ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
     ve::DevBuf<uint4> p_hit, p_meta;
     ve::DevBuf<uint8_t> p_vis;
     ve::DevBuf<uint32_t> live0, live1, rayq;
     ve::DevBuf<uint32_t> counters;
     ve::DevBuf<unsigned long long> stats;
+    ve::DevBuf<unsigned long long> totals;
     unsigned long long* h_stats = nullptr;  // pinned
+    // host-side running totals (ve_get_total_stats)
+    uint64_t tot_frames = 0, tot_h2d = 0, tot_d2h = 0;
+    uint32_t tot_launches = 0, tot_trace_launches = 0;
+    float tot_ms[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t last_h2d = 0, last_d2h = 0;
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
@@ -879,10 +899,13 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
         return rc;
     if ((rc = c->d_views.ensure(n_views))) return rc;
     if (c->h_views_cap < n_views) {
-        if (c->h_views) cudaFreeHost(c->h_views);
-        c->h_views = nullptr;
-        if (cudaMallocHost(&c->h_views, sizeof(DevView) * n_views) != cudaSuccess)
-            return fail(VE_ERR_NOMEM, "pinned view table allocation failed");
+        cudaStreamSynchronize(c->stream);
+        for (int k = 0; k < ve_ctx::kStaging; k++) {
+            if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
+            c->h_views[k] = nullptr;
+            if (cudaMallocHost(&c->h_views[k], sizeof(DevView) * n_views) != cudaSuccess)
+                return fail(VE_ERR_NOMEM, "pinned view table allocation failed");
+        }
         c->h_views_cap = n_views;
     }
     return VE_OK;
@@ -919,13 +942,17 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (rc) return rc;
     if ((flags & VE_FRAME_PATH_RGB) && (rc = c->path_rgb.ensure(paths * 3))) return rc;
     if ((rc = sync_scenes(c))) return rc;
-    // view table
+    // view table, written into a staging slot whose previous copy has run
+    const int slot = c->staging_next;
+    c->staging_next = (slot + 1) % ve_ctx::kStaging;
+    VE_CUDA(cudaEventSynchronize(c->staging_ev[slot]));
+    DevView* hv = c->h_views[slot];
     uint32_t tile_base = 0;
     uint64_t pix_base = 0, path_base = 0;
     for (uint32_t i = 0; i < nv; i++) {
         const ve_view& v = views[i];
         const ve_frame_config& f = v.frame;
-        DevView& d = c->h_views[i];
+        DevView& d = hv[i];
         std::memset(&d, 0, sizeof(d));
         std::memcpy(d.cam, v.camera, sizeof(d.cam));
         d.scene = uint32_t(v.scene_id);
@@ -949,9 +976,14 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     const bool timing = (flags & VE_FRAME_TIMING) != 0;
     const bool count = (flags & VE_FRAME_COUNT_FETCH) != 0;
     uint32_t launches = 0, trace_launches = 0;
-    VE_CUDA(cudaMemcpyAsync(c->d_views.p, c->h_views, sizeof(DevView) * nv, cudaMemcpyHostToDevice, st));
+    VE_CUDA(cudaMemcpyAsync(c->d_views.p, hv, sizeof(DevView) * nv, cudaMemcpyHostToDevice, st));
+    VE_CUDA(cudaEventRecord(c->staging_ev[slot], st));
+    uint64_t h2d = sizeof(DevView) * nv, d2h = 0;
     VE_CUDA(cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st));
     VE_CUDA(cudaMemsetAsync(c->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), st));
+    // paths of pixels without a primary hit are never spawned: their debug
+    // slots read as zero
+    if (flags & VE_FRAME_PATH_RGB) VE_CUDA(cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st));
     // events: 0 start, 1 after decay, 2 after primary, then per pass
     // (shade, trace) pairs, last = after resolve
     int ne = 0;
@@ -1009,6 +1041,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     k_resolve<<<tiles, 256, 0, st>>>(a);
     launches++;
     rec();
+    k_accum_stats<<<1, 32, 0, st>>>(c->stats.p, c->totals.p);
+    launches++;
     VE_CUDA(cudaGetLastError());
     c->last_launches = launches;
     c->last_trace_launches = trace_launches;
@@ -1026,6 +1060,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         cudaEventElapsedTime(&t, c->ev[ne - 2], c->ev[ne - 1]); c->last.ms_resolve = t;
         cudaEventElapsedTime(&t, c->ev[0], c->ev[ne - 1]); c->last.ms_total = t;
+        c->tot_ms[0] += c->last.ms_total; c->tot_ms[1] += c->last.ms_primary; c->tot_ms[2] += c->last.ms_trace;
+        c->tot_ms[3] += c->last.ms_shade; c->tot_ms[4] += c->last.ms_resolve; c->tot_ms[5] += c->last.ms_decay;
     }
     VE_CUDA(cudaMemcpyAsync(c->h_stats, c->stats.p, ST_TOTAL * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     // host outputs
@@ -1036,18 +1072,27 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             const uint64_t np = uint64_t(f.width) * f.height;
             const uint64_t nq = np * f.spp;
             ve_frame_outputs& o = outs[i];
-            if (o.gbuffer) VE_CUDA(cudaMemcpyAsync(o.gbuffer, c->gbuf.p + pb, np * 16, cudaMemcpyDeviceToHost, st));
-            if (o.voxel_id) VE_CUDA(cudaMemcpyAsync(o.voxel_id, c->out_vid.p + pb, np * 4, cudaMemcpyDeviceToHost, st));
-            if (o.hit_node) VE_CUDA(cudaMemcpyAsync(o.hit_node, c->out_node.p + pb, np * 4, cudaMemcpyDeviceToHost, st));
-            if (o.rgb) VE_CUDA(cudaMemcpyAsync(o.rgb, c->out_rgb.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st));
-            if (o.mapped) VE_CUDA(cudaMemcpyAsync(o.mapped, c->out_mapped.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st));
-            if (o.path_rgb && (f.flags & VE_FRAME_PATH_RGB))
+            if (o.gbuffer) { VE_CUDA(cudaMemcpyAsync(o.gbuffer, c->gbuf.p + pb, np * 16, cudaMemcpyDeviceToHost, st)); d2h += np * 16; }
+            if (o.voxel_id) { VE_CUDA(cudaMemcpyAsync(o.voxel_id, c->out_vid.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
+            if (o.hit_node) { VE_CUDA(cudaMemcpyAsync(o.hit_node, c->out_node.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
+            if (o.rgb) { VE_CUDA(cudaMemcpyAsync(o.rgb, c->out_rgb.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st)); d2h += np * 12; }
+            if (o.mapped) { VE_CUDA(cudaMemcpyAsync(o.mapped, c->out_mapped.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st)); d2h += np * 12; }
+            if (o.path_rgb && (f.flags & VE_FRAME_PATH_RGB)) {
                 VE_CUDA(cudaMemcpyAsync(o.path_rgb, c->path_rgb.p + 3 * qb, nq * 12, cudaMemcpyDeviceToHost, st));
+                d2h += nq * 12;
+            }
             pb += np;
             qb += nq;
         }
         VE_CUDA(cudaStreamSynchronize(st));
     }
+    c->last_h2d = h2d;
+    c->last_d2h = d2h;
+    c->tot_frames++;
+    c->tot_h2d += h2d;
+    c->tot_d2h += d2h;
+    c->tot_launches += launches;
+    c->tot_trace_launches += trace_launches;
     return VE_OK;
 }
 
@@ -1094,12 +1139,16 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
     x->grid_trace_count = x->num_sms * std::max(btc, 1);
     x->grid_shade = x->num_sms * std::max(bs, 1);
     int rc = 0;
-    if ((rc = x->counters.ensure(CNT_TOTAL)) || (rc = x->stats.ensure(ST_TOTAL)) || (rc = x->d_mats.ensure(128))) {
+    for (auto& e : x->staging_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if ((rc = x->counters.ensure(CNT_TOTAL)) || (rc = x->stats.ensure(ST_TOTAL)) ||
+        (rc = x->totals.ensure(ST_TOTAL)) || (rc = x->d_mats.ensure(128))) {
         ve_ctx_destroy(x);
         return rc;
     }
     cudaMallocHost(&x->h_stats, ST_TOTAL * sizeof(unsigned long long));
     cudaMemset(x->d_mats.p, 0, 128 * sizeof(DevMaterial));
+    cudaMemset(x->totals.p, 0, ST_TOTAL * sizeof(unsigned long long));
+    cudaMemset(x->stats.p, 0, ST_TOTAL * sizeof(unsigned long long));
     *out = x;
     return VE_OK;
 }
@@ -1118,7 +1167,11 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->live0.release(); c->live1.release(); c->rayq.release(); c->counters.release(); c->stats.release();
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
     c->out_mapped.release(); c->path_rgb.release();
-    if (c->h_views) cudaFreeHost(c->h_views);
+    for (int k = 0; k < ve_ctx::kStaging; k++) {
+        if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
+        if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
+    }
+    c->totals.release();
     if (c->h_stats) cudaFreeHost(c->h_stats);
     for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1302,11 +1355,7 @@ int ve_render_batch(ve_ctx* c, const ve_view* views, uint32_t n, ve_frame_output
     return render_batch(c, views, n, outs);
 }
 
-int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
-    if (!c || !s) return fail(VE_ERR_INVALID, "get_stats: null argument");
-    VE_CUDA(cudaStreamSynchronize(c->stream));
-    ve_frame_stats r = c->last;
-    const unsigned long long* h = c->h_stats;
+static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
     r.rays_primary = h[ST_RAYS_PRIMARY];
     r.rays_bounce = h[ST_RAYS_BOUNCE];
     r.rays_shadow = h[ST_RAYS_SHADOW];
@@ -1315,6 +1364,48 @@ int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
     r.deposits = h[ST_DEPOSITS];
     r.deposits_dropped = h[ST_DROPPED];
     r.dda_steps = h[ST_STEPS];
+    r.fetch_nodes_trace = h[ST_FETCH_TRACE];
+    r.dda_steps_trace = h[ST_STEPS_TRACE];
+}
+
+int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
+    if (!c || !s) return fail(VE_ERR_INVALID, "get_total_stats: null argument");
+    unsigned long long h[ST_TOTAL];
+    VE_CUDA(cudaMemcpyAsync(h, c->totals.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    ve_frame_stats r{};
+    fill_counters(r, h);
+    r.frames = c->tot_frames;
+    r.h2d_bytes = c->tot_h2d;
+    r.d2h_bytes = c->tot_d2h;
+    r.ms_total = c->tot_ms[0]; r.ms_primary = c->tot_ms[1]; r.ms_trace = c->tot_ms[2];
+    r.ms_shade = c->tot_ms[3]; r.ms_resolve = c->tot_ms[4]; r.ms_decay = c->tot_ms[5];
+    r.kernel_launches = c->tot_launches;
+    r.trace_launches = c->tot_trace_launches;
+    r.cache_capacity = 1ull << c->cfg.hash_log2;
+    *s = r;
+    return VE_OK;
+}
+
+int ve_reset_total_stats(ve_ctx* c) {
+    if (!c) return fail(VE_ERR_INVALID, "reset_total_stats: null context");
+    VE_CUDA(cudaMemsetAsync(c->totals.p, 0, ST_TOTAL * sizeof(unsigned long long), c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    c->tot_frames = c->tot_h2d = c->tot_d2h = 0;
+    c->tot_launches = c->tot_trace_launches = 0;
+    for (float& m : c->tot_ms) m = 0.0f;
+    return VE_OK;
+}
+
+int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
+    if (!c || !s) return fail(VE_ERR_INVALID, "get_stats: null argument");
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    ve_frame_stats r = c->last;
+    const unsigned long long* h = c->h_stats;
+    fill_counters(r, h);
+    r.frames = 1;
+    r.h2d_bytes = c->last_h2d;
+    r.d2h_bytes = c->last_d2h;
     r.kernel_launches = c->last_launches;
     r.trace_launches = c->last_trace_launches;
     r.cache_capacity = 1ull << c->cfg.hash_log2;
