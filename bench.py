@@ -172,7 +172,7 @@ def run_reference(args, W, rank, world):
     mats = ve.terrain_materials(W.seed)
     orc = Oracle()
     # normals as the device pass computes them (3x3x3 occupancy gradient)
-    words = _words_with_normals(ve, words, W.depth)
+    words = _words_with_normals(orc, words, W.depth)
     threads = os.cpu_count() or 1
     rr = OracleRenderer(orc)
     rows_per_step = max(threads, 16)
@@ -212,16 +212,15 @@ def rays_of_oracle(s):
     return s["rays_primary"] + s["rays_bounce"] + s["rays_shadow"]
 
 
-def _words_with_normals(ve, words, depth):
-    with ve.Renderer(hash_log2=8) as r:
-        sid = r.upload_scene(words, depth)
-        return r.download_scene(sid)
+def _words_with_normals(orc, words, depth):
+    """Leaf normals filled on the CPU by the oracle (bitmask occupancy)."""
+    return orc.fill_normals(words, depth, fast=True, threads=os.cpu_count() or 1)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

@@ -62,6 +62,7 @@ class Oracle:
         L.oracle_build.restype = _U64
         L.oracle_build.argtypes = [_U32, _np(np.uint32), _U64, _np(np.uint32), _U64, ctypes.POINTER(_U32)]
         L.oracle_fill_normals.argtypes = [_np(np.uint32), _U64, _U32]
+        L.oracle_fill_normals_mode.argtypes = [_np(np.uint32), _U64, _U32, ctypes.c_int, _U32]
         L.oracle_lookup_occupied.restype = ctypes.c_int
         L.oracle_lookup_occupied.argtypes = [_np(np.uint32), _U64, _U32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int64]
@@ -94,9 +95,11 @@ class Oracle:
         self.lib.oracle_build(depth, v, n, out, size, ctypes.byref(nv))
         return out
 
-    def fill_normals(self, words: np.ndarray, depth: int) -> np.ndarray:
+    def fill_normals(self, words: np.ndarray, depth: int, fast: bool = False, threads: int = 1) -> np.ndarray:
+        """Leaf normal fields by tree-descent occupancy lookups, or (fast) by
+        an occupancy bitmask of all leaves."""
         w = np.ascontiguousarray(words, np.uint32).copy()
-        self.lib.oracle_fill_normals(w, w.size, depth)
+        self.lib.oracle_fill_normals_mode(w, w.size, depth, 1 if fast else 0, threads)
         return w
 
     def occupied(self, words, depth, x, y, z) -> bool:

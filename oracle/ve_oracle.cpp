@@ -483,9 +483,37 @@ struct CacheEntry {
     uint64_t count = 0;
     double weight = 0, r = 0, g = 0, b = 0, l2 = 0;
 };
+// Sharded by vid so the merge and the decay run in parallel; within a
+// shard, deposits merge in (thread, row) order: deterministic.
+constexpr uint32_t kShards = 64;
+inline uint32_t shard_of(uint32_t vid) { return hash32(vid) & (kShards - 1); }
 struct Cache {
-    std::unordered_map<uint32_t, CacheEntry> map;
+    std::unordered_map<uint32_t, CacheEntry> map[kShards];
+    const CacheEntry* find(uint32_t vid) const {
+        const auto& m = map[shard_of(vid)];
+        auto it = m.find(vid);
+        return it == m.end() ? nullptr : &it->second;
+    }
+    size_t size() const {
+        size_t n = 0;
+        for (const auto& m : map) n += m.size();
+        return n;
+    }
 };
+
+template <typename F>
+void run_parallel(uint32_t n, uint32_t threads, F&& fn) {
+    if (threads <= 1) {
+        for (uint32_t i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < threads; t++)
+        th.emplace_back([&, t] {
+            for (uint32_t i = t; i < n; i += threads) fn(i);
+        });
+    for (auto& x : th) x.join();
+}
 
 struct Deposit {
     uint32_t vid;
@@ -608,9 +636,9 @@ struct Avg {
 Avg lookup_avg(const Cache& c, uint32_t vid) {
     Avg a{{0, 0, 0}, 0, 0};
     if (vid == 0) return a;
-    auto it = c.map.find(vid);
-    if (it == c.map.end()) return a;
-    const CacheEntry& e = it->second;
+    const CacheEntry* ep = c.find(vid);
+    if (!ep) return a;
+    const CacheEntry& e = *ep;
     a.count = e.count;
     if (e.count == 0 || e.weight <= 0.0) return a;
     const double inv = 1.0 / e.weight;
@@ -655,12 +683,16 @@ uint64_t oracle_build(uint32_t depth, const uint32_t* xyzm, uint64_t n, uint32_t
 
 // normal.comp restated over the 3x3x3 neighbourhood; writes the normal field
 // into every leaf word of `words` (in place).  Leaves are found by walking
-// the tree from the root.
-void oracle_fill_normals(uint32_t* words, uint64_t n, uint32_t depth) {
+// the tree from the root.  mode 0: every neighbour occupancy by a tree
+// descent (lookupOccupied, normal.comp:55-70); mode 1: the same occupancy
+// read from a bitmask of all leaves (identical on valid trees, fast enough
+// for depth-10 scenes), with `threads` workers.
+void oracle_fill_normals_mode(uint32_t* words, uint64_t n, uint32_t depth, int mode, uint32_t threads) {
     std::vector<uint32_t> copy(words, words + n);
     Scene s{copy.data(), n, depth};
     const uint32_t L = 1u << depth;
     struct E { uint32_t off, level, x, y, z; };
+    std::vector<E> leaves;
     std::vector<E> st;
     // root block: slots 1..8 are the root's children at CPU level 2
     for (uint32_t i = 0; i < 8; i++) {
@@ -672,24 +704,57 @@ void oracle_fill_normals(uint32_t* words, uint64_t n, uint32_t depth) {
         st.pop_back();
         const uint32_t raw = s.fetch(e.off);
         if (raw & 1u) {
+            if (e.level >= depth) continue;
             const uint32_t next = node_next(raw);
             const uint32_t half = L >> (e.level + 1);
             for (uint32_t i = 0; i < 8; i++)
                 st.push_back({next + i, e.level + 1, e.x + ((i & 4) ? half : 0u), e.y + ((i & 2) ? half : 0u),
                               e.z + ((i & 1) ? half : 0u)});
         } else if (node_material(raw) != 0u && e.level == depth) {
+            leaves.push_back(e);
+        }
+    }
+    std::vector<uint64_t> bits;
+    if (mode == 1) {
+        bits.assign(((uint64_t(1) << (3 * depth)) + 63) / 64, 0ull);
+        for (const E& e : leaves) {
+            const uint64_t b = ((uint64_t(e.z) << depth | e.y) << depth) | e.x;
+            bits[b >> 6] |= 1ull << (b & 63);
+        }
+    }
+    auto occupied = [&](int64_t x, int64_t y, int64_t z) {
+        if (mode == 0) return lookup_occupied(s, x, y, z);
+        if (x < 0 || y < 0 || z < 0 || x >= L || y >= L || z >= L) return false;
+        const uint64_t b = ((uint64_t(z) << depth | uint64_t(y)) << depth) | uint64_t(x);
+        return bool((bits[b >> 6] >> (b & 63)) & 1u);
+    };
+    auto work = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; i++) {
+            const E& e = leaves[i];
             int ax = 0, ay = 0, az = 0;
             for (int dx = -1; dx <= 1; dx++)
                 for (int dy = -1; dy <= 1; dy++)
                     for (int dz = -1; dz <= 1; dz++) {
                         if (dx == 0 && dy == 0 && dz == 0) continue;
-                        if (!lookup_occupied(s, int64_t(e.x) + dx, int64_t(e.y) + dy, int64_t(e.z) + dz)) {
+                        if (!occupied(int64_t(e.x) + dx, int64_t(e.y) + dy, int64_t(e.z) + dz)) {
                             ax += dx; ay += dy; az += dz;
                         }
                     }
-            words[e.off] = (raw & 0xFFu) | encode_normal_field(ax, ay, az);
+            words[e.off] = (copy[e.off] & 0xFFu) | encode_normal_field(ax, ay, az);
         }
+    };
+    if (threads <= 1) {
+        work(0, leaves.size());
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < threads; t++)
+            th.emplace_back(work, leaves.size() * t / threads, leaves.size() * (t + 1) / threads);
+        for (auto& x : th) x.join();
     }
+}
+
+void oracle_fill_normals(uint32_t* words, uint64_t n, uint32_t depth) {
+    oracle_fill_normals_mode(words, n, depth, 0, 1);
 }
 
 int oracle_lookup_occupied(const uint32_t* words, uint64_t n, uint32_t depth, int64_t x, int64_t y, int64_t z) {
@@ -753,12 +818,13 @@ uint64_t oracle_cache_dump(void* rp, uint32_t* vids, uint64_t* counts, double* v
     Renderer* r = static_cast<Renderer*>(rp);
     uint64_t i = 0;
     std::vector<uint32_t> keys;
-    keys.reserve(r->cache.map.size());
-    for (auto& kv : r->cache.map) keys.push_back(kv.first);
+    keys.reserve(r->cache.size());
+    for (auto& m : r->cache.map)
+        for (auto& kv : m) keys.push_back(kv.first);
     std::sort(keys.begin(), keys.end());
     for (uint32_t k : keys) {
         if (i >= cap) break;
-        const CacheEntry& e = r->cache.map[k];
+        const CacheEntry& e = *r->cache.find(k);
         if (vids) vids[i] = k;
         if (counts) counts[i] = e.count;
         if (values) {
@@ -778,7 +844,7 @@ uint64_t oracle_cache_dump(void* rp, uint32_t* vids, uint64_t* counts, double* v
 //   3 AccumPass: decay then deposit into the FP64 cache (fixed merge order)
 //   4 AvgPass + tonemap per pixel (resolve.comp:362-382, final.frag:11-18)
 // Rows [row_begin, row_end) are rendered (all rows when row_end == 0) with
-// `threads` std::threads, one contiguous row band each.  gbuf: 4 u32 per
+// `threads` std::threads, rows interleaved across threads.  gbuf: 4 u32 per
 // pixel; rgb, mapped: 3 f32 per pixel (null to skip).  Paths' per-sample
 // values are written to `path_rgb` (3 f32 per path, index pix*spp+s) when
 // non-null.
@@ -795,27 +861,30 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     if (threads == 0) threads = 1;
 
     // temporal decay of the cache before this frame's deposits
-    for (auto& kv : R->cache.map) {
-        CacheEntry& e = kv.second;
-        const double k = P->decay;
-        e.weight *= k; e.r *= k; e.g *= k; e.b *= k; e.l2 *= k;
-    }
+    run_parallel(kShards, threads, [&](uint32_t sh) {
+        for (auto& kv : R->cache.map[sh]) {
+            CacheEntry& e = kv.second;
+            const double k = P->decay;
+            e.weight *= k; e.r *= k; e.g *= k; e.b *= k; e.l2 *= k;
+        }
+    });
 
     const f3 cpos = mk(cam[0], cam[1], cam[2]);
     const f3 plane = mk(cam[4], cam[5], cam[6]);
     const f3 right = mk(cam[8], cam[9], cam[10]);
     const f3 up = mk(cam[12], cam[13], cam[14]);
 
-    std::vector<std::vector<Deposit>> deps(threads);
+    std::vector<std::vector<std::vector<Deposit>>> deps(threads, std::vector<std::vector<Deposit>>(kShards));
     std::vector<ov_stats> tstats(threads);
     std::vector<RayCounters> trc(threads);
     const uint32_t rows = row_end - row_begin;
+    // static interleaved rows (row r -> thread r mod threads): balanced and
+    // deterministic; deposits merge in thread order below
+    (void)rows;
     auto work = [&](uint32_t t) {
-        const uint32_t r0 = row_begin + uint32_t(uint64_t(rows) * t / threads);
-        const uint32_t r1 = row_begin + uint32_t(uint64_t(rows) * (t + 1) / threads);
         ov_stats& st = tstats[t];
         std::memset(&st, 0, sizeof(st));
-        for (uint32_t py = r0; py < r1; py++) {
+        for (uint32_t py = row_begin + t; py < row_end; py += threads) {
             for (uint32_t px = 0; px < W; px++) {
                 // pixel -> ray (generate_primary.comp:44-52)
                 const float ndx = (float(px) + 0.5f) / float(W) * 2.0f - 1.0f;
@@ -844,7 +913,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                         float* o = path_rgb + 3 * (uint64_t(pix) * P->spp + smp);
                         o[0] = dp.rgb[0]; o[1] = dp.rgb[1]; o[2] = dp.rgb[2];
                     }
-                    deps[t].push_back(dp);
+                    deps[t][shard_of(vid)].push_back(dp);
                 }
             }
         }
@@ -865,17 +934,20 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         total.fetch_restart += trc[t].fetch_restart;
         total.fetch_min += trc[t].fetch_min;
         total.steps += trc[t].steps;
-        for (const Deposit& d : deps[t]) {
-            CacheEntry& e = R->cache.map[d.vid];
-            const double r = d.rgb[0], g = d.rgb[1], b = d.rgb[2];
-            const float Lf = ((d.rgb[0] + d.rgb[1]) + d.rgb[2]) / 3.0f;
-            e.count += 1;
-            e.weight += 1.0;
-            e.r += r; e.g += g; e.b += b;
-            e.l2 += double(Lf * Lf);
-            total.deposits++;
-        }
+        for (uint32_t sh = 0; sh < kShards; sh++) total.deposits += deps[t][sh].size();
     }
+    run_parallel(kShards, threads, [&](uint32_t sh) {
+        auto& m = R->cache.map[sh];
+        for (uint32_t t = 0; t < threads; t++)
+            for (const Deposit& d : deps[t][sh]) {
+                CacheEntry& e = m[d.vid];
+                const float Lf = ((d.rgb[0] + d.rgb[1]) + d.rgb[2]) / 3.0f;
+                e.count += 1;
+                e.weight += 1.0;
+                e.r += double(d.rgb[0]); e.g += double(d.rgb[1]); e.b += double(d.rgb[2]);
+                e.l2 += double(Lf * Lf);
+            }
+    });
 
     // AvgPass (resolve.comp main :362-382 with resolveDefault :224-261,
     // reconstructTimeout :193-219, and the visualisation modes :266-359)

@@ -822,9 +822,19 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
-    cudaEvent_t ev[48] = {};
+    // per-frame CUDA-event sets in a ring: elapsed times are read when the
+    // slot is reused or the stats are queried, so timed frames never wait
+    static constexpr int kTimingSlots = 16, kEvents = 48;
+    struct TimingSlot {
+        cudaEvent_t ev[kEvents] = {};
+        int n = 0;            // events recorded
+        uint32_t passes = 0;  // shade passes
+        bool pending = false;
+    } timing[kTimingSlots];
+    int timing_next = 0;
     ve_frame_stats last{};
     bool last_timing = false;
+    int last_timing_slot = -1;
     uint32_t last_launches = 0, last_trace_launches = 0;
 };
 
@@ -911,6 +921,45 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
     return VE_OK;
 }
 
+// Reads one frame's event set (waits for its last event) and adds it to the
+// running totals; `out` receives the frame's own stage times when non-null.
+static void collect_timing(ve_ctx* c, ve_ctx::TimingSlot& ts, ve_frame_stats* out) {
+    if (!ts.pending) return;
+    cudaEventSynchronize(ts.ev[ts.n - 1]);
+    ve_frame_stats f{};
+    float t = 0;
+    cudaEventElapsedTime(&t, ts.ev[0], ts.ev[1]); f.ms_decay = t;
+    cudaEventElapsedTime(&t, ts.ev[1], ts.ev[2]); f.ms_primary = t;
+    for (uint32_t pass = 0; pass < ts.passes; pass++) {
+        const int e0 = 2 + 2 * int(pass);
+        cudaEventElapsedTime(&t, ts.ev[e0], ts.ev[e0 + 1]); f.ms_shade += t;
+        cudaEventElapsedTime(&t, ts.ev[e0 + 1], ts.ev[e0 + 2]); f.ms_trace += t;
+    }
+    cudaEventElapsedTime(&t, ts.ev[ts.n - 2], ts.ev[ts.n - 1]); f.ms_resolve = t;
+    cudaEventElapsedTime(&t, ts.ev[0], ts.ev[ts.n - 1]); f.ms_total = t;
+    c->tot_ms[0] += f.ms_total; c->tot_ms[1] += f.ms_primary; c->tot_ms[2] += f.ms_trace;
+    c->tot_ms[3] += f.ms_shade; c->tot_ms[4] += f.ms_resolve; c->tot_ms[5] += f.ms_decay;
+    ts.pending = false;
+    if (out) {
+        out->ms_total = f.ms_total; out->ms_primary = f.ms_primary; out->ms_trace = f.ms_trace;
+        out->ms_shade = f.ms_shade; out->ms_resolve = f.ms_resolve; out->ms_decay = f.ms_decay;
+    }
+}
+
+static void collect_all_timing(ve_ctx* c) {
+    for (int i = 0; i < ve_ctx::kTimingSlots; i++) {
+        const int k = (c->timing_next + i) % ve_ctx::kTimingSlots;
+        if (c->timing[k].pending) {
+            ve_frame_stats f{};
+            collect_timing(c, c->timing[k], &f);
+            if (k == c->last_timing_slot) {
+                c->last.ms_total = f.ms_total; c->last.ms_primary = f.ms_primary; c->last.ms_trace = f.ms_trace;
+                c->last.ms_shade = f.ms_shade; c->last.ms_resolve = f.ms_resolve; c->last.ms_decay = f.ms_decay;
+            }
+        }
+    }
+}
+
 static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_outputs* outs) {
     if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "render: no views");
     if (nv > 65535u) return fail(VE_ERR_INVALID, "render: at most 65535 views per batch");
@@ -986,9 +1035,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (flags & VE_FRAME_PATH_RGB) VE_CUDA(cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st));
     // events: 0 start, 1 after decay, 2 after primary, then per pass
     // (shade, trace) pairs, last = after resolve
+    ve_ctx::TimingSlot* ts = nullptr;
+    if (timing) {
+        ts = &c->timing[c->timing_next];
+        c->timing_next = (c->timing_next + 1) % ve_ctx::kTimingSlots;
+        if (ts->pending) collect_timing(c, *ts, nullptr);
+    }
     int ne = 0;
     auto rec = [&]() {
-        if (timing) cudaEventRecord(c->ev[ne], st);
+        if (timing) cudaEventRecord(ts->ev[ne], st);
         ne++;
     };
     rec();
@@ -1049,19 +1104,12 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     c->last_timing = timing;
     std::memset(&c->last, 0, sizeof(c->last));
     if (timing) {
-        cudaEventSynchronize(c->ev[ne - 1]);
-        float t = 0;
-        cudaEventElapsedTime(&t, c->ev[0], c->ev[1]); c->last.ms_decay = t;
-        cudaEventElapsedTime(&t, c->ev[1], c->ev[2]); c->last.ms_primary = t;
-        for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
-            const int e0 = 2 + 2 * int(pass);
-            cudaEventElapsedTime(&t, c->ev[e0], c->ev[e0 + 1]); c->last.ms_shade += t;
-            cudaEventElapsedTime(&t, c->ev[e0 + 1], c->ev[e0 + 2]); c->last.ms_trace += t;
-        }
-        cudaEventElapsedTime(&t, c->ev[ne - 2], c->ev[ne - 1]); c->last.ms_resolve = t;
-        cudaEventElapsedTime(&t, c->ev[0], c->ev[ne - 1]); c->last.ms_total = t;
-        c->tot_ms[0] += c->last.ms_total; c->tot_ms[1] += c->last.ms_primary; c->tot_ms[2] += c->last.ms_trace;
-        c->tot_ms[3] += c->last.ms_shade; c->tot_ms[4] += c->last.ms_resolve; c->tot_ms[5] += c->last.ms_decay;
+        ts->n = ne;
+        ts->passes = max_b + 2u;
+        ts->pending = true;
+        c->last_timing_slot = int(ts - c->timing);
+    } else {
+        c->last_timing_slot = -1;
     }
     VE_CUDA(cudaMemcpyAsync(c->h_stats, c->stats.p, ST_TOTAL * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     // host outputs
@@ -1130,7 +1178,8 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
         delete x;
         return fail(VE_ERR_CUDA, "ctx_create: stream creation failed");
     }
-    for (auto& e : x->ev) cudaEventCreate(&e);
+    for (auto& slot : x->timing)
+        for (auto& e : slot.ev) cudaEventCreate(&e);
     int bt = 0, btc = 0, bs = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);
@@ -1173,7 +1222,9 @@ int ve_ctx_destroy(ve_ctx* c) {
     }
     c->totals.release();
     if (c->h_stats) cudaFreeHost(c->h_stats);
-    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+    for (auto& slot : c->timing)
+        for (auto& e : slot.ev)
+            if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return VE_OK;
@@ -1373,6 +1424,7 @@ int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
     unsigned long long h[ST_TOTAL];
     VE_CUDA(cudaMemcpyAsync(h, c->totals.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    collect_all_timing(c);
     ve_frame_stats r{};
     fill_counters(r, h);
     r.frames = c->tot_frames;
@@ -1391,6 +1443,7 @@ int ve_reset_total_stats(ve_ctx* c) {
     if (!c) return fail(VE_ERR_INVALID, "reset_total_stats: null context");
     VE_CUDA(cudaMemsetAsync(c->totals.p, 0, ST_TOTAL * sizeof(unsigned long long), c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    collect_all_timing(c);
     c->tot_frames = c->tot_h2d = c->tot_d2h = 0;
     c->tot_launches = c->tot_trace_launches = 0;
     for (float& m : c->tot_ms) m = 0.0f;
@@ -1400,6 +1453,7 @@ int ve_reset_total_stats(ve_ctx* c) {
 int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
     if (!c || !s) return fail(VE_ERR_INVALID, "get_stats: null argument");
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    collect_all_timing(c);
     ve_frame_stats r = c->last;
     const unsigned long long* h = c->h_stats;
     fill_counters(r, h);
