@@ -218,6 +218,31 @@ int ve_get_stats(ve_ctx* ctx, ve_frame_stats* stats);
 int ve_get_total_stats(ve_ctx* ctx, ve_frame_stats* stats);
 int ve_reset_total_stats(ve_ctx* ctx);
 
+/* ======================================================================
+ * Allocation-free entry point (no counterpart in the reference)
+ * ==================================================================== */
+
+/* Fills the normal field of every leaf of a node array that already lives in
+ * device memory (the same 3x3x3 occupancy-gradient pass ve_scene_upload runs),
+ * without allocating anything.  It exists for callers that may not call
+ * cudaMalloc: hosts that own the whole device-memory budget (an engine's or a
+ * service's arena) and forbid libraries from allocating behind them, and
+ * latency-critical threads that cannot afford cudaMalloc/cudaFree stalling the
+ * device.  The caller passes the device node array; the work is enqueued on
+ * `stream` (a cudaStream_t, NULL = default stream) and is complete when the
+ * stream reaches it.
+ *
+ * Scratch: a fixed file-scope device array of VE_NOALLOC_SCRATCH_BYTES
+ * (frontiers + occupancy bitmask), present on every GPU that loads the
+ * library until the process exits, which limits the scene to depth <= 7
+ * (VE_ERR_CAPACITY beyond).  The first call on a device looks up that array's
+ * device address with the device current; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (on different streams, or from several threads) race on it. */
+#define VE_NOALLOC_MAX_DEPTH 7
+#define VE_NOALLOC_SCRATCH_BYTES (256u + 2u * (1u << 18) * 8u + (1u << 21) / 8u)
+int ve_fill_normals_noalloc(uint32_t* device_words, uint64_t n_words, uint32_t depth, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -138,6 +138,7 @@ _SIGNATURES = {
     "ve_render_batch": ([_P, _PTR(ViewC), _U32, _P], ctypes.c_int),
     "ve_get_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
     "ve_get_total_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
+    "ve_fill_normals_noalloc": ([_P, _U64, _U32, _P], ctypes.c_int),
     "ve_reset_total_stats": ([_P], ctypes.c_int),
 }
 

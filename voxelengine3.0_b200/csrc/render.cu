@@ -740,6 +740,26 @@ __global__ void __launch_bounds__(256) k_leaf_pass(uint32_t* nodes, uint64_t n_w
 }
 
 // ---------------------------------------------------------------------------
+// allocation-free leaf normal pass: its scratch lives in this fixed device
+// array (the frontiers and the occupancy bitmask of a depth <= 7 scene),
+// held by every GPU that loads the library until the process exits
+// ---------------------------------------------------------------------------
+constexpr uint32_t kNoAllocMaxDepth = 7;
+constexpr uint64_t kNoAllocFrontier = 1ull << 18;  // 64^3: every size-2 cell of a depth-7 scene
+constexpr uint64_t kNoAllocOccWords = (1ull << (3 * kNoAllocMaxDepth)) / 32;
+constexpr size_t kNoAllocCounterBytes = 256;
+constexpr size_t kNoAllocBytes = kNoAllocCounterBytes + 2 * kNoAllocFrontier * 8 + kNoAllocOccWords * 4;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// seeds the root frontier entry (slot 0, origin 0) and its count
+__global__ void k_noalloc_seed(uint32_t* counters, unsigned long long* frontier) {
+    if (threadIdx.x == 0) {
+        counters[0] = 1u;
+        frontier[0] = 0ull;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 static thread_local std::string g_err;
@@ -1464,6 +1484,62 @@ int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
     r.trace_launches = c->last_trace_launches;
     r.cache_capacity = 1ull << c->cfg.hash_log2;
     *s = r;
+    return VE_OK;
+}
+
+// Allocation-free variant of the leaf normal pass (see include/ve.h).  The
+// scratch is the file-scope g_noalloc_scratch; its device address is looked up
+// once per device (first call on that device, with that device current).
+static void* g_noalloc_ptr[64] = {};
+static std::mutex g_noalloc_mu;
+
+int ve_fill_normals_noalloc(uint32_t* words, uint64_t n_words, uint32_t depth, void* stream) {
+    if (!words) return fail(VE_ERR_INVALID, "fill_normals_noalloc: null node array");
+    if (n_words < 9 || n_words >= (1ull << 32))
+        return fail(VE_ERR_INVALID, "fill_normals_noalloc: n_words must be in [9, 2^32)");
+    if (depth < 1 || depth > kNoAllocMaxDepth)
+        return fail(VE_ERR_CAPACITY, "fill_normals_noalloc: depth must be in [1, 7] (fixed device scratch of " +
+                                         std::to_string(kNoAllocBytes) + " bytes)");
+    int dev = 0;
+    VE_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(VE_ERR_INVALID, "fill_normals_noalloc: device index out of range");
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return fail(VE_ERR_CUDA, std::string("fill_normals_noalloc: cudaGetSymbolAddress: ") +
+                                             cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = p;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(base);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(b);
+    unsigned long long* fa = reinterpret_cast<unsigned long long*>(b + kNoAllocCounterBytes);
+    unsigned long long* fb = fa + kNoAllocFrontier;
+    uint32_t* occ = reinterpret_cast<uint32_t*>(fb + kNoAllocFrontier);
+    // the array keeps the previous call's contents: clear counters and bitmask
+    VE_CUDA(cudaMemsetAsync(cnt, 0, kNoAllocCounterBytes, st));
+    VE_CUDA(cudaMemsetAsync(occ, 0, ((1ull << (3 * depth)) + 31) / 32 * 4, st));
+    k_noalloc_seed<<<1, 32, 0, st>>>(cnt, fa);
+    int n_sms = 148;
+    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = n_sms * 8;
+    unsigned long long* in = fa;
+    unsigned long long* out = fb;
+    for (uint32_t k = 0; k + 1 < depth; k++) {
+        k_expand<<<grid, 256, 0, st>>>(words, n_words, depth, k, in, cnt + k, out, cnt + k + 1,
+                                        uint32_t(kNoAllocFrontier));
+        std::swap(in, out);
+    }
+    const uint32_t* lc = cnt + (depth - 1);
+    k_leaf_pass<<<grid, 256, 0, st>>>(words, n_words, depth, in, lc, occ, 0, uint32_t(kNoAllocFrontier));
+    k_leaf_pass<<<grid, 256, 0, st>>>(words, n_words, depth, in, lc, occ, 1, uint32_t(kNoAllocFrontier));
+    VE_CUDA(cudaGetLastError());
     return VE_OK;
 }
 
