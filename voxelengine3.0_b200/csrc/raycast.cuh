@@ -28,100 +28,133 @@ __device__ __forceinline__ uint32_t fetch_node(const uint32_t* __restrict__ node
     return off < n ? __ldg(nodes + off) : 0u;
 }
 
-template <bool COUNT>
-__device__ __forceinline__ Hit raycast(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, f3 o, f3 d,
-                                       uint32_t controlchecks, RayCount& rc) {
-    const uint32_t L = 1u << D;
-    const float Lf = float(L);
-    Hit h;
+// The DDA as a resumable state machine: dda_init performs the origin advance
+// and the entry intersection, dda_step one iteration of the reference loop
+// `while (inBounds(r_pos) && q++ <= controlchecks)`.  Both return true when
+// the ray is finished, with the result in `h`.
+struct Dda {
+    f3 o, d, inv, r;
+    uint32_t q, cc;
+    uint32_t lux, luy, luz, e_last;
+    bool first;
+    uint32_t base[17];
+};
+
+__device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlchecks, uint32_t D, Hit& h) {
+    const float Lf = float(1u << D);
     h.status = kEscaped;
     h.id = 0;
     h.material = 0;
     h.x = h.y = h.z = 0;
     h.size = 0;
-    const f3 inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    o = add(o, muls(d, 4.0f));
-    uint32_t q = 0;
-    f3 r;
-    if (in_bounds(o, Lf)) {
-        r = o;
+    s.inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    s.d = d;
+    s.o = add(o, muls(d, 4.0f));
+    s.q = 0;
+    s.cc = controlchecks;
+    s.base[0] = 0u;
+    s.lux = s.luy = s.luz = s.e_last = 0;
+    s.first = true;
+    if (in_bounds(s.o, Lf)) {
+        s.r = s.o;
     } else {
-        const f3 t1 = mul(mk((0.0f - o.x) + 0.001f, (0.0f - o.y) + 0.001f, (0.0f - o.z) + 0.001f), inv);
-        const f3 t2 = mul(mk((Lf - o.x) - 0.001f, (Lf - o.y) - 0.001f, (Lf - o.z) - 0.001f), inv);
+        const f3 t1 = mul(mk((0.0f - s.o.x) + 0.001f, (0.0f - s.o.y) + 0.001f, (0.0f - s.o.z) + 0.001f), s.inv);
+        const f3 t2 = mul(mk((Lf - s.o.x) - 0.001f, (Lf - s.o.y) - 0.001f, (Lf - s.o.z) - 0.001f), s.inv);
         const float t_enter = gmax(gmax(gmin(t1.x, t2.x), gmin(t1.y, t2.y)), gmin(t1.z, t2.z));
         const float t_exit = gmin(gmin(gmax(t1.x, t2.x), gmax(t1.y, t2.y)), gmax(t1.z, t2.z));
-        q++;
+        s.q++;
         if (t_exit < t_enter || t_exit < 0.0f) {
-            h.checks = q;
-            return h;
+            h.checks = s.q;
+            return true;
         }
-        r = add(muls(d, t_enter), o);
+        s.r = add(muls(d, t_enter), s.o);
     }
-    uint32_t base[17];
-    base[0] = 0u;
-    uint32_t lux = 0, luy = 0, luz = 0, e_last = 0;
-    bool first = true;
-    while (in_bounds(r, Lf) && q++ <= controlchecks) {
-        if (COUNT) rc.steps++;
-        const uint32_t ux = uint32_t(r.x), uy = uint32_t(r.y), uz = uint32_t(r.z);
-        bool reuse = false;
-        uint32_t start = 0;
-        if (!first) {
-            const uint32_t xd = (ux ^ lux) | (uy ^ luy) | (uz ^ luz);
-            if (xd == 0u) {
-                reuse = true;
-            } else {
-                const uint32_t hb = 31u - uint32_t(__clz(xd));
-                start = hb >= D ? 0u : D - hb;
-                reuse = start > e_last;
-            }
-        }
-        uint32_t k = e_last;
-        if (!reuse) {
-            first = false;
-            lux = ux; luy = uy; luz = uz;
-            bool found = false;
-            uint32_t off = 0;
-            for (k = start; k < D; k++) {
-                off = base[k] + locate(ux, uy, uz, L >> k);
-                const uint32_t raw = fetch_node(nodes, n_words, off);
-                if (COUNT) rc.fetch++;
-                if (!(raw & 1u)) {
-                    found = true;
-                    break;
-                }
-                base[k + 1] = raw >> 4;
-            }
-            e_last = k;
-            if (!found) {
-                off = base[D] + locate(ux, uy, uz, 1u);
-                const uint32_t raw = fetch_node(nodes, n_words, off);
-                if (COUNT) rc.fetch++;
-                const uint32_t mat = (raw & 254u) >> 1;
-                if (mat != 0u) {
-                    h.status = kHit;
-                    h.id = off;
-                    h.material = mat;
-                    h.x = ux; h.y = uy; h.z = uz;
-                    h.size = 1u;
-                    h.checks = q;
-                    return h;
-                }
-            }
-        }
-        const uint32_t size = L >> k;
-        const uint32_t px = ux & ~(size - 1u), py = uy & ~(size - 1u), pz = uz & ~(size - 1u);
-        const f3 bmin = mk(float(px), float(py), float(pz));
-        const float fs = float(size);
-        const f3 t1 = mul(mk((bmin.x - o.x) - 0.001f, (bmin.y - o.y) - 0.001f, (bmin.z - o.z) - 0.001f), inv);
-        const f3 t2 = mul(mk(((bmin.x + fs) - o.x) + 0.001f, ((bmin.y + fs) - o.y) + 0.001f,
-                             ((bmin.z + fs) - o.z) + 0.001f),
-                          inv);
-        const float t_exit = gmin(gmin(gmax(t1.x, t2.x), gmax(t1.y, t2.y)), gmax(t1.z, t2.z));
-        r = add(muls(d, t_exit), o);
+    return false;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                         Hit& h, RayCount& rc) {
+    const uint32_t L = 1u << D;
+    const float Lf = float(L);
+    if (!in_bounds(s.r, Lf)) {
+        h.status = kEscaped;
+        h.checks = s.q;
+        return true;
     }
-    h.status = in_bounds(r, Lf) ? kTimeout : kEscaped;
-    h.checks = q;
+    if (!(s.q++ <= s.cc)) {
+        h.status = kTimeout;
+        h.checks = s.q;
+        return true;
+    }
+    if (COUNT) rc.steps++;
+    const uint32_t ux = uint32_t(s.r.x), uy = uint32_t(s.r.y), uz = uint32_t(s.r.z);
+    bool reuse = false;
+    uint32_t start = 0;
+    if (!s.first) {
+        const uint32_t xd = (ux ^ s.lux) | (uy ^ s.luy) | (uz ^ s.luz);
+        if (xd == 0u) {
+            reuse = true;
+        } else {
+            const uint32_t hb = 31u - uint32_t(__clz(xd));
+            start = hb >= D ? 0u : D - hb;
+            reuse = start > s.e_last;
+        }
+    }
+    uint32_t k = s.e_last;
+    if (!reuse) {
+        s.first = false;
+        s.lux = ux; s.luy = uy; s.luz = uz;
+        bool found = false;
+        uint32_t off = 0;
+        for (k = start; k < D; k++) {
+            off = s.base[k] + locate(ux, uy, uz, L >> k);
+            const uint32_t raw = fetch_node(nodes, n_words, off);
+            if (COUNT) rc.fetch++;
+            if (!(raw & 1u)) {
+                found = true;
+                break;
+            }
+            s.base[k + 1] = raw >> 4;
+        }
+        s.e_last = k;
+        if (!found) {
+            off = s.base[D] + locate(ux, uy, uz, 1u);
+            const uint32_t raw = fetch_node(nodes, n_words, off);
+            if (COUNT) rc.fetch++;
+            const uint32_t mat = (raw & 254u) >> 1;
+            if (mat != 0u) {
+                h.status = kHit;
+                h.id = off;
+                h.material = mat;
+                h.x = ux; h.y = uy; h.z = uz;
+                h.size = 1u;
+                h.checks = s.q;
+                return true;
+            }
+        }
+    }
+    const uint32_t size = L >> k;
+    const uint32_t px = ux & ~(size - 1u), py = uy & ~(size - 1u), pz = uz & ~(size - 1u);
+    const f3 bmin = mk(float(px), float(py), float(pz));
+    const float fs = float(size);
+    const f3 t1 = mul(mk((bmin.x - s.o.x) - 0.001f, (bmin.y - s.o.y) - 0.001f, (bmin.z - s.o.z) - 0.001f), s.inv);
+    const f3 t2 = mul(mk(((bmin.x + fs) - s.o.x) + 0.001f, ((bmin.y + fs) - s.o.y) + 0.001f,
+                         ((bmin.z + fs) - s.o.z) + 0.001f),
+                      s.inv);
+    const float t_exit = gmin(gmin(gmax(t1.x, t2.x), gmax(t1.y, t2.y)), gmax(t1.z, t2.z));
+    s.r = add(muls(s.d, t_exit), s.o);
+    return false;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ Hit raycast(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, f3 o, f3 d,
+                                       uint32_t controlchecks, RayCount& rc) {
+    Dda s;
+    Hit h;
+    if (dda_init(s, o, d, controlchecks, D, h)) return h;
+    while (!dda_step<COUNT>(s, nodes, n_words, D, h, rc)) {
+    }
     return h;
 }
 

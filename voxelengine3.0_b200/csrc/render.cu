@@ -74,7 +74,7 @@ struct DevView {
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
-enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_TOTAL = 64 };
+enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_TOTAL = 64 };
 enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
     ST_RAYS_BOUNCE,
@@ -308,36 +308,68 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
 }
 
 // trace.comp:25-70 for extension rays; shadow rays test escape toward the sun.
+//
+// Persistent kernel with per-lane refill: a lane whose ray has finished takes
+// the next queue entry (one warp-aggregated atomicAdd on a per-pass cursor
+// serves all idle lanes of the warp, once at least 8 are idle or none is
+// busy), so warps stay full although ray lengths differ by 100x.
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
-    uint32_t fetch = 0, steps = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t e = a.rayq[i];
-        const uint32_t p = e & 0x7FFFFFFFu;
-        const bool shadow = (e >> 31) != 0u;
-        const uint4 meta = a.p_meta[p];
-        const DevView& v = a.views[meta.z & 0xFFFFu];
-        const DevScene S = a.scenes[v.scene];
-        const f3 o = ld3(a.p_ray_o[p]);
-        const f3 d = shadow ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
-        RayCount rc;
-        const Hit h = raycast<COUNT>(S.nodes, S.n_words, S.depth, o, d, v.cc_bounce, rc);
-        if (shadow) {
-            a.p_vis[p] = h.status == kEscaped ? 1u : 0u;
-        } else {
-            a.p_hit[p] = make_uint4(h.status, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+    uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
+    const uint32_t lane = lane_id();
+    bool active = false, exhausted = false;
+    uint32_t e = 0, D = 0;
+    const uint32_t* nodes = nullptr;
+    uint64_t n_words = 0;
+    Dda s;
+    Hit h;
+    RayCount rc;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+        const unsigned busy = __ballot_sync(0xffffffffu, active);
+        if (idle == 0u && busy == 0u) break;
+        bool finished = false;
+        if (idle != 0u && (__popc(idle) >= 8 || busy == 0u)) {
+            const int leader = __ffs(idle) - 1;
+            uint32_t base = 0;
+            if (int(lane) == leader) base = atomicAdd(cursor, uint32_t(__popc(idle)));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                const uint32_t idx = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+                if (idx < n) {
+                    e = a.rayq[idx];
+                    const uint32_t p = e & 0x7FFFFFFFu;
+                    const uint4 meta = a.p_meta[p];
+                    const DevView& v = a.views[meta.z & 0xFFFFu];
+                    const DevScene S = a.scenes[v.scene];
+                    nodes = S.nodes;
+                    n_words = S.n_words;
+                    D = S.depth;
+                    const f3 o = ld3(a.p_ray_o[p]);
+                    const f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
+                    finished = dda_init(s, o, d, v.cc_bounce, D, h);
+                    active = !finished;
+                } else {
+                    exhausted = true;
+                }
+            }
         }
-        if (COUNT) {
-            fetch += rc.fetch;
-            steps += rc.steps;
+        if (active) {
+            finished = dda_step<COUNT>(s, nodes, n_words, D, h, rc);
+            if (finished) active = false;
+        }
+        if (finished) {
+            const uint32_t p = e & 0x7FFFFFFFu;
+            if (e >> 31) a.p_vis[p] = h.status == kEscaped ? 1u : 0u;
+            else a.p_hit[p] = make_uint4(h.status, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
         }
     }
     if (COUNT) {
-        warp_add_stat(&a.stats[ST_FETCH], fetch);
-        warp_add_stat(&a.stats[ST_STEPS], steps);
-        warp_add_stat(&a.stats[ST_FETCH_TRACE], fetch);
-        warp_add_stat(&a.stats[ST_STEPS_TRACE], steps);
+        warp_add_stat(&a.stats[ST_FETCH], rc.fetch);
+        warp_add_stat(&a.stats[ST_STEPS], rc.steps);
+        warp_add_stat(&a.stats[ST_FETCH_TRACE], rc.fetch);
+        warp_add_stat(&a.stats[ST_STEPS_TRACE], rc.steps);
     }
 }
 
@@ -1200,6 +1232,24 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
     }
     for (auto& slot : x->timing)
         for (auto& e : slot.ev) cudaEventCreate(&e);
+    {
+        // scale factors of the Halton digit loop: f_0 = 1/b, f_{k+1} = f_k / b,
+        // the same IEEE single-precision division sequence as the loop itself
+        static const uint32_t bases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+        float tab[16][24];
+        for (int r = 0; r < 16; r++) {
+            volatile float f = 1.0f;
+            for (int k = 0; k < 24; k++) {
+                f = f / float(bases[r]);
+                tab[r][k] = f;
+            }
+        }
+        if (cudaMemcpyToSymbol(c_halton_f, tab, sizeof(tab)) != cudaSuccess) {
+            cudaStreamDestroy(x->stream);
+            delete x;
+            return fail(VE_ERR_CUDA, "ctx_create: constant table upload failed");
+        }
+    }
     int bt = 0, btc = 0, bs = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);

@@ -63,32 +63,59 @@ __device__ __forceinline__ uint32_t voxel_key(uint32_t x, uint32_t y, uint32_t z
     return hash32(x | (y << 10) | (z << 20)) & 0x7FFFFFFFu;
 }
 
-// halton + rand (internal.glsl:57-89)
-__device__ __forceinline__ float halton(uint32_t i, uint32_t b) {
-    float f = 1.0f, r = 0.0f;
-    const float fb = float(b);
+// halton + rand (internal.glsl:57-89).
+//
+// Same values as the loop `f /= b; q = i / b; r += f * (i - q*b); i = q` run
+// with a runtime base, computed faster:
+//   * the digit loop is instantiated per base so every division is by a
+//     compile-time constant (multiply-high + shift);
+//   * the scale factors f_k = (((1/b)/b)/...) are the IEEE quotients of that
+//     same division sequence, read from a table built once on the host with
+//     identical single-precision divisions;
+//   * base 2: every partial sum has <= 24 significant bits, so the float sum is
+//     exact and equals the bit-reversed low 24 bits of i scaled by 2^-24.
+__constant__ float c_halton_f[16][24];
+
+template <uint32_t B>
+__device__ __forceinline__ float halton_const(uint32_t i, int row) {
+    float r = 0.0f;
+#pragma unroll 1
     for (int k = 0; k < 24 && i > 0u; k++) {
-        f = f / fb;
-        const uint32_t q = i / b;
-        r = r + f * float(i - q * b);
+        const uint32_t q = i / B;
+        r = r + c_halton_f[row][k] * float(i - q * B);
         i = q;
     }
     return r;
 }
-__device__ __forceinline__ uint32_t halton_base(uint32_t idx) {
-    // {2,3,5,7,11,13,17,19,23,29,31,37,41,43,47,53}
-    const uint32_t lo = (idx < 8u) ? (idx < 4u ? (idx < 2u ? (idx == 0u ? 2u : 3u) : (idx == 2u ? 5u : 7u))
-                                               : (idx < 6u ? (idx == 4u ? 11u : 13u) : (idx == 6u ? 17u : 19u)))
-                                   : (idx < 12u ? (idx < 10u ? (idx == 8u ? 23u : 29u) : (idx == 10u ? 31u : 37u))
-                                                : (idx < 14u ? (idx == 12u ? 41u : 43u) : (idx == 14u ? 47u : 53u)));
-    return lo;
+__device__ __forceinline__ float halton2(uint32_t i) {
+    return float(__brev(i) >> 8) * 5.9604644775390625e-8f;  // exact: <= 24 significant bits
+}
+__device__ __forceinline__ float halton_idx(uint32_t i, uint32_t idx) {
+    switch (idx) {
+        case 0: return halton2(i);
+        case 1: return halton_const<3>(i, 1);
+        case 2: return halton_const<5>(i, 2);
+        case 3: return halton_const<7>(i, 3);
+        case 4: return halton_const<11>(i, 4);
+        case 5: return halton_const<13>(i, 5);
+        case 6: return halton_const<17>(i, 6);
+        case 7: return halton_const<19>(i, 7);
+        case 8: return halton_const<23>(i, 8);
+        case 9: return halton_const<29>(i, 9);
+        case 10: return halton_const<31>(i, 10);
+        case 11: return halton_const<37>(i, 11);
+        case 12: return halton_const<41>(i, 12);
+        case 13: return halton_const<43>(i, 13);
+        case 14: return halton_const<47>(i, 14);
+        default: return halton_const<53>(i, 15);
+    }
 }
 __device__ __forceinline__ float rand01(uint32_t& state) {
     const uint32_t dim = state & 0xFFu;
     const uint32_t sample_idx = state >> 8;
     state = (sample_idx << 8) | ((dim + 1u) & 0xFFu);
     const uint32_t effective = sample_idx ^ ((dim >> 4) * 0x9E3779B9u);
-    return halton(effective, halton_base(dim & 15u));
+    return halton_idx(effective, dim & 15u);
 }
 
 // sin/cos of 2*pi*u: quadrant reduction then Taylor polynomials of degree
@@ -148,8 +175,11 @@ __device__ __forceinline__ f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float r
     const f3 H = normalize(sub(L, V));
     const float NdotH = gmax(dot(N, H), 0.001f);
     const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
-    const float specular = spec_norm * powf(NdotH, spec_exp);
     const float kS = specular_intensity * metallic;
+    // the lobe is multiplied by kS: with kS == 0 the product is +0 for every
+    // finite NdotH (pow of a value in [0.001, 1+eps] is finite) and NaN when
+    // NdotH is NaN, which (NdotH - NdotH) reproduces without calling powf
+    const float specular = kS != 0.0f ? spec_norm * powf(NdotH, spec_exp) : spec_norm * (NdotH - NdotH);
     const float kD = 1.0f - kS * 0.5f;
     const f3 diffuse = muls(muls(albedo, kD), 0.31831f);
     const float sp = specular * kS;
