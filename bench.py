@@ -217,6 +217,81 @@ def _words_with_normals(orc, words, depth):
     return orc.fill_normals(words, depth, fast=True, threads=os.cpu_count() or 1)
 
 
+def run_batching(args, rank, world):
+    """64 views (resolutions 128^2..1080p, spp 1-8, bounces 1-4, random poses)
+    over 4 resident octrees of depth 8, 9, 10, 10: one batched wavefront per
+    frame (one launch per kernel and bounce for all views, CUDA-graph replay,
+    autotuned launch shapes) against 64 per-view plain renders."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=300.0, device=local)
+    torch.cuda.set_device(local)
+    vs = wl.batching_views(64, seed=7 + rank)
+    scene_words = []
+    for depth, variant, seed in wl.BATCH_SCENES:
+        w, nv = ve.terrain_words(depth, variant, seed)
+        scene_words.append((w, depth, nv))
+    results = {}
+    for mode in ("batched", "per_view"):
+        r = ve.Renderer(device=local, hash_log2=22, graphs=(mode == "batched"))
+        r.set_materials(ve.terrain_materials(1))
+        sids = [r.upload_scene(w, d) for w, d, _ in scene_words]
+        views = []
+        for v in vs:
+            cam = ve.camera_ubo(v["eye"], v["dir"], 70.0, v["width"] / v["height"])
+            fc = ve.FrameConfig(width=v["width"], height=v["height"], spp=v["spp"], bounces=v["bounces"],
+                                frame_index=v["frame"], primary_controlchecks=300, bounce_controlchecks=300)
+            views.append((sids[v["scene"]], cam, fc))
+        tuned = r.autotune(views, frames_per_trial=1) if mode == "batched" else r.launch_config()
+        stream = torch.cuda.ExternalStream(r.stream, device=local)
+
+        def frame():
+            if mode == "batched":
+                r.render_batch(views, outputs=())
+            else:
+                for v in views:
+                    r.render(*v, outputs=())
+
+        for _ in range(args.warmup):
+            frame()
+        r.synchronize()
+        r.reset_total_stats()
+        torch.cuda.synchronize(local)
+        vd.barrier(dist)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            frame()
+        e1.record(stream)
+        e1.synchronize()
+        ms = vd.max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+        tot = r.total_stats()
+        rays = vd.sum_over_ranks(rays_of(tot), dist, f"cuda:{local}")
+        results[mode] = {"mrays_s": rays / (ms / 1e3) / 1e6, "ms_per_frame": ms / args.steps,
+                         "rays_per_frame": rays_of(tot) / args.steps, "launch_config": tuned,
+                         "kernel_launches_per_frame": tot["kernel_launches"] / args.steps}
+        r.close()
+    if rank == 0:
+        line = {"metric": "Mrays/s, 64-view batch over 4 octrees (depth 8/9/10/10)",
+                "value": results["batched"]["mrays_s"], "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": results["batched"]["ms_per_frame"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded views)",
+                "config": {"workload": "batching: 64 views, resolutions {128^2,256^2,640x360,1280x720,1920x1080}, "
+                                       "spp 1-8, bounces 1-4, 4 octrees depth 8/9/10/10",
+                           "pixels": int(sum(v["width"] * v["height"] for v in vs))},
+                "batched": results["batched"], "per_view_plain": results["per_view"],
+                "speedup_vs_per_view": results["batched"]["mrays_s"] / results["per_view"]["mrays_s"]}
+        print(json.dumps(line), flush=True)
+    vd.shutdown(dist)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -225,6 +300,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["large", "batching"], default="large")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -238,17 +314,14 @@ def main():
     W = wl.LARGE
     if args.impl == "reference":
         return run_reference(args, W, rank, world)
+    if args.workload == "batching":
+        return run_batching(args, rank, world)
 
     import torch
 
-    dist = None
-    if world > 1:
-        import datetime
+    import ve_b200.dist as vd
 
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = vd.init("nccl", timeout_s=300.0, device=local)
     torch.cuda.set_device(local)
     torch.cuda.init()
 
@@ -259,8 +332,10 @@ def main():
     sid = r.upload_scene(words, W.depth)
     stream = torch.cuda.ExternalStream(r.stream, device=local)
 
-    def frame(i):  # replicas: rank r takes every world-th orbit frame
-        return (rank + world * i) % W.frames
+    plan = vd.frame_assignment(args.warmup + args.steps, rank, world, W.frames)  # replicas
+
+    def frame(i):
+        return plan[i]
 
     def cams(i):
         eye, d = wl.orbit_camera(frame(i), W.frames, W.seed)
@@ -268,26 +343,18 @@ def main():
 
     K, Wm = args.steps, args.warmup
     cam_list = [cams(Wm + i) for i in range(K)]
+    dev = f"cuda:{local}"
 
     def barrier():
         torch.cuda.synchronize(local)
         r.synchronize()
-        if dist:
-            dist.barrier()
+        vd.barrier(dist)
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return vd.max_over_ranks(x, dist, dev)
 
     def sum_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return vd.sum_over_ranks(x, dist, dev)
 
     # warm-up
     for i in range(Wm):
@@ -382,9 +449,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     r.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    vd.shutdown(dist)
     return 0
 
 

@@ -43,6 +43,8 @@ extern "C" {
 #define VE_FRAME_TIMING 1u        /* per-pass CUDA-event times into ve_frame_stats */
 #define VE_FRAME_COUNT_FETCH 2u   /* count node-word fetches on the device */
 #define VE_FRAME_PATH_RGB 4u      /* keep every path's deposit value (debug) */
+#define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
+                                     replaying a CUDA graph of the frame's kernel sequence */
 
 /* RendererConfig (src/renderer/core.hpp:30-42) plus device sizing.  The
  * radiance cache replaces the lBuffer hash image (renderer.cpp:27-40):
@@ -211,12 +213,69 @@ int ve_render(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
  * batch: one primary pass over all views, one trace and one shade pass per
  * bounce depth for all their paths, one resolve pass. `outs` may be NULL. */
 int ve_render_batch(ve_ctx* ctx, const ve_view* views, uint32_t n_views, ve_frame_outputs* outs);
+/* Launch shape of the persistent bounce kernels: resident blocks per SM of
+ * the trace and shade kernels (0 = occupancy maximum) and the number of idle
+ * lanes at which a trace warp refills itself with new rays. */
+typedef struct ve_launch_config {
+    uint32_t trace_blocks_per_sm;
+    uint32_t shade_blocks_per_sm;
+    uint32_t refill_threshold;
+    uint32_t reserved;
+} ve_launch_config;
+int ve_get_launch_config(ve_ctx* ctx, ve_launch_config* cfg);
+int ve_set_launch_config(ve_ctx* ctx, const ve_launch_config* cfg);
+/* Autotuner (no reference counterpart): renders the given views with
+ * candidate launch shapes (coordinate descent over trace blocks/SM, shade
+ * blocks/SM, refill threshold; `frames_per_trial` timed frames each), keeps
+ * the fastest in the context and returns it.  The trial frames deposit into
+ * the scenes' radiance caches like any render. */
+int ve_autotune(ve_ctx* ctx, const ve_view* views, uint32_t n_views, uint32_t frames_per_trial,
+                ve_launch_config* best);
+
 /* stats of the last render call (synchronises the context stream) */
 int ve_get_stats(ve_ctx* ctx, ve_frame_stats* stats);
 /* stats summed over every render call since ve_reset_total_stats (device
  * counters accumulate on the stream: no host synchronisation per frame) */
 int ve_get_total_stats(ve_ctx* ctx, ve_frame_stats* stats);
 int ve_reset_total_stats(ve_ctx* ctx);
+
+/* ======================================================================
+ * Render server: continuous batching (no reference counterpart; the
+ * reference renders one interactive view per Renderer::run)
+ * ==================================================================== */
+
+/* Requests are admitted first come first served while their framebuffer
+ * (pixel_capacity pool) and path-state (path_capacity pool) ranges fit — the
+ * per-request part of the HBM budget; scenes and radiance caches stay
+ * resident — and join the in-flight wavefront at the next bounce pass.  The
+ * server owns the context's stream while it exists. */
+typedef struct ve_server ve_server;
+typedef struct ve_server_config {
+    uint64_t pixel_capacity; /* pooled pixels: GBuffer + outputs, 48 B each */
+    uint64_t path_capacity;  /* pooled path states, 145 B each */
+    uint32_t max_requests;   /* view slots (requests on the GPU at once) */
+    uint32_t flags;
+} ve_server_config;
+typedef struct ve_request_info {
+    uint64_t request_id;
+    double submit_s, admit_s, done_s; /* steady-clock seconds */
+    uint64_t pixels, paths;
+} ve_request_info;
+typedef struct ve_server_stats {
+    uint64_t completed, admitted, queued, in_flight, max_in_flight, steps;
+    uint64_t pool_bytes, scene_bytes;
+} ve_server_stats;
+int ve_server_create(ve_ctx* ctx, const ve_server_config* cfg, ve_server** out);
+/* voxel_id_out (1 x u32 per pixel) and rgb_out (3 x f32 per pixel) may be NULL;
+ * they must stay valid until ve_server_wait returns for this request */
+int ve_server_submit(ve_server* s, const ve_view* view, uint32_t* voxel_id_out, float* rgb_out,
+                     uint64_t* request_id);
+/* waits for a request (VE_ERR_TIMEOUT when not done within timeout_ms), then
+ * forgets it */
+int ve_server_wait(ve_server* s, uint64_t request_id, uint32_t timeout_ms, ve_request_info* info);
+int ve_server_get_stats(ve_server* s, ve_server_stats* stats);
+/* finishes queued and in-flight requests, then stops the worker */
+int ve_server_destroy(ve_server* s);
 
 /* ======================================================================
  * Allocation-free entry point (no counterpart in the reference)

@@ -43,6 +43,7 @@ SCENE_KEEP_NORMALS = 1
 FRAME_TIMING = 1
 FRAME_COUNT_FETCH = 2
 FRAME_PATH_RGB = 4
+CFG_NO_GRAPHS = 1
 
 
 class VeError(RuntimeError):
@@ -77,6 +78,11 @@ class FrameOutputsC(ctypes.Structure):
                 ("rgb", ctypes.c_void_p), ("mapped", ctypes.c_void_p), ("path_rgb", ctypes.c_void_p)]
 
 
+class LaunchConfigC(ctypes.Structure):
+    _fields_ = [("trace_blocks_per_sm", ctypes.c_uint32), ("shade_blocks_per_sm", ctypes.c_uint32),
+                ("refill_threshold", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
 class FrameStatsC(ctypes.Structure):
     _fields_ = [("rays_primary", ctypes.c_uint64), ("rays_bounce", ctypes.c_uint64),
                 ("rays_shadow", ctypes.c_uint64), ("fetch_nodes", ctypes.c_uint64), ("paths", ctypes.c_uint64),
@@ -87,6 +93,21 @@ class FrameStatsC(ctypes.Structure):
                 ("ms_shade", ctypes.c_float), ("ms_resolve", ctypes.c_float), ("ms_decay", ctypes.c_float),
                 ("trace_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
                 ("cache_capacity", ctypes.c_uint64)]
+
+
+class ServerConfigC(ctypes.Structure):
+    _fields_ = [("pixel_capacity", ctypes.c_uint64), ("path_capacity", ctypes.c_uint64),
+                ("max_requests", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
+
+
+class RequestInfoC(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_uint64), ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("done_s", ctypes.c_double), ("pixels", ctypes.c_uint64), ("paths", ctypes.c_uint64)]
+
+
+class ServerStatsC(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("completed", "admitted", "queued", "in_flight", "max_in_flight",
+                                               "steps", "pool_bytes", "scene_bytes")]
 
 
 _P = ctypes.c_void_p
@@ -139,6 +160,14 @@ _SIGNATURES = {
     "ve_get_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
     "ve_get_total_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
     "ve_fill_normals_noalloc": ([_P, _U64, _U32, _P], ctypes.c_int),
+    "ve_get_launch_config": ([_P, _PTR(LaunchConfigC)], ctypes.c_int),
+    "ve_server_create": ([_P, _PTR(ServerConfigC), _PTR(_P)], ctypes.c_int),
+    "ve_server_submit": ([_P, _PTR(ViewC), _P, _P, _PTR(_U64)], ctypes.c_int),
+    "ve_server_wait": ([_P, _U64, _U32, _PTR(RequestInfoC)], ctypes.c_int),
+    "ve_server_get_stats": ([_P, _PTR(ServerStatsC)], ctypes.c_int),
+    "ve_server_destroy": ([_P], ctypes.c_int),
+    "ve_set_launch_config": ([_P, _PTR(LaunchConfigC)], ctypes.c_int),
+    "ve_autotune": ([_P, _PTR(ViewC), _U32, _U32, _PTR(LaunchConfigC)], ctypes.c_int),
     "ve_reset_total_stats": ([_P], ctypes.c_int),
 }
 
@@ -406,9 +435,9 @@ def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
 class Renderer:
     """The device renderer (one CUDA context stream, owned device memory)."""
 
-    def __init__(self, device: int = 0, hash_log2: int = 22, hash_probes: int = 64):
+    def __init__(self, device: int = 0, hash_log2: int = 22, hash_probes: int = 64, graphs: bool = True):
         self._lib = load_library()
-        cfg = RendererConfigC(device, hash_log2, hash_probes, 0)
+        cfg = RendererConfigC(device, hash_log2, hash_probes, 0 if graphs else CFG_NO_GRAPHS)
         h = _P()
         _check(self._lib.ve_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -516,6 +545,25 @@ class Renderer:
         _check(self._lib.ve_render_batch(self._h, arr, len(views), outs if want else None))
         return results
 
+    def launch_config(self) -> Dict[str, int]:
+        c = LaunchConfigC()
+        _check(self._lib.ve_get_launch_config(self._h, ctypes.byref(c)))
+        return {k: getattr(c, k) for k, _ in LaunchConfigC._fields_}
+
+    def set_launch_config(self, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
+                          refill_threshold: int = 8) -> None:
+        c = LaunchConfigC(trace_blocks_per_sm, shade_blocks_per_sm, refill_threshold, 0)
+        _check(self._lib.ve_set_launch_config(self._h, ctypes.byref(c)))
+
+    def autotune(self, views: Sequence[tuple], frames_per_trial: int = 2) -> Dict[str, int]:
+        """views: (scene_id, camera, FrameConfig) tuples; returns the chosen launch config."""
+        arr = (ViewC * len(views))()
+        for i, (sid, cam, fc) in enumerate(views):
+            arr[i] = self.make_view(sid, cam, fc)
+        best = LaunchConfigC()
+        _check(self._lib.ve_autotune(self._h, arr, len(views), frames_per_trial, ctypes.byref(best)))
+        return {k: getattr(best, k) for k, _ in LaunchConfigC._fields_}
+
     def stats(self) -> Dict[str, float]:
         """Counters and timings of the last render call."""
         s = FrameStatsC()
@@ -544,7 +592,55 @@ class Renderer:
         return self.render(self.scene, self.camera, fc, outputs)
 
 
+class Server:
+    """Render server with continuous batching over one Renderer's context."""
+
+    def __init__(self, renderer: "Renderer", pixel_capacity: int, path_capacity: int, max_requests: int = 64):
+        self._lib = load_library()
+        self.renderer = renderer
+        cfg = ServerConfigC(pixel_capacity, path_capacity, max_requests, 0)
+        h = _P()
+        _check(self._lib.ve_server_create(renderer._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._buffers: Dict[int, tuple] = {}
+
+    def submit(self, scene_id: int, camera: np.ndarray, fc: FrameConfig, want_vid: bool = True,
+               want_rgb: bool = True) -> int:
+        view = Renderer.make_view(scene_id, camera, fc)
+        vid = np.zeros((fc.height, fc.width), np.uint32) if want_vid else None
+        rgb = np.zeros((fc.height, fc.width, 3), np.float32) if want_rgb else None
+        rid = _U64()
+        _check(self._lib.ve_server_submit(self._h, ctypes.byref(view), _ptr(vid), _ptr(rgb), ctypes.byref(rid)))
+        self._buffers[rid.value] = (vid, rgb)
+        return rid.value
+
+    def wait(self, request_id: int, timeout_ms: int = 120000) -> Dict[str, object]:
+        info = RequestInfoC()
+        _check(self._lib.ve_server_wait(self._h, request_id, timeout_ms, ctypes.byref(info)))
+        vid, rgb = self._buffers.pop(request_id)
+        return {"voxel_id": vid, "rgb": rgb, "submit_s": info.submit_s, "admit_s": info.admit_s,
+                "done_s": info.done_s, "latency_s": info.done_s - info.submit_s, "pixels": info.pixels,
+                "paths": info.paths}
+
+    def stats(self) -> Dict[str, int]:
+        st = ServerStatsC()
+        _check(self._lib.ve_server_get_stats(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStatsC._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            rc = self._lib.ve_server_destroy(self._h)
+            self._h = None
+            _check(rc)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 __all__ = [
     "OctreeCPU", "Octree", "Renderer", "FrameConfig", "VeError", "camera_ubo", "look_at", "terrain_words",
-    "terrain_voxels", "terrain_materials", "load_library", "SUN_DIR",
+    "terrain_voxels", "terrain_materials", "load_library", "SUN_DIR", "Server",
 ]

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -116,6 +117,9 @@ struct FrameArgs {
     float* out_rgb;
     float* out_mapped;
     float* path_rgb;
+    uint32_t refill;       // idle lanes at which a trace warp takes new rays
+    uint32_t view_offset;  // index of views[0] in the view table the paths refer to
+    uint32_t* remaining;   // per view slot: paths not yet deposited (serving), or null
 };
 
 // ---------------------------------------------------------------------------
@@ -295,12 +299,17 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
             a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             a.p_hit[p] = make_uint4(kHit, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
-            a.p_meta[p] = make_uint4(vid, rng, vi, pix);
+            a.p_meta[p] = make_uint4(vid, rng, vi + a.view_offset, pix);
             a.live[0][q + s] = uint32_t(p);
         }
     }
     warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside ? 1u : 0u);
     warp_add_stat(&a.stats[ST_PATHS], spawn ? v.spp : 0u);
+    if (a.remaining) {  // the whole block belongs to one view
+        uint32_t sp = spawn ? v.spp : 0u;
+        for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        if (lane_id() == 0 && sp) atomicAdd(&a.remaining[vi + a.view_offset], sp);
+    }
     if (COUNT) {
         warp_add_stat(&a.stats[ST_FETCH], rc.fetch);
         warp_add_stat(&a.stats[ST_STEPS], rc.steps);
@@ -311,10 +320,10 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
 //
 // Persistent kernel with per-lane refill: a lane whose ray has finished takes
 // the next queue entry (one warp-aggregated atomicAdd on a per-pass cursor
-// serves all idle lanes of the warp, once at least 8 are idle or none is
+// serves all idle lanes of the warp, once `refill` of them are idle or none is
 // busy), so warps stay full although ray lengths differ by 100x.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
@@ -323,6 +332,7 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t* nodes = nullptr;
     uint64_t n_words = 0;
     Dda s;
+    uint32_t base[17];
     Hit h;
     RayCount rc;
     for (;;) {
@@ -330,13 +340,13 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
         const unsigned busy = __ballot_sync(0xffffffffu, active);
         if (idle == 0u && busy == 0u) break;
         bool finished = false;
-        if (idle != 0u && (__popc(idle) >= 8 || busy == 0u)) {
+        if (idle != 0u && (uint32_t(__popc(idle)) >= a.refill || busy == 0u)) {
             const int leader = __ffs(idle) - 1;
-            uint32_t base = 0;
-            if (int(lane) == leader) base = atomicAdd(cursor, uint32_t(__popc(idle)));
-            base = __shfl_sync(0xffffffffu, base, leader);
+            uint32_t first_idx = 0;
+            if (int(lane) == leader) first_idx = atomicAdd(cursor, uint32_t(__popc(idle)));
+            first_idx = __shfl_sync(0xffffffffu, first_idx, leader);
             if (!active && !exhausted) {
-                const uint32_t idx = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+                const uint32_t idx = first_idx + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (idx < n) {
                     e = a.rayq[idx];
                     const uint32_t p = e & 0x7FFFFFFFu;
@@ -348,7 +358,7 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
                     D = S.depth;
                     const f3 o = ld3(a.p_ray_o[p]);
                     const f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
-                    finished = dda_init(s, o, d, v.cc_bounce, D, h);
+                    finished = dda_init<COUNT>(s, base, o, d, v.cc_bounce, D, h, rc);
                     active = !finished;
                 } else {
                     exhausted = true;
@@ -356,7 +366,7 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_step<COUNT>(s, nodes, n_words, D, h, rc);
+            finished = dda_iter<COUNT>(s, base, nodes, n_words, D, h, rc);
             if (finished) active = false;
         }
         if (finished) {
@@ -380,7 +390,7 @@ __global__ void k_accum_stats(const unsigned long long* frame, unsigned long lon
 
 // shade.comp:543-575, 838-908 (bounce/shade loop) with the sun next-event
 // estimate in the place of the dormant emissive NEE, and the AccumPass deposit.
-__global__ void __launch_bounds__(256) k_shade(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
     const uint32_t* live_in = a.live[pass & 1u];
@@ -394,7 +404,7 @@ __global__ void __launch_bounds__(256) k_shade(FrameArgs a, uint32_t pass) {
         const uint32_t p = valid ? live_in[i] : 0u;
         bool do_dep = false, app_live = false, app_ext = false, app_sh = false;
         float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
-        uint32_t dvid = 0, dscene = 0;
+        uint32_t dvid = 0, dscene = 0, dview = 0;
         if (valid) {
             uint4 meta = a.p_meta[p];
             const uint32_t vi = meta.z & 0xFFFFu;
@@ -516,6 +526,7 @@ __global__ void __launch_bounds__(256) k_shade(FrameArgs a, uint32_t pass) {
                 dl2 = Lf * Lf;
                 dvid = meta.x;
                 dscene = v.scene;
+                dview = vi;
                 if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
                     a.path_rgb[3ull * p + 0] = dr;
                     a.path_rgb[3ull * p + 1] = dg;
@@ -532,6 +543,13 @@ __global__ void __launch_bounds__(256) k_shade(FrameArgs a, uint32_t pass) {
         n_ext += app_ext ? 1u : 0u;
         n_sh += app_sh ? 1u : 0u;
         warp_deposit(do_dep, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
+        if (a.remaining) {  // serving: count finished paths per view slot
+            const unsigned dm = __ballot_sync(0xffffffffu, do_dep);
+            if (do_dep) {
+                const unsigned peers = __match_any_sync(dm, dview);
+                if (int(lane_id()) == __ffs(peers) - 1) atomicSub(&a.remaining[dview], uint32_t(__popc(peers)));
+            }
+        }
     }
     warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
@@ -874,6 +892,8 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
+    int occ_trace = 1, occ_trace_count = 1, occ_shade = 1;  // occupancy maxima (blocks/SM)
+    ve_launch_config launch{0, 0, 8, 0};
     // per-frame CUDA-event sets in a ring: elapsed times are read when the
     // slot is reused or the stats are queried, so timed frames never wait
     static constexpr int kTimingSlots = 16, kEvents = 48;
@@ -887,6 +907,18 @@ struct ve_ctx {
     ve_frame_stats last{};
     bool last_timing = false;
     int last_timing_slot = -1;
+    // CUDA graphs of the per-frame kernel sequence, keyed by what shapes it;
+    // `gen` changes whenever a buffer or scene the kernels point at moves
+    uint64_t gen = 1;
+    struct GraphEntry {
+        std::vector<uint64_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint32_t launches = 0, trace_launches = 0;
+        uint64_t last_use = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t graph_clock = 0;
+    uint64_t graph_captures = 0, graph_replays = 0;
     uint32_t last_launches = 0, last_trace_launches = 0;
 };
 
@@ -899,8 +931,10 @@ static int sync_scenes(ve_ctx* c) {
         const SceneSlot& s = c->scenes[i];
         h[i] = DevScene{s.nodes, s.n_words, s.cache, s.depth, c->cfg.hash_log2, c->cfg.hash_probes, 0u};
     }
+    const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
     if (rc) return rc;
+    if (old != c->d_scenes.p) c->gen++;
     VE_CUDA(cudaMemcpyAsync(c->d_scenes.p, h.data(), h.size() * sizeof(DevScene), cudaMemcpyHostToDevice, c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
     c->scenes_dirty = false;
@@ -951,6 +985,21 @@ static int compute_normals(ve_ctx* c, SceneSlot& s) {
 
 static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_views) {
     int rc = 0;
+    const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->p_ray_o.p,
+                            c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p, c->p_pend.p, c->p_hit.p,
+                            c->p_meta.p, c->p_vis.p, c->live0.p, c->live1.p, c->rayq.p, c->d_views.p};
+    struct GenBump {
+        ve_ctx* c;
+        const void* const* before;
+        ~GenBump() {
+            const void* after[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p,
+                                   c->p_ray_o.p, c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p,
+                                   c->p_pend.p, c->p_hit.p, c->p_meta.p, c->p_vis.p, c->live0.p, c->live1.p,
+                                   c->rayq.p, c->d_views.p};
+            for (size_t i = 0; i < sizeof(after) / sizeof(after[0]); i++)
+                if (after[i] != before[i]) { c->gen++; break; }
+        }
+    } bump{c, before};
     if ((rc = c->gbuf.ensure(pixels)) || (rc = c->out_vid.ensure(pixels)) || (rc = c->out_node.ensure(pixels)) ||
         (rc = c->out_rgb.ensure(pixels * 3)) || (rc = c->out_mapped.ensure(pixels * 3)))
         return rc;
@@ -1012,6 +1061,16 @@ static void collect_all_timing(ve_ctx* c) {
     }
 }
 
+// Grid sizes of the persistent kernels from the launch config (0 = the
+// occupancy maximum), clamped to what can be resident.
+static void apply_launch(ve_ctx* c) {
+    auto pick = [&](uint32_t want, int occ) { return int((want == 0 || int(want) > occ) ? occ : int(want)); };
+    c->grid_trace = c->num_sms * pick(c->launch.trace_blocks_per_sm, c->occ_trace);
+    c->grid_trace_count = c->num_sms * pick(c->launch.trace_blocks_per_sm, c->occ_trace_count);
+    c->grid_shade = c->num_sms * pick(c->launch.shade_blocks_per_sm, c->occ_shade);
+    if (c->launch.refill_threshold == 0 || c->launch.refill_threshold > 32) c->launch.refill_threshold = 8;
+}
+
 static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_outputs* outs) {
     if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "render: no views");
     if (nv > 65535u) return fail(VE_ERR_INVALID, "render: at most 65535 views per batch");
@@ -1041,7 +1100,11 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
     int rc = ensure_frame(c, pixels, paths, nv);
     if (rc) return rc;
-    if ((flags & VE_FRAME_PATH_RGB) && (rc = c->path_rgb.ensure(paths * 3))) return rc;
+    if (flags & VE_FRAME_PATH_RGB) {
+        const void* old = c->path_rgb.p;
+        if ((rc = c->path_rgb.ensure(paths * 3))) return rc;
+        if (old != c->path_rgb.p) c->gen++;
+    }
     if ((rc = sync_scenes(c))) return rc;
     // view table, written into a staging slot whose previous copy has run
     const int slot = c->staging_next;
@@ -1080,11 +1143,6 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     VE_CUDA(cudaMemcpyAsync(c->d_views.p, hv, sizeof(DevView) * nv, cudaMemcpyHostToDevice, st));
     VE_CUDA(cudaEventRecord(c->staging_ev[slot], st));
     uint64_t h2d = sizeof(DevView) * nv, d2h = 0;
-    VE_CUDA(cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st));
-    VE_CUDA(cudaMemsetAsync(c->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), st));
-    // paths of pixels without a primary hit are never spawned: their debug
-    // slots read as zero
-    if (flags & VE_FRAME_PATH_RGB) VE_CUDA(cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st));
     // events: 0 start, 1 after decay, 2 after primary, then per pass
     // (shade, trace) pairs, last = after resolve
     ve_ctx::TimingSlot* ts = nullptr;
@@ -1098,23 +1156,14 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (timing) cudaEventRecord(ts->ev[ne], st);
         ne++;
     };
-    rec();
     // decay once per distinct scene (first view's decay factor)
-    {
-        std::vector<int> seen;
-        for (uint32_t i = 0; i < nv; i++) {
-            const int s = views[i].scene_id;
-            if (std::find(seen.begin(), seen.end(), s) != seen.end()) continue;
-            seen.push_back(s);
-            const float dk = views[i].frame.decay;
-            if (dk != 1.0f) {
-                const uint32_t n = 1u << c->cfg.hash_log2;
-                k_decay<<<c->num_sms * 8, 256, 0, st>>>(c->scenes[s].cache, n, dk);
-                launches++;
-            }
-        }
+    std::vector<std::pair<int, float>> decays;
+    for (uint32_t i = 0; i < nv; i++) {
+        const int sc = views[i].scene_id;
+        bool seen = false;
+        for (auto& d : decays) seen |= d.first == sc;
+        if (!seen) decays.emplace_back(sc, views[i].frame.decay);
     }
-    rec();
     FrameArgs a{};
     a.views = c->d_views.p;
     a.n_views = nv;
@@ -1129,27 +1178,94 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
     a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
     a.path_rgb = (flags & VE_FRAME_PATH_RGB) ? c->path_rgb.p : nullptr;
-    if (count) k_primary<true><<<tiles, 256, 0, st>>>(a);
-    else k_primary<false><<<tiles, 256, 0, st>>>(a);
-    launches++;
-    rec();
-    for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
-        k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
-        launches++;
+    a.refill = c->launch.refill_threshold;
+    a.view_offset = 0;
+    a.remaining = nullptr;
+    // the frame's kernel sequence (no host synchronisation inside)
+    auto enqueue = [&]() {
+        cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
+        cudaMemsetAsync(c->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), st);
+        // paths of pixels without a primary hit are never spawned: their
+        // debug slots read as zero
+        if (flags & VE_FRAME_PATH_RGB) cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st);
         rec();
-        if (pass <= max_b) {
-            if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
-            else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
-            launches++;
-            trace_launches++;
+        for (auto& d : decays) {
+            if (d.second != 1.0f) {
+                const uint32_t n = 1u << c->cfg.hash_log2;
+                k_decay<<<c->num_sms * 8, 256, 0, st>>>(c->scenes[d.first].cache, n, d.second);
+                launches++;
+            }
         }
         rec();
+        if (count) k_primary<true><<<tiles, 256, 0, st>>>(a);
+        else k_primary<false><<<tiles, 256, 0, st>>>(a);
+        launches++;
+        rec();
+        for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
+            k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
+            launches++;
+            rec();
+            if (pass <= max_b) {
+                if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
+                else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
+                launches++;
+                trace_launches++;
+            }
+            rec();
+        }
+        k_resolve<<<tiles, 256, 0, st>>>(a);
+        launches++;
+        rec();
+        k_accum_stats<<<1, 32, 0, st>>>(c->stats.p, c->totals.p);
+        launches++;
+    };
+    const bool use_graph = !timing && !(c->cfg.flags & VE_CFG_NO_GRAPHS);
+    if (!use_graph) {
+        enqueue();
+    } else {
+        std::vector<uint64_t> key = {c->gen, nv, tiles, max_b, flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB),
+                                     paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
+                                     uint64_t(c->launch.refill_threshold)};
+        for (auto& d : decays) {
+            uint32_t bits;
+            std::memcpy(&bits, &d.second, 4);
+            key.push_back((uint64_t(uint32_t(d.first)) << 32) | bits);
+        }
+        ve_ctx::GraphEntry* ge = nullptr;
+        for (auto& g : c->graphs)
+            if (g.key == key) ge = &g;
+        if (!ge) {
+            cudaGraph_t graph = nullptr;
+            VE_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            enqueue();
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (ce != cudaSuccess) return fail(VE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) return fail(VE_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+            if (c->graphs.size() >= 16) {
+                auto oldest = std::min_element(c->graphs.begin(), c->graphs.end(),
+                                               [](const auto& x, const auto& y) { return x.last_use < y.last_use; });
+                cudaGraphExecDestroy(oldest->exec);
+                c->graphs.erase(oldest);
+            }
+            ve_ctx::GraphEntry e;
+            e.key = key;
+            e.exec = exec;
+            e.launches = launches;
+            e.trace_launches = trace_launches;
+            c->graphs.push_back(e);
+            ge = &c->graphs.back();
+            c->graph_captures++;
+        } else {
+            launches = ge->launches;
+            trace_launches = ge->trace_launches;
+            c->graph_replays++;
+        }
+        ge->last_use = ++c->graph_clock;
+        VE_CUDA(cudaGraphLaunch(ge->exec, st));
     }
-    k_resolve<<<tiles, 256, 0, st>>>(a);
-    launches++;
-    rec();
-    k_accum_stats<<<1, 32, 0, st>>>(c->stats.p, c->totals.p);
-    launches++;
     VE_CUDA(cudaGetLastError());
     c->last_launches = launches;
     c->last_trace_launches = trace_launches;
@@ -1244,6 +1360,31 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
                 tab[r][k] = f;
             }
         }
+        // shading normals of the 19^3 stored gradients: normalize, 10-10-10
+        // code of packNormalAccum, UnpackNormal, normalize (host IEEE single)
+        static float4 ntab[19 * 19 * 19];
+        for (int ix = -9; ix <= 9; ix++)
+            for (int iy = -9; iy <= 9; iy++)
+                for (int iz = -9; iz <= 9; iz++) {
+                    volatile float ax = float(ix), ay = float(iy), az = float(iz);
+                    const float len = std::sqrt((ax * ax + ay * ay) + az * az);
+                    float n[3];
+                    if (len > 0.001f) { n[0] = ax / len; n[1] = ay / len; n[2] = az / len; }
+                    else { n[0] = 0.0f; n[1] = 1.0f; n[2] = 0.0f; }
+                    float u[3];
+                    for (int c = 0; c < 3; c++) {
+                        int q = int(std::round((n[c] + 1.0f) * 511.0f));
+                        q = q < 0 ? 0 : (q > 1022 ? 1022 : q);
+                        u[c] = float(uint32_t(q)) / 511.0f - 1.0f;
+                    }
+                    const float s2 = std::sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+                    ntab[((ix + 9) * 19 + (iy + 9)) * 19 + (iz + 9)] = make_float4(u[0] / s2, u[1] / s2, u[2] / s2, 0.0f);
+                }
+        if (cudaMemcpyToSymbol(g_normal_table, ntab, sizeof(ntab)) != cudaSuccess) {
+            cudaStreamDestroy(x->stream);
+            delete x;
+            return fail(VE_ERR_CUDA, "ctx_create: normal table upload failed");
+        }
         if (cudaMemcpyToSymbol(c_halton_f, tab, sizeof(tab)) != cudaSuccess) {
             cudaStreamDestroy(x->stream);
             delete x;
@@ -1254,9 +1395,10 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade, 256, 0);
-    x->grid_trace = x->num_sms * std::max(bt, 1);
-    x->grid_trace_count = x->num_sms * std::max(btc, 1);
-    x->grid_shade = x->num_sms * std::max(bs, 1);
+    x->occ_trace = std::max(bt, 1);
+    x->occ_trace_count = std::max(btc, 1);
+    x->occ_shade = std::max(bs, 1);
+    apply_launch(x);
     int rc = 0;
     for (auto& e : x->staging_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     if ((rc = x->counters.ensure(CNT_TOTAL)) || (rc = x->stats.ensure(ST_TOTAL)) ||
@@ -1295,6 +1437,8 @@ int ve_ctx_destroy(ve_ctx* c) {
     for (auto& slot : c->timing)
         for (auto& e : slot.ev)
             if (e) cudaEventDestroy(e);
+    for (auto& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return VE_OK;
@@ -1354,6 +1498,7 @@ int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t
         c->scenes[id] = s;
     }
     c->scenes_dirty = true;
+    c->gen++;
     *scene_id = id;
     return VE_OK;
 }
@@ -1368,6 +1513,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     cudaFree(s.cache);
     s = SceneSlot();
     c->scenes_dirty = true;
+    c->gen++;
     return VE_OK;
 }
 
@@ -1474,6 +1620,73 @@ int ve_render_batch(ve_ctx* c, const ve_view* views, uint32_t n, ve_frame_output
     if (!c) return fail(VE_ERR_INVALID, "render_batch: null context");
     cudaSetDevice(c->device);
     return render_batch(c, views, n, outs);
+}
+
+int ve_get_launch_config(ve_ctx* c, ve_launch_config* cfg) {
+    if (!c || !cfg) return fail(VE_ERR_INVALID, "get_launch_config: null argument");
+    *cfg = c->launch;
+    return VE_OK;
+}
+
+int ve_set_launch_config(ve_ctx* c, const ve_launch_config* cfg) {
+    if (!c || !cfg) return fail(VE_ERR_INVALID, "set_launch_config: null argument");
+    if (cfg->refill_threshold > 32) return fail(VE_ERR_INVALID, "set_launch_config: refill_threshold must be <= 32");
+    c->launch = *cfg;
+    apply_launch(c);
+    return VE_OK;
+}
+
+int ve_autotune(ve_ctx* c, const ve_view* views, uint32_t nv, uint32_t frames, ve_launch_config* best) {
+    if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "autotune: no views");
+    if (frames == 0) frames = 2;
+    cudaSetDevice(c->device);
+    std::vector<ve_view> tv(views, views + nv);
+    for (auto& v : tv) v.frame.flags = (v.frame.flags | VE_FRAME_TIMING) & ~VE_FRAME_PATH_RGB;
+    auto measure = [&](const ve_launch_config& cfg, float* ms) -> int {
+        c->launch = cfg;
+        apply_launch(c);
+        int rc = render_batch(c, tv.data(), nv, nullptr);  // warm-up at this shape
+        if (rc) return rc;
+        VE_CUDA(cudaStreamSynchronize(c->stream));
+        collect_all_timing(c);
+        const float t0 = c->tot_ms[0];
+        for (uint32_t f = 0; f < frames; f++)
+            if ((rc = render_batch(c, tv.data(), nv, nullptr))) return rc;
+        VE_CUDA(cudaStreamSynchronize(c->stream));
+        collect_all_timing(c);
+        *ms = (c->tot_ms[0] - t0) / float(frames);
+        return VE_OK;
+    };
+    ve_launch_config cur{uint32_t(c->occ_trace), uint32_t(c->occ_shade), 8, 0};
+    float best_ms = 0.0f;
+    int rc = measure(cur, &best_ms);
+    if (rc) return rc;
+    // coordinate descent: trace blocks/SM, shade blocks/SM, refill threshold
+    for (int tb = 1; tb <= c->occ_trace; tb++) {
+        ve_launch_config t = cur;
+        t.trace_blocks_per_sm = uint32_t(tb);
+        float ms = 0;
+        if ((rc = measure(t, &ms))) return rc;
+        if (ms < best_ms) { best_ms = ms; cur = t; }
+    }
+    for (int sb = 1; sb <= c->occ_shade; sb++) {
+        ve_launch_config t = cur;
+        t.shade_blocks_per_sm = uint32_t(sb);
+        float ms = 0;
+        if ((rc = measure(t, &ms))) return rc;
+        if (ms < best_ms) { best_ms = ms; cur = t; }
+    }
+    for (uint32_t thr : {2u, 4u, 8u, 12u, 16u, 24u}) {
+        ve_launch_config t = cur;
+        t.refill_threshold = thr;
+        float ms = 0;
+        if ((rc = measure(t, &ms))) return rc;
+        if (ms < best_ms) { best_ms = ms; cur = t; }
+    }
+    c->launch = cur;
+    apply_launch(c);
+    if (best) *best = cur;
+    return VE_OK;
 }
 
 static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
@@ -1594,3 +1807,5 @@ int ve_fill_normals_noalloc(uint32_t* words, uint64_t n_words, uint32_t depth, v
 }
 
 }  // extern "C"
+
+#include "serve.cuh"

@@ -172,17 +172,22 @@ __device__ __forceinline__ f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float r
     if (NdotL < 0.001f) return mk(0.0f, 0.0f, 0.0f);
     const float rc = gmax(roughness, 0.01f);
     const float spec_exp = 2.0f / (rc * rc);
-    const f3 H = normalize(sub(L, V));
-    const float NdotH = gmax(dot(N, H), 0.001f);
-    const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
     const float kS = specular_intensity * metallic;
-    // the lobe is multiplied by kS: with kS == 0 the product is +0 for every
-    // finite NdotH (pow of a value in [0.001, 1+eps] is finite) and NaN when
-    // NdotH is NaN, which (NdotH - NdotH) reproduces without calling powf
-    const float specular = kS != 0.0f ? spec_norm * powf(NdotH, spec_exp) : spec_norm * (NdotH - NdotH);
     const float kD = 1.0f - kS * 0.5f;
     const f3 diffuse = muls(muls(albedo, kD), 0.31831f);
-    const float sp = specular * kS;
+    float sp;
+    if (kS != 0.0f) {
+        const f3 H = normalize(sub(L, V));
+        const float NdotH = gmax(dot(N, H), 0.001f);
+        const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
+        sp = (spec_norm * powf(NdotH, spec_exp)) * kS;
+    } else {
+        // The lobe is multiplied by kS = 0: the product is +0 whenever the
+        // half vector is finite, i.e. whenever |L - V|^2 > 0 (N, L, V are
+        // finite unit vectors), and NaN otherwise (0/0 in the normalise).
+        const f3 lv = sub(L, V);
+        sp = dot(lv, lv) > 0.0f ? 0.0f : __int_as_float(0x7fc00000);
+    }
     return muls(mk(diffuse.x + sp, diffuse.y + sp, diffuse.z + sp), NdotL);
 }
 
@@ -245,7 +250,25 @@ __device__ __forceinline__ uint32_t pack1022(float c) {
     v = v < 0 ? 0 : (v > 1022 ? 1022 : v);
     return uint32_t(v);
 }
+// Shading normals of every stored gradient (19^3 codes), built on the host
+// with the same single-precision operations as shading_normal_compute.
+__device__ float4 g_normal_table[19 * 19 * 19];
+
+__device__ __forceinline__ f3 shading_normal_compute(uint32_t leaf_word, f3 ray_dir);
+
 __device__ __forceinline__ f3 shading_normal(uint32_t leaf_word, f3 ray_dir) {
+    if (leaf_word >> 31) {
+        const int ix = sext5((leaf_word >> 8) & 31u), iy = sext5((leaf_word >> 13) & 31u),
+                  iz = sext5((leaf_word >> 18) & 31u);
+        if (ix >= -9 && ix <= 9 && iy >= -9 && iy <= 9 && iz >= -9 && iz <= 9) {
+            const float4 n = __ldg(&g_normal_table[((ix + 9) * 19 + (iy + 9)) * 19 + (iz + 9)]);
+            return mk(n.x, n.y, n.z);
+        }
+    }
+    return shading_normal_compute(leaf_word, ray_dir);
+}
+
+__device__ __forceinline__ f3 shading_normal_compute(uint32_t leaf_word, f3 ray_dir) {
     if (!(leaf_word >> 31)) {
         const float ax = fabsf(ray_dir.x), ay = fabsf(ray_dir.y), az = fabsf(ray_dir.z);
         if (ax > ay && ax > az) return mk(-sgnf(ray_dir.x), 0.0f, 0.0f);

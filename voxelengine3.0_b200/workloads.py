@@ -61,6 +61,36 @@ def orbit_camera(frame: int, n_frames: int = 64, seed: int = 1, radius: float = 
     return eye.astype(np.float32), (d / np.linalg.norm(d)).astype(np.float32)
 
 
+# Batching workload: 64 views over 4 resident octrees of depth 8, 9, 10, 10
+# (seeded terrain with overhangs), resolutions drawn from BATCH_RESOLUTIONS,
+# spp uniform 1-8, bounces uniform 1-4, random poses.
+BATCH_RESOLUTIONS = [(128, 128), (256, 256), (640, 360), (1280, 720), (1920, 1080)]
+BATCH_SCENES = [(8, 1, 11), (9, 1, 12), (10, 1, 13), (10, 1, 14)]  # (depth, variant, seed)
+
+
+def random_pose(rng, depth: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Eye on a circle of radius 0.6 L at height 0.2-0.35 L, looking at the
+    terrain centre (heights are 64 +- 48 at every depth)."""
+    L = float(1 << depth)
+    th = float(rng.uniform(0.0, 2.0 * math.pi))
+    eye = np.array([L / 2 + 0.6 * L * math.cos(th), float(rng.uniform(0.2, 0.35)) * L, L / 2 + 0.6 * L * math.sin(th)])
+    target = np.array([L / 2 + float(rng.uniform(-0.1, 0.1)) * L, 64.0, L / 2 + float(rng.uniform(-0.1, 0.1)) * L])
+    d = target - eye
+    return eye.astype(np.float32), (d / np.linalg.norm(d)).astype(np.float32)
+
+
+def batching_views(n: int = 64, seed: int = 7) -> List[dict]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        sc = int(rng.integers(0, len(BATCH_SCENES)))
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+        eye, d = random_pose(rng, BATCH_SCENES[sc][0])
+        out.append({"scene": sc, "width": w, "height": h, "spp": int(rng.integers(1, 9)),
+                    "bounces": int(rng.integers(1, 5)), "eye": eye, "dir": d, "frame": i})
+    return out
+
+
 def camera_sequence(w: Workload) -> List[Tuple[np.ndarray, np.ndarray]]:
     if w.name == "small":
         return [small_camera()] * w.frames
