@@ -292,6 +292,178 @@ def run_batching(args, rank, world):
     return 0
 
 
+def _pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(math.ceil(q / 100.0 * len(xs))) - 1))
+    return xs[k]
+
+
+def run_serving(args, rank, world):
+    """Render server under a Poisson request stream at 80% of its measured
+    capacity: 8 resident octrees of depth 8-11, requests with resolutions
+    128^2..1080p, spp 1-16, bounces 1-4.  Capacity is measured first in a
+    closed loop (32 requests outstanding); the open-loop stream then submits
+    args.requests requests with exponential inter-arrival gaps.  Results go
+    to pinned host buffers.  Latency = completion - scheduled arrival.  Serial
+    plain rendering (one ve_render per request, same outputs) of a bounded
+    prefix of the same requests is the comparison."""
+    import ctypes
+    import queue
+    import threading
+
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=900.0, device=local)
+    torch.cuda.set_device(local)
+    r = ve.Renderer(device=local, hash_log2=22)
+    r.set_materials(ve.terrain_materials(1))
+    sids, scene_desc = [], []
+    for depth, variant, seed in wl.SERVING_SCENES:
+        w, nv = ve.terrain_words(depth, variant, seed)
+        sids.append(r.upload_scene(w, depth))
+        scene_desc.append({"depth": depth, "variant": variant, "voxels": int(nv), "node_words": int(len(w))})
+        del w
+    reqs = wl.serving_requests(args.requests, seed=5 + rank)
+    jobs = []
+    for q in reqs:
+        cam = ve.camera_ubo(q["eye"], q["dir"], 70.0, q["width"] / q["height"])
+        fc = ve.FrameConfig(width=q["width"], height=q["height"], spp=q["spp"], bounces=q["bounces"],
+                            frame_index=q["frame"], primary_controlchecks=300, bounce_controlchecks=300, decay=1.0)
+        jobs.append((sids[q["scene"]], cam, fc))
+    max_px = max(w * h for w, h in wl.BATCH_RESOLUTIONS)
+    n_buf = 48
+    pool = queue.Queue()
+    bufs = []
+    for i in range(n_buf):
+        hv = torch.empty(max_px, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        hr = torch.empty(3 * max_px, dtype=torch.float32, pin_memory=True).numpy()
+        bufs.append((hv, hr))
+        pool.put(i)
+    cfg = {"pixel_capacity": 8 * max_px, "path_capacity": 1 << 27, "max_requests": 64}
+    srv = ve.Server(r, **cfg)
+    st0 = srv.stats()
+
+    def serve(order, arrivals):
+        """Submits jobs[order[i]] at arrivals[i] (None: as soon as a buffer is
+        free); returns per-request records and the wall time."""
+        done = []
+        inflight = queue.Queue()
+
+        def waiter():
+            while True:
+                item = inflight.get()
+                if item is None:
+                    return
+                rid, b, t_arr, j = item
+                info = srv.wait(rid, timeout_ms=600000)
+                pool.put(b)
+                done.append((j, t_arr, info))
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.monotonic()
+        s0 = srv.stats()["rays"]
+        for i, j in enumerate(order):
+            t_arr = None
+            if arrivals is not None:
+                t_arr = t0 + arrivals[i]
+                dt = t_arr - time.monotonic()
+                if dt > 0:
+                    time.sleep(dt)
+            b = pool.get()
+            sid, cam, fc = jobs[j]
+            hv, hr = bufs[b]
+            rid = srv.submit(sid, cam, fc, out_vid=hv, out_rgb=hr)
+            inflight.put((rid, b, t_arr, j))
+        inflight.put(None)
+        th.join()
+        wall = time.monotonic() - t0
+        return done, wall, srv.stats()["rays"] - s0
+
+    # 1. capacity: closed loop, at most n_buf outstanding
+    n_cap = min(len(jobs), args.capacity_requests)
+    done, wall, rays = serve(list(range(n_cap)), None)
+    capacity_rps = n_cap / wall
+    cap_mrays = rays / wall / 1e6
+    # 2. Poisson stream at 80% of capacity
+    rate = 0.8 * capacity_rps
+    rng = np.random.default_rng(99 + rank)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs))).tolist()
+    with ClockSampler(local) as clk:
+        done, wall, rays = serve(list(range(len(jobs))), arrivals)
+    lat = [info["done_s"] - t_arr for (_, t_arr, info) in done]
+    svc = [info["done_s"] - info["admit_s"] for (_, _, info) in done]
+    qwait = [info["admit_s"] - info["submit_s"] for (_, _, info) in done]
+    stats = srv.stats()
+    srv.close()
+    # 3. serial plain rendering of a bounded prefix (ve_render per request)
+    lib = ve.load_library()
+    hv, hr = bufs[0]
+    outs = ve.FrameOutputsC()
+    outs.voxel_id = hv.ctypes.data
+    outs.rgb = hr.ctypes.data
+    r.reset_total_stats()
+    t0 = time.monotonic()
+    serial_lat = []
+    n_serial = 0
+    for j in range(len(jobs)):
+        if n_serial >= args.serial_requests or time.monotonic() - t0 > args.serial_seconds:
+            break
+        sid, cam, fc = jobs[j]
+        v = ve.Renderer.make_view(sid, cam, fc)
+        t1 = time.monotonic()
+        rc = lib.ve_render(r._h, ctypes.byref(v), ctypes.byref(outs))
+        if rc != 0:
+            raise RuntimeError(lib.ve_last_error().decode())
+        serial_lat.append(time.monotonic() - t1)
+        n_serial += 1
+    serial_wall = time.monotonic() - t0
+    serial_rays = rays_of(r.total_stats())
+    r.close()
+    mrays = rays / wall / 1e6
+    line = {"metric": "served p50/p99 latency (Poisson at 80% of capacity) and Mrays/s",
+            "value": mrays, "unit": "Mrays/s", "n_gpus": world, "steps": len(jobs), "warmup": n_cap,
+            "ms_per_step": 1e3 * wall / len(jobs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, requests and arrivals)",
+            "config": {"workload": "serving: 8 resident octrees depth 8/9/10/11 x2, resolutions "
+                                   "{128^2,256^2,640x360,1280x720,1920x1080}, spp 1-16, bounces 1-4, "
+                                   f"{len(jobs)} requests, Poisson at 80% of measured capacity",
+                       "scenes": scene_desc, "server": cfg,
+                       "hbm_budget_bytes": stats["pool_bytes"] + stats["scene_bytes"]},
+            "latency_ms": {"p50": 1e3 * _pct(lat, 50), "p90": 1e3 * _pct(lat, 90), "p99": 1e3 * _pct(lat, 99),
+                           "max": 1e3 * max(lat)},
+            "service_ms": {"p50": 1e3 * _pct(svc, 50), "p99": 1e3 * _pct(svc, 99)},
+            "queue_ms": {"p50": 1e3 * _pct(qwait, 50), "p99": 1e3 * _pct(qwait, 99)},
+            "capacity": {"requests_per_s": capacity_rps, "mrays_s": cap_mrays, "requests": n_cap},
+            "offered_requests_per_s": rate, "achieved_requests_per_s": len(jobs) / wall,
+            "max_in_flight": stats["max_in_flight"], "server_steps": stats["steps"],
+            "serial_plain": {"requests": n_serial, "mrays_s": serial_rays / serial_wall / 1e6,
+                             "requests_per_s": n_serial / serial_wall,
+                             "latency_ms_p50": 1e3 * _pct(serial_lat, 50),
+                             "latency_ms_p99": 1e3 * _pct(serial_lat, 99)},
+            "clocks": clk.summary()}
+    lines = [None] * world
+    if world > 1:
+        import torch.distributed as td
+        td.all_gather_object(lines, line)
+    else:
+        lines = [line]
+    if rank == 0:
+        if world > 1:
+            line["value"] = sum(x["value"] for x in lines)
+            line["per_rank_p99_ms"] = [x["latency_ms"]["p99"] for x in lines]
+        print(json.dumps(line), flush=True)
+    vd.shutdown(dist)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,7 +472,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving"], default="large")
+    ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
+    ap.add_argument("--capacity-requests", type=int, default=400, help="serving: closed-loop capacity sample")
+    ap.add_argument("--serial-requests", type=int, default=400, help="serving: serial plain comparison sample")
+    ap.add_argument("--serial-seconds", type=float, default=20.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -316,6 +492,8 @@ def main():
         return run_reference(args, W, rank, world)
     if args.workload == "batching":
         return run_batching(args, rank, world)
+    if args.workload == "serving":
+        return run_serving(args, rank, world)
 
     import torch
 

@@ -264,6 +264,7 @@ typedef struct ve_request_info {
 typedef struct ve_server_stats {
     uint64_t completed, admitted, queued, in_flight, max_in_flight, steps;
     uint64_t pool_bytes, scene_bytes;
+    uint64_t rays; /* primary + bounce + shadow rays traced since creation */
 } ve_server_stats;
 int ve_server_create(ve_ctx* ctx, const ve_server_config* cfg, ve_server** out);
 /* voxel_id_out (1 x u32 per pixel) and rgb_out (3 x f32 per pixel) may be NULL;

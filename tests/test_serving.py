@@ -86,18 +86,22 @@ def test_late_arrivals_overlap_with_requests_on_the_gpu(ve, world):
     sid, depth = scenes[1]
     w = helpers.workloads()
     eye, d = w.random_pose(np.random.default_rng(9), depth)
-    big = (sid, ve.camera_ubo(eye, d, 70.0, 1.0), ve.FrameConfig(width=512, height=512, spp=16, bounces=4,
+    big = (sid, ve.camera_ubo(eye, d, 70.0, 1.0), ve.FrameConfig(width=1024, height=1024, spp=8, bounces=4,
                                                                    primary_controlchecks=200,
                                                                    bounce_controlchecks=200))
-    with ve.Server(r, pixel_capacity=1 << 20, path_capacity=1 << 23, max_requests=16) as srv:
+    with ve.Server(r, pixel_capacity=1 << 21, path_capacity=1 << 24, max_requests=16) as srv:
         b = srv.submit(*big)
-        time.sleep(0.002)
+        t_end = time.monotonic() + 10.0
+        while srv.stats()["steps"] < 1 and time.monotonic() < t_end:  # the big request is on the GPU
+            time.sleep(1e-4)
         small = [srv.submit(*q) for q in reqs[:4]]
         rs = [srv.wait(i) for i in small]
         rb = srv.wait(b)
         st = srv.stats()
-    # small requests were admitted while the big one was still on the GPU
-    assert all(x["admit_s"] < rb["done_s"] for x in rs)
+    # the small requests arrived after the big one was admitted and joined it
+    # on the GPU before it finished
+    assert all(x["submit_s"] > rb["admit_s"] for x in rs)
+    assert all(x["admit_s"] < rb["done_s"] for x in rs), ([x["admit_s"] for x in rs], rb)
     assert st["max_in_flight"] >= 2
     assert st["completed"] == 5
 

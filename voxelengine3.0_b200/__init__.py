@@ -107,7 +107,7 @@ class RequestInfoC(ctypes.Structure):
 
 class ServerStatsC(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("completed", "admitted", "queued", "in_flight", "max_in_flight",
-                                               "steps", "pool_bytes", "scene_bytes")]
+                                               "steps", "pool_bytes", "scene_bytes", "rays")]
 
 
 _P = ctypes.c_void_p
@@ -605,10 +605,24 @@ class Server:
         self._buffers: Dict[int, tuple] = {}
 
     def submit(self, scene_id: int, camera: np.ndarray, fc: FrameConfig, want_vid: bool = True,
-               want_rgb: bool = True) -> int:
+               want_rgb: bool = True, out_vid: Optional[np.ndarray] = None,
+               out_rgb: Optional[np.ndarray] = None) -> int:
+        """Queues one frame request.  Results land in freshly allocated arrays,
+        or in `out_vid` (u32, >= W*H) / `out_rgb` (f32, >= 3*W*H) when given
+        (e.g. views of pinned host memory); those must outlive the request."""
         view = Renderer.make_view(scene_id, camera, fc)
-        vid = np.zeros((fc.height, fc.width), np.uint32) if want_vid else None
-        rgb = np.zeros((fc.height, fc.width, 3), np.float32) if want_rgb else None
+        npx = fc.width * fc.height
+        vid = rgb = None
+        if out_vid is not None:
+            assert out_vid.dtype == np.uint32 and out_vid.size >= npx and out_vid.flags.c_contiguous
+            vid = out_vid
+        elif want_vid:
+            vid = np.zeros((fc.height, fc.width), np.uint32)
+        if out_rgb is not None:
+            assert out_rgb.dtype == np.float32 and out_rgb.size >= 3 * npx and out_rgb.flags.c_contiguous
+            rgb = out_rgb
+        elif want_rgb:
+            rgb = np.zeros((fc.height, fc.width, 3), np.float32)
         rid = _U64()
         _check(self._lib.ve_server_submit(self._h, ctypes.byref(view), _ptr(vid), _ptr(rgb), ctypes.byref(rid)))
         self._buffers[rid.value] = (vid, rgb)

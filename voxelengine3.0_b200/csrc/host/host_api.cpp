@@ -140,7 +140,7 @@ int ve_terrain_build(uint32_t depth, uint32_t variant, uint64_t seed, uint32_t t
                      uint64_t* n_voxels) {
     if (!out) return hfail(VE_ERR_INVALID, "terrain_build: null output");
     if (depth < 1 || depth > 11) return hfail(VE_ERR_INVALID, "terrain_build: depth must be in [1, 11]");
-    if (variant > 1) return hfail(VE_ERR_INVALID, "terrain_build: variant must be 0 or 1");
+    if (variant > 2) return hfail(VE_ERR_INVALID, "terrain_build: variant must be 0, 1 or 2");
     ve_words* w = new ve_words();
     w->w = ve::build_terrain_words(ve::TerrainParams{depth, variant, seed}, threads, n_voxels);
     if (w->w.empty()) {

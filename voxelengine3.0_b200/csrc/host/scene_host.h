@@ -102,6 +102,10 @@ private:
 //   variant 1 ("overhang"): the same heightfield plus 3 octaves of 3D value
 //       noise: solid iff y+0.5 < h(x,z) + 16*fBm3((x,y,z)+0.5)/24) — carves
 //       overhangs and caves within +-16 voxels of the surface.
+//   variant 2 ("island"): variant 1 restricted to the central 1024 x 1024
+//       columns (the whole scene up to depth 10).  A depth-11 scene of this
+//       family: the full-extent terrain at depth 11 holds ~270M solid voxels,
+//       more leaf slots than the layout's 28-bit `next` field addresses.
 // material = 1 + (hash(x, y, z, seed) mod 8).
 struct TerrainParams {
     uint32_t depth;

@@ -106,19 +106,25 @@ void parallel_for(uint32_t n, uint32_t threads, const std::function<void(uint32_
 
 // ---------------------------------------------------------------------------
 TerrainField::TerrainField(const TerrainParams& p) : p_(p), L_(1u << p.depth) {
-    band_ = p.variant == 1 ? 16.0f : 0.0f;
+    band_ = p.variant != 0 ? 16.0f : 0.0f;
     heights_.resize(size_t(L_) * L_);
     const uint32_t sh = seed32(p.seed, 0x4845u);
     for (uint32_t z = 0; z < L_; z++)
         for (uint32_t x = 0; x < L_; x++)
             heights_[size_t(z) * L_ + x] =
                 float(64.0 + 32.0 * fbm2((x + 0.5) / 32.0, (z + 0.5) / 32.0, 4, sh));
+    if (p.variant == 2 && L_ > 1024u) {  // island: columns outside the central 1024 x 1024 hold nothing
+        const uint32_t lo = (L_ - 1024u) / 2u;
+        for (uint32_t z = 0; z < L_; z++)
+            for (uint32_t x = 0; x < L_; x++)
+                if (x < lo || z < lo || x >= lo + 1024u || z >= lo + 1024u) heights_[size_t(z) * L_ + x] = -1.0e6f;
+    }
 }
 
 bool TerrainField::solid(uint32_t x, uint32_t y, uint32_t z) const {
     const double yc = double(y) + 0.5;
     const double h = double(height(x, z));
-    if (p_.variant != 1) return yc < h;
+    if (p_.variant == 0) return yc < h;
     const double A = band_;
     if (yc < h - A) return true;
     if (yc >= h + A) return false;

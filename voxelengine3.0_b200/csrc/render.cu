@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
 // serves all idle lanes of the warp, once `refill` of them are idle or none is
 // busy), so warps stay full although ray lengths differ by 100x.
 template <bool COUNT>
-__global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
@@ -332,7 +332,6 @@ __global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t* nodes = nullptr;
     uint64_t n_words = 0;
     Dda s;
-    uint32_t base[17];
     Hit h;
     RayCount rc;
     for (;;) {
@@ -358,7 +357,7 @@ __global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
                     D = S.depth;
                     const f3 o = ld3(a.p_ray_o[p]);
                     const f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
-                    finished = dda_init<COUNT>(s, base, o, d, v.cc_bounce, D, h, rc);
+                    finished = dda_init(s, o, d, v.cc_bounce, D, h);
                     active = !finished;
                 } else {
                     exhausted = true;
@@ -366,7 +365,7 @@ __global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_iter<COUNT>(s, base, nodes, n_words, D, h, rc);
+            finished = dda_step<COUNT>(s, nodes, n_words, D, h, rc);
             if (finished) active = false;
         }
         if (finished) {

@@ -111,11 +111,11 @@ struct ve_server {
     ve::RangePool pix_pool, path_pool;
     uint32_t* d_remaining = nullptr;
     uint32_t* h_remaining = nullptr;  // pinned
-    uint32_t* h_counters = nullptr;   // pinned
+    unsigned long long* h_stats = nullptr;  // pinned copy of the context's per-kind ray counters
     ve::DevView* h_view = nullptr;    // pinned staging, one per slot
     uint64_t step = 0;
     // stats
-    uint64_t completed = 0, steps_run = 0, max_inflight = 0, admitted = 0;
+    uint64_t completed = 0, steps_run = 0, max_inflight = 0, admitted = 0, rays = 0;
 };
 
 namespace ve {
@@ -235,10 +235,10 @@ static void serve_loop(ve_server* s) {
             cudaMemcpyAsync(c->counters.p + CNT_LIVE, c->counters.p + CNT_LIVE + kRing, 4, cudaMemcpyDeviceToDevice,
                             st);
         s->step++;
-        s->steps_run++;
         // 3. completion: remaining path counts per slot
         cudaMemcpyAsync(s->h_remaining, s->d_remaining, sizeof(uint32_t) * s->cfg.max_requests,
                         cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(s->h_stats, c->stats.p, sizeof(unsigned long long) * ST_TOTAL, cudaMemcpyDeviceToHost, st);
         const cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             serve_fail(s, VE_ERR_CUDA, std::string("serve step: ") + cudaGetErrorString(e));
@@ -247,6 +247,8 @@ static void serve_loop(ve_server* s) {
         std::vector<ServeRequest*> finished;
         {
             std::lock_guard<std::mutex> lk(s->mu);
+            s->rays = s->h_stats[ST_RAYS_PRIMARY] + s->h_stats[ST_RAYS_BOUNCE] + s->h_stats[ST_RAYS_SHADOW];
+            s->steps_run++;
             for (size_t i = 0; i < s->active.size();) {
                 ServeRequest* r = s->active[i];
                 if (r->state == 1 && s->h_remaining[r->slot] == 0) {
@@ -316,7 +318,7 @@ int ve_server_create(ve_ctx* c, const ve_server_config* cfg, ve_server** out) {
     if (cudaMalloc(&s->d_remaining, 4ull * cfg->max_requests) != cudaSuccess ||
         cudaMallocHost(&s->h_remaining, 4ull * cfg->max_requests) != cudaSuccess ||
         cudaMallocHost(&s->h_view, sizeof(DevView) * cfg->max_requests) != cudaSuccess ||
-        cudaMallocHost(&s->h_counters, 4ull * CNT_TOTAL) != cudaSuccess) {
+        cudaMallocHost(&s->h_stats, sizeof(unsigned long long) * ST_TOTAL) != cudaSuccess) {
         ve_server_destroy(s);
         return fail(VE_ERR_NOMEM, "server_create: allocation failed");
     }
@@ -410,6 +412,7 @@ int ve_server_get_stats(ve_server* s, ve_server_stats* out) {
     for (const auto& sc : s->c->scenes)
         if (sc.live) scene_bytes += (sc.n_words + 8) * 4 + (sizeof(CacheEntry) << s->c->cfg.hash_log2);
     out->scene_bytes = scene_bytes;
+    out->rays = s->rays;
     return VE_OK;
 }
 
@@ -428,7 +431,7 @@ int ve_server_destroy(ve_server* s) {
     if (s->d_remaining) cudaFree(s->d_remaining);
     if (s->h_remaining) cudaFreeHost(s->h_remaining);
     if (s->h_view) cudaFreeHost(s->h_view);
-    if (s->h_counters) cudaFreeHost(s->h_counters);
+    if (s->h_stats) cudaFreeHost(s->h_stats);
     const int err = s->error;
     delete s;
     return err;

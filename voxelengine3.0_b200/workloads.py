@@ -91,6 +91,26 @@ def batching_views(n: int = 64, seed: int = 7) -> List[dict]:
     return out
 
 
+# Serving workload: 8 resident octrees of depth 8-11 (two per depth; depth 11
+# is the "island" variant, the overhang terrain on the central 1024^2
+# columns, because the full-extent depth-11 terrain needs more than 2^28 node
+# slots), requests {scene uniform, resolution from BATCH_RESOLUTIONS, spp 1-16,
+# bounces 1-4, seeded pose}.
+SERVING_SCENES = [(8, 1, 31), (9, 1, 32), (10, 1, 33), (11, 2, 34), (8, 1, 35), (9, 1, 36), (10, 1, 37), (11, 2, 38)]
+
+
+def serving_requests(n: int = 10000, seed: int = 5) -> List[dict]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        sc = int(rng.integers(0, len(SERVING_SCENES)))
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+        eye, d = random_pose(rng, SERVING_SCENES[sc][0])
+        out.append({"scene": sc, "width": w, "height": h, "spp": int(rng.integers(1, 17)),
+                    "bounces": int(rng.integers(1, 5)), "eye": eye, "dir": d, "frame": i})
+    return out
+
+
 def camera_sequence(w: Workload) -> List[Tuple[np.ndarray, np.ndarray]]:
     if w.name == "small":
         return [small_camera()] * w.frames
