@@ -43,6 +43,9 @@ extern "C" {
 #define VE_FRAME_TIMING 1u        /* per-pass CUDA-event times into ve_frame_stats */
 #define VE_FRAME_COUNT_FETCH 2u   /* count node-word fetches on the device */
 #define VE_FRAME_PATH_RGB 4u      /* keep every path's deposit value (debug) */
+#define VE_FRAME_LEARNED 8u       /* end paths at their second vertex with the scene's learned cache */
+#define VE_FRAME_TERMINATE_HASH 16u /* end paths at their second vertex with the hashed per-voxel cache */
+#define VE_FRAME_TRAIN 32u        /* record training samples and train the scene's learned cache */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
                                      replaying a CUDA graph of the frame's kernel sequence */
 
@@ -111,6 +114,11 @@ typedef struct ve_frame_stats {
     float ms_total, ms_primary, ms_trace, ms_shade, ms_resolve, ms_decay; /* VE_FRAME_TIMING */
     uint32_t trace_launches, kernel_launches;
     uint64_t cache_capacity;
+    uint64_t nrc_queries;         /* paths ended by the learned cache */
+    uint64_t nrc_hash_terminated; /* paths ended by the hashed per-voxel cache */
+    uint64_t nrc_samples;         /* training samples recorded */
+    float ms_learned;             /* learned-cache inference + training (VE_FRAME_TIMING) */
+    uint32_t reserved;
 } ve_frame_stats;
 
 typedef struct ve_ctx ve_ctx;
@@ -277,6 +285,55 @@ int ve_server_wait(ve_server* s, uint64_t request_id, uint32_t timeout_ms, ve_re
 int ve_server_get_stats(ve_server* s, ve_server_stats* stats);
 /* finishes queued and in-flight requests, then stops the worker */
 int ve_server_destroy(ve_server* s);
+
+/* ======================================================================
+ * Learned radiance cache (no counterpart in the reference)
+ *
+ * A multi-resolution hash-grid encoding (16 levels x 2 fp16 features) of the
+ * voxel position, the octahedral shading normal and the octahedral view
+ * direction feed a 4 x 64 ReLU MLP with a 3-channel output, evaluated and
+ * trained with bf16 tensor-core kernels (f32 accumulation, Adam).  Attached to
+ * a scene (ve_scene_set_nrc), it terminates paths at their second vertex in
+ * frames rendered with VE_FRAME_LEARNED and trains online on the paths of
+ * frames rendered with VE_FRAME_TRAIN.
+ * ==================================================================== */
+typedef struct ve_nrc ve_nrc;
+typedef struct ve_nrc_config {
+    uint32_t log2_table;      /* entries per hash-grid level, log2 (19) */
+    uint32_t base_resolution; /* coarsest grid resolution (16) */
+    uint32_t max_resolution;  /* finest grid resolution (2048) */
+    uint32_t train_samples;   /* training samples per frame (65536) */
+    float learning_rate;      /* Adam step size (1e-2) */
+    float beta1, beta2, eps;  /* Adam moments (0.9, 0.99, 1e-8) */
+    float fallback_threshold; /* per-cell validation error above which the hash cache answers (0.1) */
+    uint32_t flags;
+    uint64_t seed;            /* parameter initialisation */
+} ve_nrc_config;
+typedef struct ve_nrc_input {
+    float pos[3];        /* voxel centre / scene extent, in [0,1)^3 */
+    uint32_t reserved;
+    float normal_oct[2]; /* octahedral shading normal */
+    float view_oct[2];   /* octahedral direction toward the previous path vertex */
+} ve_nrc_input;
+int ve_nrc_create(ve_ctx* ctx, const ve_nrc_config* cfg, ve_nrc** out);
+int ve_nrc_destroy(ve_nrc* nrc);
+/* weights: 5 x 64 x 64 f32 (layer 5 uses rows 0-2); table: 16 x 2^log2_table x 2 f32 */
+int ve_nrc_param_counts(const ve_nrc* nrc, uint64_t* n_weights, uint64_t* n_table);
+int ve_nrc_get_params(ve_nrc* nrc, float* weights, float* table);
+/* replaces the parameters and restarts the optimiser */
+int ve_nrc_set_params(ve_nrc* nrc, const float* weights, const float* table);
+/* rgb: n x 3 predictions */
+int ve_nrc_infer(ve_nrc* nrc, const ve_nrc_input* in, uint32_t n, float* rgb);
+/* gradients of the mean relative L2 loss over the n samples, without an update */
+int ve_nrc_gradients(ve_nrc* nrc, const ve_nrc_input* in, const float* target, uint32_t n, float* weight_grad,
+                     float* table_grad, float* loss);
+/* one Adam step on the n samples; loss before the step */
+int ve_nrc_train(ve_nrc* nrc, const ve_nrc_input* in, const float* target, uint32_t n, float* loss);
+/* mean training loss of the last training step (learned frames or
+ * ve_nrc_train), its sample count, and the number of steps taken */
+int ve_nrc_stats(ve_nrc* nrc, float* loss, uint64_t* samples, uint64_t* steps);
+/* attaches (or, with NULL, detaches) a learned cache to a scene */
+int ve_scene_set_nrc(ve_ctx* ctx, int scene_id, ve_nrc* nrc);
 
 /* ======================================================================
  * Allocation-free entry point (no counterpart in the reference)

@@ -43,6 +43,9 @@ SCENE_KEEP_NORMALS = 1
 FRAME_TIMING = 1
 FRAME_COUNT_FETCH = 2
 FRAME_PATH_RGB = 4
+FRAME_LEARNED = 8
+FRAME_TERMINATE_HASH = 16
+FRAME_TRAIN = 32
 CFG_NO_GRAPHS = 1
 
 
@@ -92,7 +95,9 @@ class FrameStatsC(ctypes.Structure):
                 ("ms_total", ctypes.c_float), ("ms_primary", ctypes.c_float), ("ms_trace", ctypes.c_float),
                 ("ms_shade", ctypes.c_float), ("ms_resolve", ctypes.c_float), ("ms_decay", ctypes.c_float),
                 ("trace_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
-                ("cache_capacity", ctypes.c_uint64)]
+                ("cache_capacity", ctypes.c_uint64), ("nrc_queries", ctypes.c_uint64),
+                ("nrc_hash_terminated", ctypes.c_uint64), ("nrc_samples", ctypes.c_uint64),
+                ("ms_learned", ctypes.c_float), ("reserved", ctypes.c_uint32)]
 
 
 class ServerConfigC(ctypes.Structure):
@@ -108,6 +113,14 @@ class RequestInfoC(ctypes.Structure):
 class ServerStatsC(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("completed", "admitted", "queued", "in_flight", "max_in_flight",
                                                "steps", "pool_bytes", "scene_bytes", "rays")]
+
+
+class NrcConfigC(ctypes.Structure):
+    _fields_ = [("log2_table", ctypes.c_uint32), ("base_resolution", ctypes.c_uint32),
+                ("max_resolution", ctypes.c_uint32), ("train_samples", ctypes.c_uint32),
+                ("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("eps", ctypes.c_float), ("fallback_threshold", ctypes.c_float), ("flags", ctypes.c_uint32),
+                ("seed", ctypes.c_uint64)]
 
 
 _P = ctypes.c_void_p
@@ -161,6 +174,16 @@ _SIGNATURES = {
     "ve_get_total_stats": ([_P, _PTR(FrameStatsC)], ctypes.c_int),
     "ve_fill_normals_noalloc": ([_P, _U64, _U32, _P], ctypes.c_int),
     "ve_get_launch_config": ([_P, _PTR(LaunchConfigC)], ctypes.c_int),
+    "ve_nrc_create": ([_P, _PTR(NrcConfigC), _PTR(_P)], ctypes.c_int),
+    "ve_nrc_destroy": ([_P], ctypes.c_int),
+    "ve_nrc_param_counts": ([_P, _PTR(_U64), _PTR(_U64)], ctypes.c_int),
+    "ve_nrc_get_params": ([_P, _P, _P], ctypes.c_int),
+    "ve_nrc_set_params": ([_P, _P, _P], ctypes.c_int),
+    "ve_nrc_infer": ([_P, _P, _U32, _P], ctypes.c_int),
+    "ve_nrc_gradients": ([_P, _P, _P, _U32, _P, _P, _PTR(ctypes.c_float)], ctypes.c_int),
+    "ve_nrc_train": ([_P, _P, _P, _U32, _PTR(ctypes.c_float)], ctypes.c_int),
+    "ve_scene_set_nrc": ([_P, ctypes.c_int, _P], ctypes.c_int),
+    "ve_nrc_stats": ([_P, _PTR(ctypes.c_float), _PTR(_U64), _PTR(_U64)], ctypes.c_int),
     "ve_server_create": ([_P, _PTR(ServerConfigC), _PTR(_P)], ctypes.c_int),
     "ve_server_submit": ([_P, _PTR(ViewC), _P, _P, _PTR(_U64)], ctypes.c_int),
     "ve_server_wait": ([_P, _U64, _U32, _PTR(RequestInfoC)], ctypes.c_int),
@@ -441,11 +464,14 @@ class Renderer:
         h = _P()
         _check(self._lib.ve_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
+        self._children: List[object] = []
         self.hash_log2 = hash_log2
         self.scene: Optional[int] = None
         self.camera: Optional[np.ndarray] = None
 
     def close(self) -> None:
+        for child in list(getattr(self, "_children", ())):
+            child.close()
         if getattr(self, "_h", None):
             self._lib.ve_ctx_destroy(self._h)
             self._h = None
@@ -602,6 +628,7 @@ class Server:
         h = _P()
         _check(self._lib.ve_server_create(renderer._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
+        renderer._children.append(self)
         self._buffers: Dict[int, tuple] = {}
 
     def submit(self, scene_id: int, camera: np.ndarray, fc: FrameConfig, want_vid: bool = True,
@@ -645,7 +672,112 @@ class Server:
         if getattr(self, "_h", None):
             rc = self._lib.ve_server_destroy(self._h)
             self._h = None
+            if self in self.renderer._children:
+                self.renderer._children.remove(self)
             _check(rc)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class LearnedCache:
+    """Learned radiance cache (hash-grid encoding + 4 x 64 ReLU MLP, bf16
+    tensor-core kernels) living on a Renderer's device.
+
+    Inputs are float32 rows [px, py, pz, 0, nx_oct, ny_oct, vx_oct, vy_oct]:
+    the voxel centre divided by the scene extent, the octahedral shading
+    normal and the octahedral direction toward the previous path vertex."""
+
+    LEVELS = 16
+    WIDTH = 64
+    LAYERS = 5
+
+    def __init__(self, renderer: "Renderer", log2_table: int = 19, base_resolution: int = 16,
+                 max_resolution: int = 2048, train_samples: int = 65536, learning_rate: float = 1e-2,
+                 beta1: float = 0.9, beta2: float = 0.99, eps: float = 1e-8, fallback_threshold: float = 0.1,
+                 seed: int = 1):
+        self._lib = load_library()
+        self.renderer = renderer
+        self.log2_table = log2_table
+        self.config = dict(log2_table=log2_table, base_resolution=base_resolution, max_resolution=max_resolution,
+                           train_samples=train_samples, learning_rate=learning_rate, beta1=beta1, beta2=beta2,
+                           eps=eps, fallback_threshold=fallback_threshold)
+        cfg = NrcConfigC(log2_table, base_resolution, max_resolution, train_samples, learning_rate, beta1, beta2,
+                         eps, fallback_threshold, 0, seed)
+        h = _P()
+        _check(self._lib.ve_nrc_create(renderer._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        renderer._children.append(self)
+
+    @staticmethod
+    def _rows(inputs) -> np.ndarray:
+        x = np.ascontiguousarray(np.asarray(inputs, np.float32))
+        assert x.ndim == 2 and x.shape[1] == 8, "inputs are (n, 8) float32 rows"
+        return x
+
+    def param_counts(self):
+        a, b = _U64(), _U64()
+        _check(self._lib.ve_nrc_param_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def get_params(self):
+        nw, nt = self.param_counts()
+        w = np.zeros(nw, np.float32)
+        t = np.zeros(nt, np.float32)
+        _check(self._lib.ve_nrc_get_params(self._h, w.ctypes.data, t.ctypes.data))
+        return w.reshape(self.LAYERS, self.WIDTH, self.WIDTH), t.reshape(self.LEVELS, -1, 2)
+
+    def set_params(self, weights: Optional[np.ndarray] = None, table: Optional[np.ndarray] = None) -> None:
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        t = None if table is None else np.ascontiguousarray(table, np.float32)
+        nw, nt = self.param_counts()
+        assert w is None or w.size == nw
+        assert t is None or t.size == nt
+        _check(self._lib.ve_nrc_set_params(self._h, _ptr(w), _ptr(t)))
+
+    def infer(self, inputs) -> np.ndarray:
+        x = self._rows(inputs)
+        out = np.zeros((x.shape[0], 3), np.float32)
+        _check(self._lib.ve_nrc_infer(self._h, x.ctypes.data, x.shape[0], out.ctypes.data))
+        return out
+
+    def gradients(self, inputs, targets):
+        x = self._rows(inputs)
+        t = np.ascontiguousarray(np.asarray(targets, np.float32).reshape(x.shape[0], 3))
+        nw, nt = self.param_counts()
+        gw = np.zeros(nw, np.float32)
+        gt = np.zeros(nt, np.float32)
+        loss = ctypes.c_float()
+        _check(self._lib.ve_nrc_gradients(self._h, x.ctypes.data, t.ctypes.data, x.shape[0], gw.ctypes.data,
+                                          gt.ctypes.data, ctypes.byref(loss)))
+        return gw.reshape(self.LAYERS, self.WIDTH, self.WIDTH), gt.reshape(self.LEVELS, -1, 2), loss.value
+
+    def train(self, inputs, targets) -> float:
+        x = self._rows(inputs)
+        t = np.ascontiguousarray(np.asarray(targets, np.float32).reshape(x.shape[0], 3))
+        loss = ctypes.c_float()
+        _check(self._lib.ve_nrc_train(self._h, x.ctypes.data, t.ctypes.data, x.shape[0], ctypes.byref(loss)))
+        return loss.value
+
+    def attach(self, scene_id: int) -> None:
+        _check(self._lib.ve_scene_set_nrc(self.renderer._h, scene_id, self._h))
+
+    def stats(self) -> Dict[str, float]:
+        """Loss and sample count of the last training step, steps taken."""
+        loss, n, steps = ctypes.c_float(), _U64(), _U64()
+        _check(self._lib.ve_nrc_stats(self._h, ctypes.byref(loss), ctypes.byref(n), ctypes.byref(steps)))
+        return {"loss": loss.value, "samples": n.value, "steps": steps.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            if getattr(self.renderer, "_h", None):  # the context destroys its caches itself
+                self._lib.ve_nrc_destroy(self._h)
+            self._h = None
+            if self in self.renderer._children:
+                self.renderer._children.remove(self)
 
     def __enter__(self):
         return self
@@ -656,5 +788,5 @@ class Server:
 
 __all__ = [
     "OctreeCPU", "Octree", "Renderer", "FrameConfig", "VeError", "camera_ubo", "look_at", "terrain_words",
-    "terrain_voxels", "terrain_materials", "load_library", "SUN_DIR", "Server",
+    "terrain_voxels", "terrain_materials", "load_library", "SUN_DIR", "Server", "LearnedCache",
 ]

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/ve.h"
+#include "nrc.cuh"
 #include "raycast.cuh"
 #include "ve_device.cuh"
 
@@ -75,7 +76,7 @@ struct DevView {
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
-enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_TOTAL = 64 };
+enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_TOTAL = 64 };
 enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
     ST_RAYS_BOUNCE,
@@ -87,9 +88,18 @@ enum : uint32_t {
     ST_STEPS,        // DDA iterations of k_primary + k_trace
     ST_FETCH_TRACE,  // node words read by k_trace alone
     ST_STEPS_TRACE,
+    ST_NRC_QUERIES,  // paths ended at their second vertex by the learned cache
+    ST_NRC_HASH,     // ... by the hashed per-voxel cache
+    ST_NRC_SAMPLES,  // training samples recorded
     ST_TOTAL = 16
 };
-enum : uint32_t { F_PENDING = 1u, F_TERM = 2u };
+enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u };
+// a cached voxel average ends a path (VE_FRAME_TERMINATE_HASH, and the
+// learned cache's fallback) only when at least this many deposits made it
+constexpr uint32_t kHashTermMinCount = 8;
+// validation samples a cell needs before its error decides for or against the
+// learned cache
+constexpr uint32_t kMinCellSamples = 4;
 
 struct FrameArgs {
     const DevView* views;
@@ -120,6 +130,18 @@ struct FrameArgs {
     uint32_t refill;       // idle lanes at which a trace warp takes new rays
     uint32_t view_offset;  // index of views[0] in the view table the paths refer to
     uint32_t* remaining;   // per view slot: paths not yet deposited (serving), or null
+    // learned radiance cache (views with VE_FRAME_LEARNED / _TERMINATE_HASH / _TRAIN)
+    nrc::QRec* nq;         // queries: paths ended at their second vertex by the network
+    float4* nq_out;        // network predictions per query
+    nrc::QRec* ns;         // training sample inputs
+    nrc::TRec* nt;         // training sample targets
+    uint32_t nq_cap, ns_cap;
+    uint32_t train_thresh;  // a path is a training path when hash(path, frame) < this
+    float fallback_thr;     // per-cell validation error above which the hash cache answers
+    const float4* val;      // per cell: {mean target, samples}, {mean prediction}
+    uint32_t val_mask;
+    uint32_t nrc_ready;     // cells without validation samples use the network
+    uint32_t* p_aux;        // per path: training sample slot
 };
 
 // ---------------------------------------------------------------------------
@@ -387,6 +409,72 @@ __global__ void k_accum_stats(const unsigned long long* frame, unsigned long lon
     if (threadIdx.x < ST_TOTAL) total[threadIdx.x] += frame[threadIdx.x];
 }
 
+struct Avg {
+    f3 rgb;
+    uint32_t count;
+    float var;
+};
+// lookupVoxelAvg (resolve.comp:109-148) over the FP32 cache
+__device__ __forceinline__ Avg lookup_avg(const DevScene& S, uint32_t vid) {
+    Avg r{mk(0.0f, 0.0f, 0.0f), 0u, 0.0f};
+    if (vid == 0u) return r;
+    const int s = cache_find(S.cache, S.cache_log2, S.probes, vid);
+    if (s < 0) return r;
+    const CacheEntry& e = S.cache[s];
+    r.count = e.count;
+    const float4 v = e.rgbw;
+    if (r.count == 0u || !(v.w > 0.0f)) return r;
+    const float inv = 1.0f / v.w;
+    r.rgb = mk(v.x * inv, v.y * inv, v.z * inv);
+    const float meanL = ((v.x + v.y) + v.z) * inv / 3.0f;
+    r.var = gmax(e.l2 * inv - meanL * meanL, 0.0f);
+    return r;
+}
+
+// Octahedral map of a unit vector to [-1, 1]^2 (Cigolle et al. 2014): the
+// learned cache's normal and direction inputs.
+__device__ __forceinline__ float2 oct_encode(f3 v) {
+    const float sum = (fabsf(v.x) + fabsf(v.y)) + fabsf(v.z);
+    float x = v.x / sum, y = v.y / sum;
+    if (v.z < 0.0f) {
+        const float ox = (1.0f - fabsf(y)) * (x >= 0.0f ? 1.0f : -1.0f);
+        const float oy = (1.0f - fabsf(x)) * (y >= 0.0f ? 1.0f : -1.0f);
+        x = ox;
+        y = oy;
+    }
+    return make_float2(x, y);
+}
+
+// packRgbL2 clamp (shade.comp:154-160): the deposited value is the clamped
+// direct plus the clamped indirect radiance; NaN counts as zero.
+__device__ __forceinline__ void deposit_value(f3 direct, f3 indirect, float& r, float& g, float& b, float& l2) {
+    const float dv[3] = {direct.x, direct.y, direct.z};
+    const float iv[3] = {indirect.x, indirect.y, indirect.z};
+    float outv[3];
+    for (int c = 0; c < 3; c++) {
+        float x = dv[c], y = iv[c];
+        if (!(x == x)) x = 0.0f;
+        if (!(y == y)) y = 0.0f;
+        outv[c] = gclamp(x, 0.0f, 1024.0f) + gclamp(y, 0.0f, 1024.0f);
+    }
+    r = outv[0];
+    g = outv[1];
+    b = outv[2];
+    const float Lf = ((r + g) + b) / 3.0f;
+    l2 = Lf * Lf;
+}
+
+// Training target of a finished training path: the radiance it gathered
+// from its second vertex on, divided by the throughput it arrived there with.
+__device__ __forceinline__ void write_target(nrc::TRec* t, f3 total, f3 s, f3 tp) {
+    const f3 d = mk((total.x - s.x) / tp.x, (total.y - s.y) / tp.y, (total.z - s.z) / tp.z);
+    const bool ok = tp.x > 0.0f && tp.y > 0.0f && tp.z > 0.0f && isfinite(d.x) && isfinite(d.y) && isfinite(d.z);
+    t->tr = d.x;
+    t->tg = d.y;
+    t->tb = d.z;
+    t->valid = ok ? 1u : 0u;
+}
+
 // shade.comp:543-575, 838-908 (bounce/shade loop) with the sun next-event
 // estimate in the place of the dormant emissive NEE, and the AccumPass deposit.
 __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
@@ -404,11 +492,17 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
         bool do_dep = false, app_live = false, app_ext = false, app_sh = false;
         float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
         uint32_t dvid = 0, dscene = 0, dview = 0;
+        // learned-cache hand-offs, appended after the divergent part
+        bool want_q = false, want_s = false, dep_train = false, hash_term = false;
+        nrc::QRec qrec{};
+        uint32_t qcell = 0;
+        f3 s_tp = mk(0.0f, 0.0f, 0.0f), s_sum = mk(0.0f, 0.0f, 0.0f), dep_total = mk(0.0f, 0.0f, 0.0f);
         if (valid) {
             uint4 meta = a.p_meta[p];
             const uint32_t vi = meta.z & 0xFFFFu;
             uint32_t b = (meta.z >> 16) & 0xFFu;
             const uint32_t flags = meta.z >> 24;
+            uint32_t nf = flags & F_TRAIN;
             const DevView& v = a.views[vi];
             f3 tp = ld3(a.p_tp[p]);
             f3 direct = ld3(a.p_direct[p]);
@@ -445,8 +539,63 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
                     const f3 hp = mk(float(hit.z & 0xFFFFu), float(hit.z >> 16), float(hit.w & 0xFFFFu));
                     const f3 sp = add(add(hp, mk(0.5f, 0.5f, 0.5f)), N);
                     const f3 sun = mk(v.sun[0], v.sun[1], v.sun[2]);
-                    uint32_t nf = 0;
-                    if (!emissive && b < 2u && dot(N, sun) > 0.0f) {
+                    // second path vertex: a training path is recorded here, other
+                    // paths may end with a cached radiance estimate
+                    bool ended = false;
+                    if (b == 1u && !emissive && (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN))) {
+                        const uint32_t hx = hit.z & 0xFFFFu, hy = hit.z >> 16, hz = hit.w & 0xFFFFu;
+                        const uint32_t cell = hash32((hx >> 3) | ((hy >> 3) << 10) | ((hz >> 3) << 20));
+                        if ((v.flags & VE_FRAME_TRAIN) && a.ns &&
+                            hash32(p ^ (v.frame_index * 0x9E3779B9u)) < a.train_thresh) {
+                            want_s = true;
+                            nf |= F_TRAIN;
+                            s_tp = tp;
+                            s_sum = add(direct, indirect);
+                        } else if (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH)) {
+                            bool mlp = false;
+                            if ((v.flags & VE_FRAME_LEARNED) && a.nq) {
+                                const float4* cs = a.val + 2u * (cell & a.val_mask);
+                                const float4 et = cs[0], ey = cs[1];
+                                if (et.w < float(kMinCellSamples)) {
+                                    mlp = a.nrc_ready != 0u;
+                                } else {
+                                    const float ex = (ey.x - et.x) * (ey.x - et.x) / (et.x * et.x + 0.01f);
+                                    const float eg = (ey.y - et.y) * (ey.y - et.y) / (et.y * et.y + 0.01f);
+                                    const float eb = (ey.z - et.z) * (ey.z - et.z) / (et.z * et.z + 0.01f);
+                                    mlp = ((ex + eg) + eb) / 3.0f <= a.fallback_thr;
+                                }
+                            }
+                            if (mlp) {
+                                want_q = true;
+                                ended = true;
+                                a.p_tp[p] = st3(tp);
+                                a.p_direct[p] = st3(direct);
+                                a.p_indirect[p] = st3(indirect);
+                            } else {
+                                const Avg r = lookup_avg(S, voxel_key(hx, hy, hz) + 1u);
+                                if (r.count >= kHashTermMinCount) {
+                                    indirect = add(indirect, mul(tp, r.rgb));
+                                    do_dep = true;
+                                    ended = true;
+                                    hash_term = true;
+                                }
+                            }
+                        }
+                        if (want_s || want_q) {
+                            const float inv_l = 1.0f / float(1u << S.depth);
+                            qrec.px = (hp.x + 0.5f) * inv_l;
+                            qrec.py = (hp.y + 0.5f) * inv_l;
+                            qrec.pz = (hp.z + 0.5f) * inv_l;
+                            qrec.path = p;
+                            const float2 on = oct_encode(N), ov = oct_encode(mk(-dir.x, -dir.y, -dir.z));
+                            qrec.nx = on.x;
+                            qrec.ny = on.y;
+                            qrec.vx = ov.x;
+                            qrec.vy = ov.y;
+                            qcell = cell;
+                        }
+                    }
+                    if (!ended && !emissive && b < 2u && dot(N, sun) > 0.0f) {
                         const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
                         f3 c = muls(brdf, v.sun_intensity);
                         c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
@@ -456,7 +605,9 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
                     }
                     bool term = false;
                     uint32_t rng = meta.y;
-                    if (b + 1u >= v.bounces + 1u) {
+                    if (ended) {
+                        // ended by a cache: deposited now (hash) or after inference (network)
+                    } else if (b + 1u >= v.bounces + 1u) {
                         term = true;
                     } else {
                         const bool use_ggx = metallic * (1.0f - roughness) > 0.5f;
@@ -510,19 +661,11 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
                 }
             }
             if (do_dep) {
-                // packRgbL2 clamp (shade.comp:154-160), direct + indirect
-                float dv[3] = {direct.x, direct.y, direct.z};
-                const float iv[3] = {indirect.x, indirect.y, indirect.z};
-                float outv[3];
-                for (int c = 0; c < 3; c++) {
-                    float x = dv[c], y = iv[c];
-                    if (!(x == x)) x = 0.0f;
-                    if (!(y == y)) y = 0.0f;
-                    outv[c] = gclamp(x, 0.0f, 1024.0f) + gclamp(y, 0.0f, 1024.0f);
+                deposit_value(direct, indirect, dr, dg, db, dl2);
+                if ((flags | nf) & F_TRAIN) {
+                    dep_train = true;
+                    dep_total = add(direct, indirect);
                 }
-                dr = outv[0]; dg = outv[1]; db = outv[2];
-                const float Lf = ((dr + dg) + db) / 3.0f;
-                dl2 = Lf * Lf;
                 dvid = meta.x;
                 dscene = v.scene;
                 dview = vi;
@@ -541,6 +684,36 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
         if (app_sh) a.rayq[ss] = p | 0x80000000u;
         n_ext += app_ext ? 1u : 0u;
         n_sh += app_sh ? 1u : 0u;
+        if (a.nq || a.ns) {
+            // learned cache: queries (capacity = paths, never full) and
+            // training samples (a path past the capacity stays plain)
+            const uint32_t kq = warp_append(want_q, &a.counters[CNT_NRC_Q]);
+            if (want_q && kq < a.nq_cap) a.nq[kq] = qrec;
+            const uint32_t ks = warp_append(want_s, &a.counters[CNT_NRC_S]);
+            uint32_t slot = 0xFFFFFFFFu;
+            if (want_s && ks < a.ns_cap) {
+                slot = ks;
+                a.ns[ks] = qrec;
+                nrc::TRec t{};
+                t.t0 = s_tp.x; t.t1 = s_tp.y; t.t2 = s_tp.z;
+                t.s0 = s_sum.x; t.s1 = s_sum.y; t.s2 = s_sum.z;
+                t.cell = qcell;
+                a.nt[ks] = t;
+            }
+            if (want_s) a.p_aux[p] = slot;
+            if (dep_train) {
+                const uint32_t k = want_s ? slot : a.p_aux[p];
+                if (k < a.ns_cap) {
+                    nrc::TRec* t = a.nt + k;
+                    const f3 tp0 = want_s ? s_tp : mk(t->t0, t->t1, t->t2);
+                    const f3 s0 = want_s ? s_sum : mk(t->s0, t->s1, t->s2);
+                    write_target(t, dep_total, s0, tp0);
+                }
+            }
+            warp_add_stat(&a.stats[ST_NRC_QUERIES], want_q ? 1u : 0u);
+            warp_add_stat(&a.stats[ST_NRC_SAMPLES], (want_s && slot != 0xFFFFFFFFu) ? 1u : 0u);
+        }
+        warp_add_stat(&a.stats[ST_NRC_HASH], hash_term ? 1u : 0u);
         warp_deposit(do_dep, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
         if (a.remaining) {  // serving: count finished paths per view slot
             const unsigned dm = __ballot_sync(0xffffffffu, do_dep);
@@ -554,26 +727,37 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
 }
 
-struct Avg {
-    f3 rgb;
-    uint32_t count;
-    float var;
-};
-// lookupVoxelAvg (resolve.comp:109-148) over the FP32 cache
-__device__ __forceinline__ Avg lookup_avg(const DevScene& S, uint32_t vid) {
-    Avg r{mk(0.0f, 0.0f, 0.0f), 0u, 0.0f};
-    if (vid == 0u) return r;
-    const int s = cache_find(S.cache, S.cache_log2, S.probes, vid);
-    if (s < 0) return r;
-    const CacheEntry& e = S.cache[s];
-    r.count = e.count;
-    const float4 v = e.rgbw;
-    if (r.count == 0u || !(v.w > 0.0f)) return r;
-    const float inv = 1.0f / v.w;
-    r.rgb = mk(v.x * inv, v.y * inv, v.z * inv);
-    const float meanL = ((v.x + v.y) + v.z) * inv / 3.0f;
-    r.var = gmax(e.l2 * inv - meanL * meanL, 0.0f);
-    return r;
+// Paths the learned cache ended at their second vertex: add throughput x the
+// network's prediction (negative channels read as zero) to the indirect
+// radiance, then deposit like any finished path.
+__global__ void __launch_bounds__(256) k_nrc_apply(FrameArgs a) {
+    __shared__ DepSlot dep[256];
+    const uint32_t n = min(a.counters[CNT_NRC_Q], a.nq_cap);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
+        uint32_t dvid = 0, dscene = 0;
+        if (valid) {
+            const uint32_t p = a.nq[i].path;
+            const uint4 meta = a.p_meta[p];
+            const DevView& v = a.views[meta.z & 0xFFFFu];
+            const float4 y = a.nq_out[i];
+            const f3 pred = mk(y.x > 0.0f ? y.x : 0.0f, y.y > 0.0f ? y.y : 0.0f, y.z > 0.0f ? y.z : 0.0f);
+            const f3 tp = ld3(a.p_tp[p]);
+            const f3 direct = ld3(a.p_direct[p]);
+            const f3 indirect = add(ld3(a.p_indirect[p]), mul(tp, pred));
+            deposit_value(direct, indirect, dr, dg, db, dl2);
+            dvid = meta.x;
+            dscene = v.scene;
+            if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
+                a.path_rgb[3ull * p + 0] = dr;
+                a.path_rgb[3ull * p + 1] = dg;
+                a.path_rgb[3ull * p + 2] = db;
+            }
+        }
+        warp_deposit(valid, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
+    }
 }
 
 __device__ __forceinline__ float aces(float x) {  // final.frag:11-18
@@ -831,6 +1015,7 @@ struct SceneSlot {
     uint32_t depth = 0;
     CacheEntry* cache = nullptr;
     bool live = false;
+    ve_nrc* nrc = nullptr;  // learned radiance cache attached to the scene
 };
 
 template <typename T>
@@ -877,6 +1062,7 @@ struct ve_ctx {
     ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
     ve::DevBuf<uint4> p_hit, p_meta;
     ve::DevBuf<uint8_t> p_vis;
+    ve::DevBuf<uint32_t> p_aux;  // training sample slot per path (learned-cache training frames)
     ve::DevBuf<uint32_t> live0, live1, rayq;
     ve::DevBuf<uint32_t> counters;
     ve::DevBuf<unsigned long long> stats;
@@ -886,6 +1072,7 @@ struct ve_ctx {
     uint64_t tot_frames = 0, tot_h2d = 0, tot_d2h = 0;
     uint32_t tot_launches = 0, tot_trace_launches = 0;
     float tot_ms[6] = {0, 0, 0, 0, 0, 0};
+    float tot_ms_learned = 0;
     uint64_t last_h2d = 0, last_d2h = 0;
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
@@ -900,6 +1087,7 @@ struct ve_ctx {
         cudaEvent_t ev[kEvents] = {};
         int n = 0;            // events recorded
         uint32_t passes = 0;  // shade passes
+        bool learned = false; // a learned-cache segment precedes resolve
         bool pending = false;
     } timing[kTimingSlots];
     int timing_next = 0;
@@ -918,8 +1106,11 @@ struct ve_ctx {
     std::vector<GraphEntry> graphs;
     uint64_t graph_clock = 0;
     uint64_t graph_captures = 0, graph_replays = 0;
+    std::vector<ve_nrc*> nrcs;  // learned caches created on this context
     uint32_t last_launches = 0, last_trace_launches = 0;
 };
+
+#include "nrc_host.cuh"
 
 namespace ve {
 
@@ -1036,13 +1227,19 @@ static void collect_timing(ve_ctx* c, ve_ctx::TimingSlot& ts, ve_frame_stats* ou
         cudaEventElapsedTime(&t, ts.ev[e0 + 1], ts.ev[e0 + 2]); f.ms_trace += t;
     }
     cudaEventElapsedTime(&t, ts.ev[ts.n - 2], ts.ev[ts.n - 1]); f.ms_resolve = t;
+    if (ts.learned) {
+        cudaEventElapsedTime(&t, ts.ev[ts.n - 3], ts.ev[ts.n - 2]);
+        f.ms_learned = t;
+    }
     cudaEventElapsedTime(&t, ts.ev[0], ts.ev[ts.n - 1]); f.ms_total = t;
     c->tot_ms[0] += f.ms_total; c->tot_ms[1] += f.ms_primary; c->tot_ms[2] += f.ms_trace;
     c->tot_ms[3] += f.ms_shade; c->tot_ms[4] += f.ms_resolve; c->tot_ms[5] += f.ms_decay;
     ts.pending = false;
+    c->tot_ms_learned += f.ms_learned;
     if (out) {
         out->ms_total = f.ms_total; out->ms_primary = f.ms_primary; out->ms_trace = f.ms_trace;
         out->ms_shade = f.ms_shade; out->ms_resolve = f.ms_resolve; out->ms_decay = f.ms_decay;
+        out->ms_learned = f.ms_learned;
     }
 }
 
@@ -1055,6 +1252,7 @@ static void collect_all_timing(ve_ctx* c) {
             if (k == c->last_timing_slot) {
                 c->last.ms_total = f.ms_total; c->last.ms_primary = f.ms_primary; c->last.ms_trace = f.ms_trace;
                 c->last.ms_shade = f.ms_shade; c->last.ms_resolve = f.ms_resolve; c->last.ms_decay = f.ms_decay;
+                c->last.ms_learned = f.ms_learned;
             }
         }
     }
@@ -1097,8 +1295,27 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         flags |= f.flags;
     }
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
+    // learned radiance cache: one per batch, attached to the views' scenes
+    ve_nrc* nrc = nullptr;
+    for (uint32_t i = 0; i < nv; i++) {
+        if (!(views[i].frame.flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN))) continue;
+        ve_nrc* m = c->scenes[views[i].scene_id].nrc;
+        if (!m) return fail(VE_ERR_STATE, "render: VE_FRAME_LEARNED / VE_FRAME_TRAIN on a scene without a learned cache");
+        if (nrc && m != nrc) return fail(VE_ERR_INVALID, "render: at most one learned cache per batch");
+        nrc = m;
+    }
     int rc = ensure_frame(c, pixels, paths, nv);
     if (rc) return rc;
+    if (nrc) {
+        bool moved = false;
+        if ((rc = nrc::prepare_frame(nrc, paths, &moved))) return rc;
+        if (flags & VE_FRAME_TRAIN) {
+            const void* old = c->p_aux.p;
+            if ((rc = c->p_aux.ensure(paths))) return rc;
+            moved |= old != c->p_aux.p;
+        }
+        if (moved) c->gen++;
+    }
     if (flags & VE_FRAME_PATH_RGB) {
         const void* old = c->path_rgb.p;
         if ((rc = c->path_rgb.ensure(paths * 3))) return rc;
@@ -1180,6 +1397,25 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.refill = c->launch.refill_threshold;
     a.view_offset = 0;
     a.remaining = nullptr;
+    const bool learned = nrc && (flags & VE_FRAME_LEARNED);
+    const bool train = nrc && (flags & VE_FRAME_TRAIN);
+    if (nrc) {
+        a.nq = learned ? nrc->fq.p : nullptr;
+        a.nq_out = nrc->fout.p;
+        a.nq_cap = uint32_t(paths);
+        a.ns = train ? nrc->fs.p : nullptr;
+        a.nt = nrc->ftr.p;
+        a.ns_cap = nrc->cfg.train_samples;
+        // select ~1.25x the sample budget among the frame's paths (not every
+        // path reaches a second vertex); the overflow stays plain
+        const double frac = std::min(1.0, 1.25 * double(nrc->cfg.train_samples) / double(std::max<uint64_t>(paths, 1)));
+        a.train_thresh = uint32_t(std::min(4294967295.0, frac * 4294967296.0));
+        a.fallback_thr = nrc->cfg.fallback_threshold;
+        a.val = nrc->val.p;
+        a.val_mask = (1u << nrc::kValCellsLog2) - 1u;
+        a.nrc_ready = nrc->trained_steps >= nrc::kReadySteps ? 1u : 0u;
+        a.p_aux = train ? c->p_aux.p : nullptr;
+    }
     // the frame's kernel sequence (no host synchronisation inside)
     auto enqueue = [&]() {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
@@ -1212,6 +1448,21 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
             rec();
         }
+        if (learned || train) {
+            if (learned) {
+                nrc::launch_infer(nrc, st, nrc->fq.p, c->counters.p + CNT_NRC_Q, a.nq_cap, nrc->fout.p);
+                k_nrc_apply<<<c->grid_shade, 256, 0, st>>>(a);
+                launches += 2;
+            }
+            if (train) {
+                nrc::enqueue_zero_grads(nrc, st);
+                nrc::launch_train(nrc, st, nrc->fs.p, nrc->ftr.p, c->counters.p + CNT_NRC_S, a.ns_cap,
+                                  1.0f / (3.0f * float(a.ns_cap)));
+                nrc::launch_adam(nrc, st);
+                launches += 4;
+            }
+            rec();
+        }
         k_resolve<<<tiles, 256, 0, st>>>(a);
         launches++;
         rec();
@@ -1222,9 +1473,12 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (!use_graph) {
         enqueue();
     } else {
-        std::vector<uint64_t> key = {c->gen, nv, tiles, max_b, flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB),
+        std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
+                                     flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
+                                              VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN),
                                      paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
-                                     uint64_t(c->launch.refill_threshold)};
+                                     uint64_t(c->launch.refill_threshold), uint64_t(uintptr_t(nrc)),
+                                     uint64_t(a.nrc_ready)};
         for (auto& d : decays) {
             uint32_t bits;
             std::memcpy(&bits, &d.second, 4);
@@ -1273,6 +1527,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (timing) {
         ts->n = ne;
         ts->passes = max_b + 2u;
+        ts->learned = learned || train;
         ts->pending = true;
         c->last_timing_slot = int(ts - c->timing);
     } else {
@@ -1308,6 +1563,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     c->tot_d2h += d2h;
     c->tot_launches += launches;
     c->tot_trace_launches += trace_launches;
+    if (train) nrc->trained_steps++;
     return VE_OK;
 }
 
@@ -1417,6 +1673,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     if (!c) return VE_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    while (!c->nrcs.empty()) ve_nrc_destroy(c->nrcs.back());
     for (auto& s : c->scenes) {
         if (s.alloc) cudaFree(s.alloc);
         if (s.cache) cudaFree(s.cache);
@@ -1425,6 +1682,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
     c->p_indirect.release(); c->p_pend.release(); c->p_hit.release(); c->p_meta.release(); c->p_vis.release();
     c->live0.release(); c->live1.release(); c->rayq.release(); c->counters.release(); c->stats.release();
+    c->p_aux.release();
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
     c->out_mapped.release(); c->path_rgb.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
@@ -1699,6 +1957,9 @@ static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
     r.dda_steps = h[ST_STEPS];
     r.fetch_nodes_trace = h[ST_FETCH_TRACE];
     r.dda_steps_trace = h[ST_STEPS_TRACE];
+    r.nrc_queries = h[ST_NRC_QUERIES];
+    r.nrc_hash_terminated = h[ST_NRC_HASH];
+    r.nrc_samples = h[ST_NRC_SAMPLES];
 }
 
 int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
@@ -1714,6 +1975,7 @@ int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
     r.d2h_bytes = c->tot_d2h;
     r.ms_total = c->tot_ms[0]; r.ms_primary = c->tot_ms[1]; r.ms_trace = c->tot_ms[2];
     r.ms_shade = c->tot_ms[3]; r.ms_resolve = c->tot_ms[4]; r.ms_decay = c->tot_ms[5];
+    r.ms_learned = c->tot_ms_learned;
     r.kernel_launches = c->tot_launches;
     r.trace_launches = c->tot_trace_launches;
     r.cache_capacity = 1ull << c->cfg.hash_log2;
@@ -1729,6 +1991,7 @@ int ve_reset_total_stats(ve_ctx* c) {
     c->tot_frames = c->tot_h2d = c->tot_d2h = 0;
     c->tot_launches = c->tot_trace_launches = 0;
     for (float& m : c->tot_ms) m = 0.0f;
+    c->tot_ms_learned = 0.0f;
     return VE_OK;
 }
 
