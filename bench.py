@@ -464,6 +464,112 @@ def run_serving(args, rank, world):
     return 0
 
 
+def run_learned(args, rank, world):
+    """rMSE at equal time against a 64-spp plain render (16 frames x 4 spp,
+    fresh cache, decay 1) on the depth-10 scene at 1080p, fixed camera:
+    the plain method, the hashed per-voxel cache ending paths at their second
+    vertex, and the learned cache (trained online on 2^16 samples per frame
+    over `--train-frames` plain frames, then ending paths at their second
+    vertex, falling back to the hashed cache per cell).  Each method renders
+    4-spp frames from a fresh radiance cache until its device time reaches
+    that of the plain method's `--eq-frames` frames."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=600.0, device=local)
+    torch.cuda.set_device(local)
+    W = wl.LARGE
+    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
+    r = ve.Renderer(device=local, hash_log2=W.hash_log2)
+    r.set_materials(ve.terrain_materials(W.seed))
+    sid = r.upload_scene(words, W.depth)
+    eye, d = wl.orbit_camera(0, W.frames, W.seed)
+    cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+    stream = torch.cuda.ExternalStream(r.stream, device=local)
+
+    def fc(frame, spp, flags=0):
+        return ve.FrameConfig(width=W.width, height=W.height, spp=spp, bounces=W.bounces, frame_index=frame,
+                              primary_controlchecks=W.primary_controlchecks,
+                              bounce_controlchecks=W.bounce_controlchecks, decay=1.0, flags=flags)
+
+    def timed(frame, spp, flags, outputs=()):
+        """One frame; device time of its kernels (CUDA events inside the
+        library), host copies of the outputs excluded."""
+        out = r.render(sid, cam, fc(frame, spp, flags | ve.FRAME_TIMING), outputs=outputs)
+        return out, r.stats()["ms_total"]
+
+    # reference: 64 spp through the per-voxel cache
+    r.cache_reset(sid)
+    for k in range(15):
+        r.render(sid, cam, fc(90000 + k, 4), outputs=())
+    ref = r.render(sid, cam, fc(90015, 4), outputs=("voxel_id", "rgb"))
+    mask = ref["voxel_id"] != 0
+    refrgb = ref["rgb"]
+
+    def rmse(img):
+        e = (img - refrgb) ** 2 / (refrgb ** 2 + 0.01)
+        return float(e[mask].mean())
+
+    # online training of the learned cache on plain frames
+    m = ve.LearnedCache(r, log2_table=19, train_samples=65536, seed=1)
+    m.attach(sid)
+    train_ms = 0.0
+    losses = []
+    for f in range(args.train_frames):
+        _, ms = timed(1000 + f, W.spp, ve.FRAME_TRAIN)
+        train_ms += ms
+        losses.append(m.stats()["loss"])
+
+    def run_method(flags, budget_ms, max_frames):
+        r.cache_reset(sid)
+        t = 0.0
+        n = 0
+        img = None
+        stats = {"nrc_queries": 0, "nrc_hash_terminated": 0, "paths": 0}
+        while n < max_frames:
+            out, ms = timed(20000 + n, W.spp, flags, outputs=("rgb",))
+            if budget_ms is not None and n > 0 and t + ms > budget_ms * 1.0001:
+                break
+            t += ms
+            n += 1
+            img = out["rgb"]  # the image after n frames (host copy outside the timed kernels)
+            st = r.stats()
+            for k in stats:
+                stats[k] += st[k]
+            if budget_ms is None and n >= max_frames:
+                break
+        return {"rmse": rmse(img), "frames": n, "ms": t, "spp": n * W.spp, **stats}
+
+    plain = run_method(0, None, args.eq_frames)
+    budget = plain["ms"]
+    stream.synchronize()
+    hashed = run_method(ve.FRAME_TERMINATE_HASH, budget, 64)
+    learned = run_method(ve.FRAME_LEARNED | ve.FRAME_TRAIN, budget, 64)
+    line = {"metric": "rMSE at equal time vs 64-spp plain render (learned cache)", "value": learned["rmse"],
+            "unit": "relative MSE", "n_gpus": world, "steps": learned["frames"], "warmup": args.train_frames,
+            "ms_per_step": learned["ms"] / max(learned["frames"], 1), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 network / f32 tracer",
+            "data": "synthetic (seeded terrain, fixed orbit camera)",
+            "config": {"workload": "learned: depth-10 terrain 1920x1080, 4 spp x 3 bounces per frame, "
+                                   "64-spp reference (16 x 4 spp through the per-voxel cache), equal device time",
+                       "network": "hash grid 16 x 2 fp16 (2^19/level) + oct normal + oct view -> 4 x 64 ReLU -> 3",
+                       "train_frames": args.train_frames, "train_samples_per_frame": 65536,
+                       "budget_ms": budget},
+            "plain": plain, "hash_terminated": hashed, "learned": learned,
+            "train_ms_per_frame": train_ms / max(args.train_frames, 1),
+            "train_loss_first_last": [losses[0] if losses else None, losses[-1] if losses else None]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    m.close()
+    r.close()
+    vd.shutdown(dist)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -472,7 +578,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching", "serving"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned"], default="large")
+    ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
+    ap.add_argument("--eq-frames", type=int, default=4, help="learned: plain frames setting the time budget")
     ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
     ap.add_argument("--capacity-requests", type=int, default=400, help="serving: closed-loop capacity sample")
     ap.add_argument("--serial-requests", type=int, default=400, help="serving: serial plain comparison sample")
@@ -494,6 +602,8 @@ def main():
         return run_batching(args, rank, world)
     if args.workload == "serving":
         return run_serving(args, rank, world)
+    if args.workload == "learned":
+        return run_learned(args, rank, world)
 
     import torch
 
