@@ -529,7 +529,8 @@ def run_learned(args, rank, world):
         t = 0.0
         n = 0
         img = None
-        stats = {"nrc_queries": 0, "nrc_hash_terminated": 0, "paths": 0}
+        stats = {"nrc_queries": 0, "nrc_hash_terminated": 0, "paths": 0, "ms_learned": 0.0, "ms_trace": 0.0,
+                 "ms_shade": 0.0, "ms_primary": 0.0, "rays_bounce": 0, "rays_shadow": 0}
         while n < max_frames:
             out, ms = timed(20000 + n, W.spp, flags, outputs=("rgb",))
             if budget_ms is not None and n > 0 and t + ms > budget_ms * 1.0001:
@@ -548,6 +549,7 @@ def run_learned(args, rank, world):
     budget = plain["ms"]
     stream.synchronize()
     hashed = run_method(ve.FRAME_TERMINATE_HASH, budget, 64)
+    learned_frozen = run_method(ve.FRAME_LEARNED, budget, 64)
     learned = run_method(ve.FRAME_LEARNED | ve.FRAME_TRAIN, budget, 64)
     line = {"metric": "rMSE at equal time vs 64-spp plain render (learned cache)", "value": learned["rmse"],
             "unit": "relative MSE", "n_gpus": world, "steps": learned["frames"], "warmup": args.train_frames,
@@ -560,6 +562,7 @@ def run_learned(args, rank, world):
                        "train_frames": args.train_frames, "train_samples_per_frame": 65536,
                        "budget_ms": budget},
             "plain": plain, "hash_terminated": hashed, "learned": learned,
+            "learned_inference_only": learned_frozen,
             "train_ms_per_frame": train_ms / max(args.train_frames, 1),
             "train_loss_first_last": [losses[0] if losses else None, losses[-1] if losses else None]}
     if rank == 0:

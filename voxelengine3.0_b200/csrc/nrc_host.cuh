@@ -132,7 +132,8 @@ static int prepare_frame(ve_nrc* m, uint64_t paths, bool* moved) {
 
 static int check_status(ve_nrc* m) {
     uint32_t s = 0;
-    VE_CUDA(cudaMemcpy(&s, m->status.p, 4, cudaMemcpyDeviceToHost));
+    VE_CUDA(cudaMemcpyAsync(&s, m->status.p, 4, cudaMemcpyDeviceToHost, m->c->stream));
+    VE_CUDA(cudaStreamSynchronize(m->c->stream));
     if (s) return fail(VE_ERR_CUDA, "learned cache: a tensor-core wait timed out");
     return VE_OK;
 }
@@ -267,8 +268,12 @@ int ve_nrc_get_params(ve_nrc* m, float* weights, float* table) {
     if (!m) return fail(VE_ERR_INVALID, "nrc_get_params: null handle");
     cudaSetDevice(m->c->device);
     VE_CUDA(cudaStreamSynchronize(m->c->stream));
-    if (weights) VE_CUDA(cudaMemcpy(weights, m->w.p, sizeof(float) * nrc::kWParams, cudaMemcpyDeviceToHost));
-    if (table) VE_CUDA(cudaMemcpy(table, m->tp.p, sizeof(float2) * m->n_table, cudaMemcpyDeviceToHost));
+    // the context's stream is non-blocking: every copy goes through it
+    if (weights)
+        VE_CUDA(cudaMemcpyAsync(weights, m->w.p, sizeof(float) * nrc::kWParams, cudaMemcpyDeviceToHost, m->c->stream));
+    if (table)
+        VE_CUDA(cudaMemcpyAsync(table, m->tp.p, sizeof(float2) * m->n_table, cudaMemcpyDeviceToHost, m->c->stream));
+    VE_CUDA(cudaStreamSynchronize(m->c->stream));
     return VE_OK;
 }
 
@@ -280,12 +285,15 @@ int ve_nrc_set_params(ve_nrc* m, const float* weights, const float* table) {
     cudaStream_t st = m->c->stream;
     VE_CUDA(cudaStreamSynchronize(st));
     if (weights) {
-        VE_CUDA(cudaMemcpy(m->w.p, weights, sizeof(float) * kWParams, cudaMemcpyHostToDevice));
+        // on the context's (non-blocking) stream, so the kernels below see the
+        // whole copy: a legacy-stream copy from pageable memory may return
+        // before its DMA has landed
+        VE_CUDA(cudaMemcpyAsync(m->w.p, weights, sizeof(float) * kWParams, cudaMemcpyHostToDevice, st));
         VE_CUDA(cudaMemsetAsync(m->wimg.p, 0, kWImage, st));
         k_nrc_weights_image<<<(kWParams + 255) / 256, 256, 0, st>>>(m->w.p, m->wimg.p);
     }
     if (table) {
-        VE_CUDA(cudaMemcpy(m->tp.p, table, sizeof(float2) * m->n_table, cudaMemcpyHostToDevice));
+        VE_CUDA(cudaMemcpyAsync(m->tp.p, table, sizeof(float2) * m->n_table, cudaMemcpyHostToDevice, st));
         k_nrc_table_half<<<m->c->num_sms * 8, 256, 0, st>>>(m->tp.p, m->th.p, m->n_table);
     }
     // a new parameter set restarts the optimiser
@@ -374,8 +382,9 @@ int ve_nrc_stats(ve_nrc* m, float* loss, uint64_t* samples, uint64_t* steps) {
     VE_CUDA(cudaStreamSynchronize(m->c->stream));
     float l = 0.0f;
     uint32_t n = 0;
-    VE_CUDA(cudaMemcpy(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost));
-    VE_CUDA(cudaMemcpy(&n, m->nvalid.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    VE_CUDA(cudaMemcpyAsync(&l, m->loss.p, sizeof(float), cudaMemcpyDeviceToHost, m->c->stream));
+    VE_CUDA(cudaMemcpyAsync(&n, m->nvalid.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, m->c->stream));
+    VE_CUDA(cudaStreamSynchronize(m->c->stream));
     int rc;
     if ((rc = nrc::check_status(m))) return rc;
     if (loss) *loss = n ? l / (3.0f * float(n)) : 0.0f;

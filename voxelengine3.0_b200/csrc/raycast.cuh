@@ -13,6 +13,14 @@
 //   new position lies in the previous terminal (empty) cell the previous
 //   result is reused outright.  The node words read per ray are then the
 //   distinct nodes along its walk instead of (depth+1) per step.
+//
+//   A descent that restarts above level T0 reads one word of the scene's
+//   top table instead of levels 0..T0-1: per cell of the level-(T0-1)
+//   grid, the child-block offset reached at level T0, or the terminal level
+//   when the cell is empty higher up (built from the node words by
+//   k_build_top, bit-identical to walking them).  This shortens the longest
+//   descents of a warp — those that cross a coarse cell boundary — which set
+//   its lock-step cost.  Fetch-counting runs (COUNT) walk every level.
 #pragma once
 #include "ve_device.cuh"
 
@@ -72,9 +80,17 @@ __device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlche
     return false;
 }
 
+// Top-table entry of the cell containing (x, y, z): (offset << 1) | 1 when
+// levels 0..T0-1 are internal (offset = child block of the level-T0 node),
+// else (terminal level << 1).
+__device__ __forceinline__ uint32_t top_index(uint32_t x, uint32_t y, uint32_t z, uint32_t D, uint32_t T0) {
+    const uint32_t sh = D - T0 + 1u, b = T0 - 1u;
+    return ((((x >> sh) << b) | (y >> sh)) << b) | (z >> sh);
+}
+
 template <bool COUNT>
 __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
-                                         Hit& h, RayCount& rc) {
+                                         const uint32_t* __restrict__ top, uint32_t T0, Hit& h, RayCount& rc) {
     const uint32_t L = 1u << D;
     const float Lf = float(L);
     if (!in_bounds(s.r, Lf)) {
@@ -107,7 +123,18 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
         s.lux = ux; s.luy = uy; s.luz = uz;
         bool found = false;
         uint32_t off = 0;
-        for (k = start; k < D; k++) {
+        k = start;
+        if (!COUNT && start < T0) {
+            const uint32_t ent = __ldg(top + top_index(ux, uy, uz, D, T0));
+            if (ent & 1u) {
+                s.base[T0] = ent >> 1;
+                k = T0;
+            } else {
+                k = ent >> 1;
+                found = true;
+            }
+        }
+        for (; !found && k < D; k++) {
             off = s.base[k] + locate(ux, uy, uz, L >> k);
             const uint32_t raw = fetch_node(nodes, n_words, off);
             if (COUNT) rc.fetch++;
@@ -148,12 +175,13 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
 }
 
 template <bool COUNT>
-__device__ __forceinline__ Hit raycast(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, f3 o, f3 d,
+__device__ __forceinline__ Hit raycast(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                       const uint32_t* __restrict__ top, uint32_t T0, f3 o, f3 d,
                                        uint32_t controlchecks, RayCount& rc) {
     Dda s;
     Hit h;
     if (dda_init(s, o, d, controlchecks, D, h)) return h;
-    while (!dda_step<COUNT>(s, nodes, n_words, D, h, rc)) {
+    while (!dda_step<COUNT>(s, nodes, n_words, D, top, T0, h, rc)) {
     }
     return h;
 }

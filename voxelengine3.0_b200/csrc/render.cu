@@ -53,7 +53,8 @@ struct DevScene {
     uint32_t depth;
     uint32_t cache_log2;
     uint32_t probes;
-    uint32_t pad;
+    uint32_t top_level;   // T0: levels 0..T0-1 resolved by the top table (0: none)
+    const uint32_t* top;  // top table, (2^(T0-1))^3 words
 };
 
 struct DevMaterial {
@@ -277,67 +278,6 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
     }
 }
 
-// RayPass primary (generate_primary.comp:38-85) + path seeding (emit.comp:39-101)
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
-    const uint32_t tile = blockIdx.x;
-    const uint32_t vi = find_view(a.views, a.n_views, tile);
-    const DevView& v = a.views[vi];
-    uint32_t px, py;
-    tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
-    const bool inside = px < v.W && py < v.H;
-    const DevScene S = a.scenes[v.scene];
-    Hit h;
-    h.status = kEscaped;
-    h.checks = 0;
-    f3 dir = mk(0.0f, 0.0f, 0.0f);
-    RayCount rc;
-    uint32_t vid = 0;
-    if (inside) {
-        const float ndx = (float(px) + 0.5f) / float(v.W) * 2.0f - 1.0f;
-        const float ndy = (float(py) + 0.5f) / float(v.H) * 2.0f - 1.0f;
-        const f3 plane = mk(v.cam[4], v.cam[5], v.cam[6]);
-        const f3 right = mk(v.cam[8], v.cam[9], v.cam[10]);
-        const f3 up = mk(v.cam[12], v.cam[13], v.cam[14]);
-        dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
-        h = raycast<COUNT>(S.nodes, S.n_words, S.depth, mk(v.cam[0], v.cam[1], v.cam[2]), dir, v.cc_primary, rc);
-        if (h.status == kHit) vid = voxel_key(h.x, h.y, h.z) + 1u;
-        const uint32_t pix = py * v.W + px;
-        a.gbuf[v.pix_base + pix] = make_uint4(h.checks, h.status == kHit ? h.material : 0u,
-                                              h.status == kHit ? h.id : 0u, vid);
-    }
-    const bool spawn = inside && vid != 0u;
-    const uint32_t q = warp_append(spawn, &a.counters[CNT_LIVE + 0], v.spp);
-    if (spawn) {
-        const uint32_t pix = py * v.W + px;
-        for (uint32_t s = 0; s < v.spp; s++) {
-            const unsigned long long p = v.path_base + (unsigned long long)pix * v.spp + s;
-            const uint32_t list_idx = pix * v.spp + s;
-            // emit.comp:171-174
-            const uint32_t sample_idx = v.frame_index + pix * 2654435761u + list_idx * 1442695040u;
-            const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
-            a.p_ray_d[p] = st3(dir);
-            a.p_tp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.p_hit[p] = make_uint4(kHit, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
-            a.p_meta[p] = make_uint4(vid, rng, vi + a.view_offset, pix);
-            a.live[0][q + s] = uint32_t(p);
-        }
-    }
-    warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside ? 1u : 0u);
-    warp_add_stat(&a.stats[ST_PATHS], spawn ? v.spp : 0u);
-    if (a.remaining) {  // the whole block belongs to one view
-        uint32_t sp = spawn ? v.spp : 0u;
-        for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
-        if (lane_id() == 0 && sp) atomicAdd(&a.remaining[vi + a.view_offset], sp);
-    }
-    if (COUNT) {
-        warp_add_stat(&a.stats[ST_FETCH], rc.fetch);
-        warp_add_stat(&a.stats[ST_STEPS], rc.steps);
-    }
-}
-
 // trace.comp:25-70 for extension rays; shadow rays test escape toward the sun.
 //
 // Persistent kernel with per-lane refill: a lane whose ray has finished takes
@@ -345,13 +285,14 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
 // serves all idle lanes of the warp, once `refill` of them are idle or none is
 // busy), so warps stay full although ray lengths differ by 100x.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
     bool active = false, exhausted = false;
-    uint32_t e = 0, D = 0;
+    uint32_t e = 0, D = 0, T0 = 0;
     const uint32_t* nodes = nullptr;
+    const uint32_t* top = nullptr;
     uint64_t n_words = 0;
     Dda s;
     Hit h;
@@ -377,6 +318,8 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
                     nodes = S.nodes;
                     n_words = S.n_words;
                     D = S.depth;
+                    top = S.top;
+                    T0 = S.top_level;
                     const f3 o = ld3(a.p_ray_o[p]);
                     const f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
                     finished = dda_init(s, o, d, v.cc_bounce, D, h);
@@ -387,7 +330,7 @@ __global__ void __launch_bounds__(256) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_step<COUNT>(s, nodes, n_words, D, h, rc);
+            finished = dda_step<COUNT>(s, nodes, n_words, D, top, T0, h, rc);
             if (finished) active = false;
         }
         if (finished) {
@@ -475,8 +418,354 @@ __device__ __forceinline__ void write_target(nrc::TRec* t, f3 total, f3 s, f3 tp
     t->valid = ok ? 1u : 0u;
 }
 
-// shade.comp:543-575, 838-908 (bounce/shade loop) with the sun next-event
-// estimate in the place of the dormant emissive NEE, and the AccumPass deposit.
+// Per-path result of one shading step, consumed by the warp-collective
+// appends and deposits of the calling kernel.
+struct ShadeOut {
+    bool do_dep = false, app_live = false, app_ext = false, app_sh = false;
+    // learned cache: a query (its record parked in the path's ray slots until
+    // the warp's append), a recorded training sample, a hash-cache ending
+    bool want_q = false, sampled = false, hash_term = false;
+    float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
+    uint32_t dvid = 0, dscene = 0, dview = 0;
+};
+
+// One step of the bounce/shade loop (shade.comp:543-575, 838-908) for path
+// p, with the sun next-event estimate in the place of the dormant emissive
+// NEE: `hit` is the result of the ray along `dir` (ignored for a path marked
+// F_TERM), tp/direct/indirect the path state after any pending sun term was
+// resolved.  Writes the continuing path's state; the queue appends and the
+// AccumPass deposit are left to shade_emit.
+__device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4 meta, f3 tp, f3 direct,
+                                           f3 indirect, f3 dir, uint4 hit, ShadeOut& o) {
+    const uint32_t vi = meta.z & 0xFFFFu;
+    uint32_t b = (meta.z >> 16) & 0xFFu;
+    const uint32_t flags = meta.z >> 24;
+    uint32_t nf = flags & F_TRAIN;
+    uint32_t train_slot = 0xFFFFFFFFu;
+    const DevView& v = a.views[vi];
+    if (flags & F_TERM) {
+        o.do_dep = true;
+    } else {
+        if (hit.x != kHit) {  // miss (shade.comp:558-564): constant sky
+            indirect = add(indirect, mul(mk(v.sky[0], v.sky[1], v.sky[2]), tp));
+            o.do_dep = true;
+        } else {
+            const DevScene S = a.scenes[v.scene];
+            const uint32_t mi = hit.w >> 16;
+            const DevMaterial m = a.mats[mi & 127u];
+            const f3 albedo = mk(m.albedo_rough.x, m.albedo_rough.y, m.albedo_rough.z);
+            const float roughness = m.albedo_rough.w, metallic = m.params.x, spec = m.params.y;
+            const bool emissive = m.params.z != 0.0f;
+            const f3 N = shading_normal(fetch_node(S.nodes, S.n_words, hit.y), dir);
+            if (emissive) {  // shade.comp:576-583
+                const float k = m.params.w;
+                f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
+                em = mk(gmin(em.x, 20.0f), gmin(em.y, 20.0f), gmin(em.z, 20.0f));
+                if (b == 0u) direct = add(direct, em); else indirect = add(indirect, em);
+            }
+            const f3 hp = mk(float(hit.z & 0xFFFFu), float(hit.z >> 16), float(hit.w & 0xFFFFu));
+            const f3 sp = add(add(hp, mk(0.5f, 0.5f, 0.5f)), N);
+            const f3 sun = mk(v.sun[0], v.sun[1], v.sun[2]);
+            // second path vertex: a training path is recorded here, other
+            // paths may end with a cached radiance estimate
+            bool ended = false;
+            if (b == 1u && !emissive && (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN))) {
+                const uint32_t hx = hit.z & 0xFFFFu, hy = hit.z >> 16, hz = hit.w & 0xFFFFu;
+                const uint32_t cell = hash32((hx >> 3) | ((hy >> 3) << 10) | ((hz >> 3) << 20));
+                if ((v.flags & VE_FRAME_TRAIN) && a.ns &&
+                    hash32(p ^ (v.frame_index * 0x9E3779B9u)) < a.train_thresh) {
+                    nf |= F_TRAIN;
+                    train_slot = atomicAdd(&a.counters[CNT_NRC_S], 1u);  // ~2^16 per frame
+                    if (train_slot < a.ns_cap) {
+                        nrc::TRec t{};
+                        t.t0 = tp.x; t.t1 = tp.y; t.t2 = tp.z;
+                        const f3 sum = add(direct, indirect);
+                        t.s0 = sum.x; t.s1 = sum.y; t.s2 = sum.z;
+                        t.cell = cell;
+                        a.nt[train_slot] = t;
+                        o.sampled = true;
+                    } else {
+                        train_slot = 0xFFFFFFFFu;
+                    }
+                    a.p_aux[p] = train_slot;
+                } else if (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH)) {
+                    bool mlp = false;
+                    if ((v.flags & VE_FRAME_LEARNED) && a.nq) {
+                        const float4* cs = a.val + 2u * (cell & a.val_mask);
+                        const float4 et = cs[0], ey = cs[1];
+                        if (et.w < float(kMinCellSamples)) {
+                            mlp = a.nrc_ready != 0u;
+                        } else {
+                            const float ex = (ey.x - et.x) * (ey.x - et.x) / (et.x * et.x + 0.01f);
+                            const float eg = (ey.y - et.y) * (ey.y - et.y) / (et.y * et.y + 0.01f);
+                            const float eb = (ey.z - et.z) * (ey.z - et.z) / (et.z * et.z + 0.01f);
+                            mlp = ((ex + eg) + eb) / 3.0f <= a.fallback_thr;
+                        }
+                    }
+                    if (mlp) {
+                        o.want_q = true;
+                        ended = true;
+                        a.p_tp[p] = st3(tp);
+                        a.p_direct[p] = st3(direct);
+                        a.p_indirect[p] = st3(indirect);
+                    } else {
+                        const Avg r = lookup_avg(S, voxel_key(hx, hy, hz) + 1u);
+                        if (r.count >= kHashTermMinCount) {
+                            indirect = add(indirect, mul(tp, r.rgb));
+                            o.do_dep = true;
+                            ended = true;
+                            o.hash_term = true;
+                        }
+                    }
+                }
+                if (o.sampled || o.want_q) {
+                    const float inv_l = 1.0f / float(1u << S.depth);
+                    const float2 on = oct_encode(N), ov = oct_encode(mk(-dir.x, -dir.y, -dir.z));
+                    nrc::QRec qr;
+                    qr.px = (hp.x + 0.5f) * inv_l;
+                    qr.py = (hp.y + 0.5f) * inv_l;
+                    qr.pz = (hp.z + 0.5f) * inv_l;
+                    qr.path = p;
+                    qr.nx = on.x;
+                    qr.ny = on.y;
+                    qr.vx = ov.x;
+                    qr.vy = ov.y;
+                    if (o.sampled) {
+                        a.ns[train_slot] = qr;
+                    } else {  // parked in the ended path's ray slots until the warp's query append
+                        a.p_ray_o[p] = make_float4(qr.px, qr.py, qr.pz, __uint_as_float(qr.path));
+                        a.p_ray_d[p] = make_float4(qr.nx, qr.ny, qr.vx, qr.vy);
+                    }
+                }
+            }
+            if (!ended && !emissive && b < 2u && dot(N, sun) > 0.0f) {
+                const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
+                f3 c = muls(brdf, v.sun_intensity);
+                c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
+                a.p_pend[p] = st3(mul(tp, c), b == 0u ? 0.0f : 1.0f);
+                nf |= F_PENDING;
+                o.app_sh = true;
+            }
+            bool term = false;
+            uint32_t rng = meta.y;
+            if (ended) {
+                // ended by a cache: deposited now (hash) or after inference (network)
+            } else if (b + 1u >= v.bounces + 1u) {
+                term = true;
+            } else {
+                const bool use_ggx = metallic * (1.0f - roughness) > 0.5f;
+                f3 sdir, bt;
+                if (use_ggx) {
+                    const f3 V = mk(-dir.x, -dir.y, -dir.z);
+                    const f3 H = sample_ggx_vndf(N, V, roughness, rng);
+                    sdir = reflect(dir, H);
+                    if (dot(sdir, N) <= 0.0f) {
+                        sdir = cosine_direction(N, rng);
+                        bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
+                    } else {
+                        const f3 F0 = mk(0.04f * (1.0f - metallic) + albedo.x * metallic,
+                                         0.04f * (1.0f - metallic) + albedo.y * metallic,
+                                         0.04f * (1.0f - metallic) + albedo.z * metallic);
+                        bt = ggx_throughput(N, V, sdir, H, roughness, F0);
+                    }
+                } else {
+                    sdir = cosine_direction(N, rng);
+                    bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
+                }
+                f3 ntp = mul(tp, bt);
+                if (b + 1u >= 2u) {  // Russian roulette, RR_START_BOUNCE = 2
+                    const float pr = gclamp(gmax(ntp.x, gmax(ntp.y, ntp.z)), 0.05f, 0.95f);
+                    const float xi = rand01(rng);
+                    if (xi > pr) term = true;
+                    else ntp = divs(ntp, pr);
+                }
+                if (!term) {
+                    tp = ntp;
+                    dir = sdir;
+                    b++;
+                    o.app_ext = true;
+                }
+            }
+            if (term) {
+                if (nf & F_PENDING) nf |= F_TERM;
+                else o.do_dep = true;
+            }
+            if (o.app_ext || (nf & F_PENDING)) {
+                o.app_live = true;
+                a.p_ray_o[p] = st3(sp);
+                a.p_ray_d[p] = st3(dir);
+                a.p_tp[p] = st3(tp);
+                a.p_direct[p] = st3(direct);
+                a.p_indirect[p] = st3(indirect);
+                meta.y = rng;
+                meta.z = vi | (b << 16) | (nf << 24);
+                a.p_meta[p] = meta;
+            }
+        }
+    }
+    if (o.do_dep) {
+        deposit_value(direct, indirect, o.dr, o.dg, o.db, o.dl2);
+        if ((flags | nf) & F_TRAIN) {  // training path: its target
+            const uint32_t k = (nf & F_TRAIN) && !(flags & F_TRAIN) ? train_slot : a.p_aux[p];
+            if (k < a.ns_cap) {
+                nrc::TRec* t = a.nt + k;
+                write_target(t, add(direct, indirect), mk(t->s0, t->s1, t->s2), mk(t->t0, t->t1, t->t2));
+            }
+        }
+        o.dvid = meta.x;
+        o.dscene = v.scene;
+        o.dview = vi;
+        if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
+            a.path_rgb[3ull * p + 0] = o.dr;
+            a.path_rgb[3ull * p + 1] = o.dg;
+            a.path_rgb[3ull * p + 2] = o.db;
+        }
+    }
+}
+
+// The warp-collective part of a shading step: queue appends (live paths,
+// extension and shadow rays, learned-cache queries and samples) and the
+// warp-aggregated deposit.  Called by all 32 lanes.
+__device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const ShadeOut& o, uint32_t* live_out,
+                                           uint32_t* live_cnt, uint32_t* ray_cnt, DepSlot* dep, uint32_t& n_ext,
+                                           uint32_t& n_sh) {
+    const uint32_t sl = warp_append(o.app_live, live_cnt);
+    if (o.app_live) live_out[sl] = p;
+    const uint32_t se = warp_append(o.app_ext, ray_cnt);
+    if (o.app_ext) a.rayq[se] = p;
+    const uint32_t ss = warp_append(o.app_sh, ray_cnt);
+    if (o.app_sh) a.rayq[ss] = p | 0x80000000u;
+    n_ext += o.app_ext ? 1u : 0u;
+    n_sh += o.app_sh ? 1u : 0u;
+    if (a.nq || a.ns) {
+        // learned cache: query records move from the path's ray slots into
+        // the query queue (capacity = paths, never full)
+        const uint32_t kq = warp_append(o.want_q, &a.counters[CNT_NRC_Q]);
+        if (o.want_q && kq < a.nq_cap) {
+            const float4 r0 = a.p_ray_o[p], r1 = a.p_ray_d[p];
+            nrc::QRec q;
+            q.px = r0.x; q.py = r0.y; q.pz = r0.z; q.path = __float_as_uint(r0.w);
+            q.nx = r1.x; q.ny = r1.y; q.vx = r1.z; q.vy = r1.w;
+            a.nq[kq] = q;
+        }
+        warp_add_stat(&a.stats[ST_NRC_QUERIES], o.want_q ? 1u : 0u);
+        warp_add_stat(&a.stats[ST_NRC_SAMPLES], o.sampled ? 1u : 0u);
+    }
+    warp_add_stat(&a.stats[ST_NRC_HASH], o.hash_term ? 1u : 0u);
+    warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, a.stats);
+    if (a.remaining) {  // serving: count finished paths per view slot
+        const unsigned dm = __ballot_sync(0xffffffffu, o.do_dep);
+        if (o.do_dep) {
+            const unsigned peers = __match_any_sync(dm, o.dview);
+            if (int(lane_id()) == __ffs(peers) - 1) atomicSub(&a.remaining[o.dview], uint32_t(__popc(peers)));
+        }
+    }
+}
+
+// RayPass primary (generate_primary.comp:38-85) + path seeding (emit.comp:39-101).
+// FUSED: each seeded path also takes its first shading step here, from the
+// hit in registers (the same shade_step the shade pass runs), appending its
+// rays and live entry for trace pass 0 / shade pass 1 — the frame's largest
+// shade pass never round-trips the path state through memory.
+template <bool COUNT, bool FUSED>
+__global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
+    __shared__ DepSlot dep[FUSED ? 256 : 1];
+    const uint32_t tile = blockIdx.x;
+    const uint32_t vi = find_view(a.views, a.n_views, tile);
+    const DevView& v = a.views[vi];
+    uint32_t px, py;
+    tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
+    const bool inside = px < v.W && py < v.H;
+    const DevScene S = a.scenes[v.scene];
+    Hit h;
+    h.status = kEscaped;
+    h.checks = 0;
+    f3 dir = mk(0.0f, 0.0f, 0.0f);
+    RayCount rc;
+    uint32_t vid = 0;
+    if (inside) {
+        const float ndx = (float(px) + 0.5f) / float(v.W) * 2.0f - 1.0f;
+        const float ndy = (float(py) + 0.5f) / float(v.H) * 2.0f - 1.0f;
+        const f3 plane = mk(v.cam[4], v.cam[5], v.cam[6]);
+        const f3 right = mk(v.cam[8], v.cam[9], v.cam[10]);
+        const f3 up = mk(v.cam[12], v.cam[13], v.cam[14]);
+        dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
+        h = raycast<COUNT>(S.nodes, S.n_words, S.depth, S.top, S.top_level, mk(v.cam[0], v.cam[1], v.cam[2]), dir,
+                           v.cc_primary, rc);
+        if (h.status == kHit) vid = voxel_key(h.x, h.y, h.z) + 1u;
+        const uint32_t pix = py * v.W + px;
+        a.gbuf[v.pix_base + pix] = make_uint4(h.checks, h.status == kHit ? h.material : 0u,
+                                              h.status == kHit ? h.id : 0u, vid);
+    }
+    const bool spawn = inside && vid != 0u;
+    if (FUSED) {
+        // the warp's (pixel, sample) pairs in chunks of 32, pixel-major: the
+        // lanes of one chunk hold consecutive path slots (a row of the warp's
+        // 8 x 4 pixel block), so path-state stores and queue entries stay
+        // coalesced.  Lane i traced pixel i of the block.
+        uint32_t n_ext = 0, n_sh = 0;
+        const uint32_t lane = lane_id();
+        const uint32_t spp = v.spp;  // one view per block: uniform
+        const uint32_t pix = py * v.W + px;
+        const uint32_t hxy = h.x | (h.y << 16), hzm = h.z | (h.material << 16);
+        for (uint32_t it = 0; it < spp; it++) {
+            const uint32_t qi = it * 32u + lane;
+            const uint32_t src = qi / spp, s = qi - src * spp;
+            const bool sp = __shfl_sync(0xffffffffu, spawn ? 1 : 0, int(src)) != 0;
+            const uint32_t svid = __shfl_sync(0xffffffffu, vid, int(src));
+            const uint32_t spix = __shfl_sync(0xffffffffu, pix, int(src));
+            const uint32_t sid = __shfl_sync(0xffffffffu, h.id, int(src));
+            const uint32_t sxy = __shfl_sync(0xffffffffu, hxy, int(src));
+            const uint32_t szm = __shfl_sync(0xffffffffu, hzm, int(src));
+            const f3 sdir = mk(__shfl_sync(0xffffffffu, dir.x, int(src)), __shfl_sync(0xffffffffu, dir.y, int(src)),
+                               __shfl_sync(0xffffffffu, dir.z, int(src)));
+            const uint32_t p = uint32_t(v.path_base + (unsigned long long)spix * spp + s);
+            ShadeOut o;
+            if (sp) {
+                const uint32_t list_idx = spix * spp + s;
+                // emit.comp:171-174
+                const uint32_t sample_idx = v.frame_index + spix * 2654435761u + list_idx * 1442695040u;
+                const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+                shade_step(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
+                           mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sid, sxy, szm), o);
+            }
+            shade_emit(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
+                       dep + (threadIdx.x & ~31u), n_ext, n_sh);
+        }
+        warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
+        warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+    }
+    const uint32_t q = FUSED ? 0u : warp_append(spawn, &a.counters[CNT_LIVE + 0], v.spp);
+    if (!FUSED && spawn) {
+        const uint32_t pix = py * v.W + px;
+        for (uint32_t s = 0; s < v.spp; s++) {
+            const unsigned long long p = v.path_base + (unsigned long long)pix * v.spp + s;
+            const uint32_t list_idx = pix * v.spp + s;
+            // emit.comp:171-174
+            const uint32_t sample_idx = v.frame_index + pix * 2654435761u + list_idx * 1442695040u;
+            const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+            a.p_ray_d[p] = st3(dir);
+            a.p_tp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.p_hit[p] = make_uint4(kHit, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+            a.p_meta[p] = make_uint4(vid, rng, vi + a.view_offset, pix);
+            a.live[0][q + s] = uint32_t(p);
+        }
+    }
+    warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside ? 1u : 0u);
+    warp_add_stat(&a.stats[ST_PATHS], spawn ? v.spp : 0u);
+    if (a.remaining) {  // the whole block belongs to one view
+        uint32_t sp = spawn ? v.spp : 0u;
+        for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        if (lane_id() == 0 && sp) atomicAdd(&a.remaining[vi + a.view_offset], sp);
+    }
+    if (COUNT) {
+        warp_add_stat(&a.stats[ST_FETCH], rc.fetch);
+        warp_add_stat(&a.stats[ST_STEPS], rc.steps);
+    }
+}
+
 __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
@@ -489,25 +778,12 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < n;
         const uint32_t p = valid ? live_in[i] : 0u;
-        bool do_dep = false, app_live = false, app_ext = false, app_sh = false;
-        float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
-        uint32_t dvid = 0, dscene = 0, dview = 0;
-        // learned-cache hand-offs, appended after the divergent part
-        bool want_q = false, want_s = false, dep_train = false, hash_term = false;
-        nrc::QRec qrec{};
-        uint32_t qcell = 0;
-        f3 s_tp = mk(0.0f, 0.0f, 0.0f), s_sum = mk(0.0f, 0.0f, 0.0f), dep_total = mk(0.0f, 0.0f, 0.0f);
+        ShadeOut o;
         if (valid) {
-            uint4 meta = a.p_meta[p];
-            const uint32_t vi = meta.z & 0xFFFFu;
-            uint32_t b = (meta.z >> 16) & 0xFFu;
+            const uint4 meta = a.p_meta[p];
             const uint32_t flags = meta.z >> 24;
-            uint32_t nf = flags & F_TRAIN;
-            const DevView& v = a.views[vi];
-            f3 tp = ld3(a.p_tp[p]);
             f3 direct = ld3(a.p_direct[p]);
             f3 indirect = ld3(a.p_indirect[p]);
-            f3 dir = ld3(a.p_ray_d[p]);
             if (flags & F_PENDING) {
                 if (a.p_vis[p]) {
                     const float4 pe = a.p_pend[p];
@@ -515,213 +791,10 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
                     else indirect = add(indirect, ld3(pe));
                 }
             }
-            if (flags & F_TERM) {
-                do_dep = true;
-            } else {
-                const uint4 hit = a.p_hit[p];
-                if (hit.x != kHit) {  // miss (shade.comp:558-564): constant sky
-                    indirect = add(indirect, mul(mk(v.sky[0], v.sky[1], v.sky[2]), tp));
-                    do_dep = true;
-                } else {
-                    const DevScene S = a.scenes[v.scene];
-                    const uint32_t mi = hit.w >> 16;
-                    const DevMaterial m = a.mats[mi & 127u];
-                    const f3 albedo = mk(m.albedo_rough.x, m.albedo_rough.y, m.albedo_rough.z);
-                    const float roughness = m.albedo_rough.w, metallic = m.params.x, spec = m.params.y;
-                    const bool emissive = m.params.z != 0.0f;
-                    const f3 N = shading_normal(fetch_node(S.nodes, S.n_words, hit.y), dir);
-                    if (emissive) {  // shade.comp:576-583
-                        const float k = m.params.w;
-                        f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
-                        em = mk(gmin(em.x, 20.0f), gmin(em.y, 20.0f), gmin(em.z, 20.0f));
-                        if (b == 0u) direct = add(direct, em); else indirect = add(indirect, em);
-                    }
-                    const f3 hp = mk(float(hit.z & 0xFFFFu), float(hit.z >> 16), float(hit.w & 0xFFFFu));
-                    const f3 sp = add(add(hp, mk(0.5f, 0.5f, 0.5f)), N);
-                    const f3 sun = mk(v.sun[0], v.sun[1], v.sun[2]);
-                    // second path vertex: a training path is recorded here, other
-                    // paths may end with a cached radiance estimate
-                    bool ended = false;
-                    if (b == 1u && !emissive && (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN))) {
-                        const uint32_t hx = hit.z & 0xFFFFu, hy = hit.z >> 16, hz = hit.w & 0xFFFFu;
-                        const uint32_t cell = hash32((hx >> 3) | ((hy >> 3) << 10) | ((hz >> 3) << 20));
-                        if ((v.flags & VE_FRAME_TRAIN) && a.ns &&
-                            hash32(p ^ (v.frame_index * 0x9E3779B9u)) < a.train_thresh) {
-                            want_s = true;
-                            nf |= F_TRAIN;
-                            s_tp = tp;
-                            s_sum = add(direct, indirect);
-                        } else if (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH)) {
-                            bool mlp = false;
-                            if ((v.flags & VE_FRAME_LEARNED) && a.nq) {
-                                const float4* cs = a.val + 2u * (cell & a.val_mask);
-                                const float4 et = cs[0], ey = cs[1];
-                                if (et.w < float(kMinCellSamples)) {
-                                    mlp = a.nrc_ready != 0u;
-                                } else {
-                                    const float ex = (ey.x - et.x) * (ey.x - et.x) / (et.x * et.x + 0.01f);
-                                    const float eg = (ey.y - et.y) * (ey.y - et.y) / (et.y * et.y + 0.01f);
-                                    const float eb = (ey.z - et.z) * (ey.z - et.z) / (et.z * et.z + 0.01f);
-                                    mlp = ((ex + eg) + eb) / 3.0f <= a.fallback_thr;
-                                }
-                            }
-                            if (mlp) {
-                                want_q = true;
-                                ended = true;
-                                a.p_tp[p] = st3(tp);
-                                a.p_direct[p] = st3(direct);
-                                a.p_indirect[p] = st3(indirect);
-                            } else {
-                                const Avg r = lookup_avg(S, voxel_key(hx, hy, hz) + 1u);
-                                if (r.count >= kHashTermMinCount) {
-                                    indirect = add(indirect, mul(tp, r.rgb));
-                                    do_dep = true;
-                                    ended = true;
-                                    hash_term = true;
-                                }
-                            }
-                        }
-                        if (want_s || want_q) {
-                            const float inv_l = 1.0f / float(1u << S.depth);
-                            qrec.px = (hp.x + 0.5f) * inv_l;
-                            qrec.py = (hp.y + 0.5f) * inv_l;
-                            qrec.pz = (hp.z + 0.5f) * inv_l;
-                            qrec.path = p;
-                            const float2 on = oct_encode(N), ov = oct_encode(mk(-dir.x, -dir.y, -dir.z));
-                            qrec.nx = on.x;
-                            qrec.ny = on.y;
-                            qrec.vx = ov.x;
-                            qrec.vy = ov.y;
-                            qcell = cell;
-                        }
-                    }
-                    if (!ended && !emissive && b < 2u && dot(N, sun) > 0.0f) {
-                        const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
-                        f3 c = muls(brdf, v.sun_intensity);
-                        c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
-                        a.p_pend[p] = st3(mul(tp, c), b == 0u ? 0.0f : 1.0f);
-                        nf |= F_PENDING;
-                        app_sh = true;
-                    }
-                    bool term = false;
-                    uint32_t rng = meta.y;
-                    if (ended) {
-                        // ended by a cache: deposited now (hash) or after inference (network)
-                    } else if (b + 1u >= v.bounces + 1u) {
-                        term = true;
-                    } else {
-                        const bool use_ggx = metallic * (1.0f - roughness) > 0.5f;
-                        f3 sdir, bt;
-                        if (use_ggx) {
-                            const f3 V = mk(-dir.x, -dir.y, -dir.z);
-                            const f3 H = sample_ggx_vndf(N, V, roughness, rng);
-                            sdir = reflect(dir, H);
-                            if (dot(sdir, N) <= 0.0f) {
-                                sdir = cosine_direction(N, rng);
-                                bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
-                            } else {
-                                const f3 F0 = mk(0.04f * (1.0f - metallic) + albedo.x * metallic,
-                                                 0.04f * (1.0f - metallic) + albedo.y * metallic,
-                                                 0.04f * (1.0f - metallic) + albedo.z * metallic);
-                                bt = ggx_throughput(N, V, sdir, H, roughness, F0);
-                            }
-                        } else {
-                            sdir = cosine_direction(N, rng);
-                            bt = evaluate_brdf(dir, sdir, N, albedo, roughness, metallic, spec);
-                        }
-                        f3 ntp = mul(tp, bt);
-                        if (b + 1u >= 2u) {  // Russian roulette, RR_START_BOUNCE = 2
-                            const float pr = gclamp(gmax(ntp.x, gmax(ntp.y, ntp.z)), 0.05f, 0.95f);
-                            const float xi = rand01(rng);
-                            if (xi > pr) term = true;
-                            else ntp = divs(ntp, pr);
-                        }
-                        if (!term) {
-                            tp = ntp;
-                            dir = sdir;
-                            b++;
-                            app_ext = true;
-                        }
-                    }
-                    if (term) {
-                        if (nf & F_PENDING) nf |= F_TERM;
-                        else do_dep = true;
-                    }
-                    if (app_ext || (nf & F_PENDING)) {
-                        app_live = true;
-                        a.p_ray_o[p] = st3(sp);
-                        a.p_ray_d[p] = st3(dir);
-                        a.p_tp[p] = st3(tp);
-                        a.p_direct[p] = st3(direct);
-                        a.p_indirect[p] = st3(indirect);
-                        meta.y = rng;
-                        meta.z = vi | (b << 16) | (nf << 24);
-                        a.p_meta[p] = meta;
-                    }
-                }
-            }
-            if (do_dep) {
-                deposit_value(direct, indirect, dr, dg, db, dl2);
-                if ((flags | nf) & F_TRAIN) {
-                    dep_train = true;
-                    dep_total = add(direct, indirect);
-                }
-                dvid = meta.x;
-                dscene = v.scene;
-                dview = vi;
-                if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
-                    a.path_rgb[3ull * p + 0] = dr;
-                    a.path_rgb[3ull * p + 1] = dg;
-                    a.path_rgb[3ull * p + 2] = db;
-                }
-            }
+            const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
+            shade_step(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
         }
-        const uint32_t sl = warp_append(app_live, live_cnt);
-        if (app_live) live_out[sl] = p;
-        const uint32_t se = warp_append(app_ext, ray_cnt);
-        if (app_ext) a.rayq[se] = p;
-        const uint32_t ss = warp_append(app_sh, ray_cnt);
-        if (app_sh) a.rayq[ss] = p | 0x80000000u;
-        n_ext += app_ext ? 1u : 0u;
-        n_sh += app_sh ? 1u : 0u;
-        if (a.nq || a.ns) {
-            // learned cache: queries (capacity = paths, never full) and
-            // training samples (a path past the capacity stays plain)
-            const uint32_t kq = warp_append(want_q, &a.counters[CNT_NRC_Q]);
-            if (want_q && kq < a.nq_cap) a.nq[kq] = qrec;
-            const uint32_t ks = warp_append(want_s, &a.counters[CNT_NRC_S]);
-            uint32_t slot = 0xFFFFFFFFu;
-            if (want_s && ks < a.ns_cap) {
-                slot = ks;
-                a.ns[ks] = qrec;
-                nrc::TRec t{};
-                t.t0 = s_tp.x; t.t1 = s_tp.y; t.t2 = s_tp.z;
-                t.s0 = s_sum.x; t.s1 = s_sum.y; t.s2 = s_sum.z;
-                t.cell = qcell;
-                a.nt[ks] = t;
-            }
-            if (want_s) a.p_aux[p] = slot;
-            if (dep_train) {
-                const uint32_t k = want_s ? slot : a.p_aux[p];
-                if (k < a.ns_cap) {
-                    nrc::TRec* t = a.nt + k;
-                    const f3 tp0 = want_s ? s_tp : mk(t->t0, t->t1, t->t2);
-                    const f3 s0 = want_s ? s_sum : mk(t->s0, t->s1, t->s2);
-                    write_target(t, dep_total, s0, tp0);
-                }
-            }
-            warp_add_stat(&a.stats[ST_NRC_QUERIES], want_q ? 1u : 0u);
-            warp_add_stat(&a.stats[ST_NRC_SAMPLES], (want_s && slot != 0xFFFFFFFFu) ? 1u : 0u);
-        }
-        warp_add_stat(&a.stats[ST_NRC_HASH], hash_term ? 1u : 0u);
-        warp_deposit(do_dep, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
-        if (a.remaining) {  // serving: count finished paths per view slot
-            const unsigned dm = __ballot_sync(0xffffffffu, do_dep);
-            if (do_dep) {
-                const unsigned peers = __match_any_sync(dm, dview);
-                if (int(lane_id()) == __ffs(peers) - 1) atomicSub(&a.remaining[dview], uint32_t(__popc(peers)));
-            }
-        }
+        shade_emit(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), n_ext, n_sh);
     }
     warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
@@ -1014,6 +1087,8 @@ struct SceneSlot {
     uint64_t n_words = 0;
     uint32_t depth = 0;
     CacheEntry* cache = nullptr;
+    uint32_t* top = nullptr;  // top table of the DDA descent (see raycast.cuh)
+    uint32_t top_level = 0;
     bool live = false;
     ve_nrc* nrc = nullptr;  // learned radiance cache attached to the scene
 };
@@ -1119,7 +1194,7 @@ static int sync_scenes(ve_ctx* c) {
     std::vector<DevScene> h(std::max<size_t>(c->scenes.size(), 1));
     for (size_t i = 0; i < c->scenes.size(); i++) {
         const SceneSlot& s = c->scenes[i];
-        h[i] = DevScene{s.nodes, s.n_words, s.cache, s.depth, c->cfg.hash_log2, c->cfg.hash_probes, 0u};
+        h[i] = DevScene{s.nodes, s.n_words, s.cache, s.depth, c->cfg.hash_log2, c->cfg.hash_probes, s.top_level, s.top};
     }
     const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
@@ -1128,6 +1203,47 @@ static int sync_scenes(ve_ctx* c) {
     VE_CUDA(cudaMemcpyAsync(c->d_scenes.p, h.data(), h.size() * sizeof(DevScene), cudaMemcpyHostToDevice, c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
     c->scenes_dirty = false;
+    return VE_OK;
+}
+
+// Top table of the DDA descent: one word per cell of the level-(T0-1) grid,
+// found by walking levels 0..T0-1 of the node words exactly as the descent
+// does (out-of-range words read as zero).
+__global__ void k_build_top(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, uint32_t T0,
+                            uint32_t* __restrict__ top) {
+    const uint32_t b = T0 - 1u, n = 1u << (3u * b);
+    const uint32_t sh = D - T0 + 1u, L = 1u << D;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t x = (i >> (2u * b)) << sh, y = ((i >> b) & ((1u << b) - 1u)) << sh, z = (i & ((1u << b) - 1u)) << sh;
+        uint32_t base = 0, ent = 0;
+        bool terminal = false;
+        for (uint32_t k = 0; k < T0; k++) {
+            const uint32_t raw = dev::fetch_node(nodes, n_words, base + locate(x, y, z, L >> k));
+            if (!(raw & 1u)) {
+                ent = k << 1;
+                terminal = true;
+                break;
+            }
+            base = raw >> 4;
+        }
+        top[i] = terminal ? ent : ((base << 1) | 1u);
+    }
+}
+
+// Levels resolved by the top table: 8 for depth >= 9 (a 128^3-word table,
+// 8 MB), depth - 1 below that, none under depth 3.
+static uint32_t top_levels(uint32_t D) { return D < 3u ? 0u : std::min(8u, D - 1u); }
+
+static int build_top(ve_ctx* c, SceneSlot& s) {
+    const uint32_t T0 = top_levels(s.depth);
+    if (T0 == 0) return VE_OK;
+    const size_t n = size_t(1) << (3u * (T0 - 1u));
+    if (!s.top) {
+        if (cudaMalloc(&s.top, n * 4) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene: top table allocation failed");
+    }
+    s.top_level = T0;
+    k_build_top<<<c->num_sms * 8, 256, 0, c->stream>>>(s.nodes, s.n_words, s.depth, T0, s.top);
+    VE_CUDA(cudaGetLastError());
     return VE_OK;
 }
 
@@ -1432,13 +1548,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
         }
         rec();
-        if (count) k_primary<true><<<tiles, 256, 0, st>>>(a);
-        else k_primary<false><<<tiles, 256, 0, st>>>(a);
+        if (count) k_primary<true, true><<<tiles, 256, 0, st>>>(a);
+        else k_primary<false, true><<<tiles, 256, 0, st>>>(a);
         launches++;
         rec();
         for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
-            k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
-            launches++;
+            if (pass > 0) {  // pass 0 runs inside the fused primary
+                k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
+                launches++;
+            }
             rec();
             if (pass <= max_b) {
                 if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
@@ -1635,12 +1753,12 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
                     const float s2 = std::sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
                     ntab[((ix + 9) * 19 + (iy + 9)) * 19 + (iz + 9)] = make_float4(u[0] / s2, u[1] / s2, u[2] / s2, 0.0f);
                 }
-        if (cudaMemcpyToSymbol(g_normal_table, ntab, sizeof(ntab)) != cudaSuccess) {
-            cudaStreamDestroy(x->stream);
-            delete x;
-            return fail(VE_ERR_CUDA, "ctx_create: normal table upload failed");
-        }
-        if (cudaMemcpyToSymbol(c_halton_f, tab, sizeof(tab)) != cudaSuccess) {
+        // through the context's non-blocking stream, waited for before the
+        // host tables go out of scope and before any kernel reads them
+        if (cudaMemcpyToSymbolAsync(g_normal_table, ntab, sizeof(ntab), 0, cudaMemcpyHostToDevice, x->stream) !=
+                cudaSuccess ||
+            cudaMemcpyToSymbolAsync(c_halton_f, tab, sizeof(tab), 0, cudaMemcpyHostToDevice, x->stream) != cudaSuccess ||
+            cudaStreamSynchronize(x->stream) != cudaSuccess) {
             cudaStreamDestroy(x->stream);
             delete x;
             return fail(VE_ERR_CUDA, "ctx_create: constant table upload failed");
@@ -1662,9 +1780,14 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
         return rc;
     }
     cudaMallocHost(&x->h_stats, ST_TOTAL * sizeof(unsigned long long));
-    cudaMemset(x->d_mats.p, 0, 128 * sizeof(DevMaterial));
-    cudaMemset(x->totals.p, 0, ST_TOTAL * sizeof(unsigned long long));
-    cudaMemset(x->stats.p, 0, ST_TOTAL * sizeof(unsigned long long));
+    // on the context's non-blocking stream, finished before the first use
+    cudaMemsetAsync(x->d_mats.p, 0, 128 * sizeof(DevMaterial), x->stream);
+    cudaMemsetAsync(x->totals.p, 0, ST_TOTAL * sizeof(unsigned long long), x->stream);
+    cudaMemsetAsync(x->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), x->stream);
+    if (cudaStreamSynchronize(x->stream) != cudaSuccess) {
+        ve_ctx_destroy(x);
+        return fail(VE_ERR_CUDA, "ctx_create: initialisation failed");
+    }
     *out = x;
     return VE_OK;
 }
@@ -1677,6 +1800,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     for (auto& s : c->scenes) {
         if (s.alloc) cudaFree(s.alloc);
         if (s.cache) cudaFree(s.cache);
+        if (s.top) cudaFree(s.top);
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
     c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
@@ -1736,11 +1860,18 @@ int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t
     VE_CUDA(cudaMemcpyAsync(s.nodes, words, n_words * 4, cudaMemcpyHostToDevice, c->stream));
     VE_CUDA(cudaMemsetAsync(s.cache, 0, cache_bytes, c->stream));
     s.live = true;
+    if (int rc = build_top(c, s)) {
+        cudaFree(s.alloc);
+        cudaFree(s.cache);
+        if (s.top) cudaFree(s.top);
+        return rc;
+    }
     if (!(flags & VE_SCENE_KEEP_NORMALS)) {
         int rc = compute_normals(c, s);
         if (rc) {
             cudaFree(s.alloc);
             cudaFree(s.cache);
+            if (s.top) cudaFree(s.top);
             return rc;
         }
     }
@@ -1768,6 +1899,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     SceneSlot& s = c->scenes[id];
     cudaFree(s.alloc);
     cudaFree(s.cache);
+    if (s.top) cudaFree(s.top);
     s = SceneSlot();
     c->scenes_dirty = true;
     c->gen++;
@@ -1785,6 +1917,7 @@ int ve_scene_apply_edits(ve_ctx* c, int32_t id, const uint32_t* slots, const uin
     cudaSetDevice(c->device);
     for (uint64_t i = 0; i < n; i++)
         VE_CUDA(cudaMemcpyAsync(s.nodes + slots[i], words + i, 4, cudaMemcpyHostToDevice, c->stream));
+    if (int rc = build_top(c, s)) return rc;
     if (!(flags & VE_SCENE_KEEP_NORMALS)) {
         int rc = compute_normals(c, s);
         if (rc) return rc;
@@ -1808,7 +1941,9 @@ int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64
 int ve_scene_footprint(ve_ctx* c, int32_t id, uint64_t* bytes) {
     if (!c || !bytes || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_footprint: unknown scene");
-    *bytes = (c->scenes[id].n_words + 8) * 4 + (sizeof(CacheEntry) << c->cfg.hash_log2);
+    const SceneSlot& sl = c->scenes[id];
+    const uint64_t top = sl.top_level ? (4ull << (3u * (sl.top_level - 1u))) : 0ull;
+    *bytes = (sl.n_words + 8) * 4 + (sizeof(CacheEntry) << c->cfg.hash_log2) + top;
     return VE_OK;
 }
 

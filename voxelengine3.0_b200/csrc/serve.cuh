@@ -226,7 +226,7 @@ static void serve_loop(ve_server* s) {
             // live[0] / CNT_LIVE + 0 of the arguments it is given)
             ap.counters = c->counters.p + ps;
             ap.live[0] = (ps & 1u) ? c->live1.p : c->live0.p;
-            k_primary<false><<<r->tiles, 256, 0, st>>>(ap);
+            k_primary<false, false><<<r->tiles, 256, 0, st>>>(ap);
         }
         // 2. one shade + one trace pass over every live path
         k_shade<<<c->grid_shade, 256, 0, st>>>(a, ps);
@@ -410,7 +410,9 @@ int ve_server_get_stats(ve_server* s, ve_server_stats* out) {
     out->pool_bytes = s->pix_pool.capacity() * 48ull + s->path_pool.capacity() * 145ull;
     uint64_t scene_bytes = 0;
     for (const auto& sc : s->c->scenes)
-        if (sc.live) scene_bytes += (sc.n_words + 8) * 4 + (sizeof(CacheEntry) << s->c->cfg.hash_log2);
+        if (sc.live)
+            scene_bytes += (sc.n_words + 8) * 4 + (sizeof(CacheEntry) << s->c->cfg.hash_log2) +
+                           (sc.top_level ? (4ull << (3u * (sc.top_level - 1u))) : 0ull);
     out->scene_bytes = scene_bytes;
     out->rays = s->rays;
     return VE_OK;
