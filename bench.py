@@ -58,6 +58,19 @@ def load_package():
 METRIC = "Mrays/s at 1080p depth-10 octree"
 
 
+def measured_trace_traffic():
+    """DRAM bytes per k_trace launch of this workload from the committed ncu
+    capture summary (profiles/k_trace_traffic_1080p_depth10.md), or None."""
+    p = os.path.join(ROOT, "profiles", "k_trace_traffic_1080p_depth10.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -729,7 +742,9 @@ def main():
                     "d2h_bytes_per_step": etot["d2h_bytes"] / K},
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce + shadow DDA)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind, "traffic": measured_trace_traffic(),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                           "profiles/k_trace_traffic_1080p_depth10.md",
                          "algorithmic_bytes_per_launch": trace_bytes / max(launches, 1),
                          "ms_per_launch": trace_ms / max(launches, 1)},
             "gpu_launches": int(tot["kernel_launches"]),

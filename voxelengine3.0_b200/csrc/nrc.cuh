@@ -52,9 +52,10 @@ constexpr uint32_t kWBytes = kWidth * kWidth * 2;         // 8 KB per layer imag
 constexpr uint32_t kWImage = kLayers * kWBytes;           // 40 KB
 constexpr uint32_t kWParams = kLayers * kWidth * kWidth;  // f32 master weights (layer 5 rows >= 3 are zero)
 constexpr uint32_t kOutRows = 3;
-constexpr uint32_t kSmemInfer = kWImage + kTileBytes;
+constexpr uint32_t kInferGroups = 2;  // warpgroups (independent tile streams) per inference CTA
+constexpr uint32_t kSmemInfer = kWImage + kInferGroups * kTileBytes;
 constexpr uint32_t kSmemTrain = kWImage + 6 * kTileBytes;
-constexpr uint32_t kTmemInfer = 64;
+constexpr uint32_t kTmemInfer = 64 * kInferGroups;
 constexpr uint32_t kTmemTrain = 512;
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 1.9 GHz
 
@@ -132,20 +133,28 @@ __device__ __forceinline__ void encode_row(const Args& a, const QRec& r, bool va
     for (int i = 0; i < 32; i++) row[i] = 0u;
     if (!valid) return;
     const uint32_t T = 1u << a.grid.log2T;
+    // two levels per round: 16 independent gathers in flight per thread
 #pragma unroll 1
-    for (uint32_t l = 0; l < kLevels; l++) {
-        uint32_t idx[8];
-        float w[8];
-        level_corners(a.grid, l, r.px, r.py, r.pz, idx, w);
-        float f0 = 0.0f, f1 = 0.0f;
+    for (uint32_t l = 0; l < kLevels; l += 2) {
+        uint32_t idx[2][8], h[2][8];
+        float w[2][8];
+        level_corners(a.grid, l, r.px, r.py, r.pz, idx[0], w[0]);
+        level_corners(a.grid, l + 1u, r.px, r.py, r.pz, idx[1], w[1]);
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const uint32_t h = __ldg(a.table + size_t(l) * T + idx[c]);
-            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h));
-            f0 += w[c] * f.x;
-            f1 += w[c] * f.y;
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int c = 0; c < 8; c++) h[k][c] = __ldg(a.table + size_t(l + k) * T + idx[k][c]);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[k][c]));
+                f0 += w[k][c] * f.x;
+                f1 += w[k][c] * f.y;
+            }
+            row[l + k] = tc::pack_bf16(f0, f1);
         }
-        row[l] = tc::pack_bf16(f0, f1);
     }
     row[16] = tc::pack_bf16(r.nx, r.ny);
     row[17] = tc::pack_bf16(r.vx, r.vy);
@@ -420,6 +429,107 @@ __global__ void __launch_bounds__(128, TRAIN ? 1 : 4) k_nrc_mlp(Args a) {
     tc::fence_before();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+}
+
+__device__ __forceinline__ void group_sync(uint32_t g) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1u + g) : "memory");
+}
+
+// Inference: two warpgroups per CTA run independent tile streams, each with
+// its own operand tile, tensor-memory columns (M = 128 accumulator, lanes
+// 0-127) and mbarrier, so one group's gathers and epilogues overlap the
+// other's tensor-core work; three CTAs per SM (shared memory and 384 of the
+// 512 tensor-memory columns).
+__global__ void __launch_bounds__(256, 3) k_nrc_infer(Args a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t mbar[kInferGroups];
+    __shared__ uint32_t tmem_base;
+    uint8_t* sw = smem;
+    const uint32_t tid = threadIdx.x, g = tid >> 7, t = tid & 127u, warp = tid >> 5;
+    uint8_t* sh = smem + kWImage + g * kTileBytes;
+
+    for (uint32_t i = tid; i < kWImage / 16u; i += blockDim.x)
+        reinterpret_cast<uint4*>(sw)[i] = __ldg(a.wimg + i);
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, kTmemInfer);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+        for (uint32_t k = 0; k < kInferGroups; k++) tc::mbar_init(&mbar[k], 1u);
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t t_scr = tmem_base + 64u * g;
+    const uint32_t lane_sel = ((warp & 3u) * 32u) << 16;  // the warp's quarter of the lanes
+    uint32_t phase = 0;
+    bool timed_out = false;
+    const uint32_t n = a.count ? min(*a.count, a.n) : a.n;
+    const uint32_t tiles = (n + kRows - 1u) / kRows;
+    for (uint32_t tile = blockIdx.x * kInferGroups + g; tile < tiles && !timed_out;
+         tile += gridDim.x * kInferGroups) {
+        const uint32_t row = tile * kRows + t;
+        const bool valid = row < n;
+        QRec r{};
+        if (valid) r = a.q[row];
+        {
+            uint32_t x[32];
+            encode_row(a, r, valid, x);
+            store_row(sh, t, x);
+        }
+        tc::fence_async_smem();
+        tc::fence_before();
+        group_sync(g);
+        float y[3] = {0.0f, 0.0f, 0.0f};
+        for (uint32_t l = 0; l < kLayers; l++) {
+            if (t == 0) {
+                tc::fence_after();
+                issue_forward(t_scr, sh, sw + l * kWBytes, l + 1u < kLayers ? 64u : 16u);
+                tc::commit(&mbar[g]);
+            }
+            if (!tc::mbar_wait(&mbar[g], phase, kWaitCycles)) {
+                timed_out = true;
+                break;
+            }
+            phase ^= 1u;
+            tc::fence_after();
+            if (l + 1u < kLayers) {
+#pragma unroll
+                for (uint32_t half = 0; half < 2; half++) {
+                    uint32_t v[32];
+                    tc::tmem_ld32(t_scr + lane_sel + 32u * half, v);
+                    tc::tmem_wait_ld();
+                    uint32_t pk[16];
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        pk[j] = tc::pack_bf16(fmaxf(__uint_as_float(v[2 * j]), 0.0f),
+                                              fmaxf(__uint_as_float(v[2 * j + 1]), 0.0f));
+#pragma unroll
+                    for (uint32_t c = 0; c < 4; c++)
+                        *reinterpret_cast<uint4*>(sh + tc::tile_off(t, 32u * half + 8u * c)) =
+                            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+                }
+                tc::fence_async_smem();
+                tc::fence_before();
+                group_sync(g);
+            } else {
+                uint32_t v[32];
+                tc::tmem_ld32(t_scr + lane_sel, v);
+                tc::tmem_wait_ld();
+                y[0] = __uint_as_float(v[0]);
+                y[1] = __uint_as_float(v[1]);
+                y[2] = __uint_as_float(v[2]);
+            }
+        }
+        if (timed_out) break;
+        if (valid) a.out[row] = make_float4(y[0], y[1], y[2], 0.0f);
+        tc::fence_before();
+        group_sync(g);
+    }
+    if (timed_out && t == 0) atomicOr(a.status, 1u);
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem_base, kTmemInfer);
 }
 
 // ---------------------------------------------------------------------------

@@ -95,7 +95,7 @@ static void launch_infer(ve_nrc* m, cudaStream_t st, const QRec* q, const uint32
     a.grid = m->grid;
     a.out = out;
     a.status = m->status.p;
-    k_nrc_mlp<false><<<m->grid_infer, 128, kSmemInfer, st>>>(a);
+    k_nrc_infer<<<m->grid_infer, 128 * kInferGroups, kSmemInfer, st>>>(a);
 }
 
 static void launch_adam(ve_nrc* m, cudaStream_t st) {
@@ -210,17 +210,28 @@ int ve_nrc_create(ve_ctx* c, const ve_nrc_config* cfg, ve_nrc** out) {
     static_assert(kSmemTrain <= 227u * 1024u, "training tile set exceeds shared memory");
     if (cudaFuncSetAttribute(k_nrc_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemTrain)) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(k_nrc_mlp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemInfer)) !=
+        cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemInfer)) !=
             cudaSuccess) {
         ve_nrc_destroy(m);
         return fail(VE_ERR_CUDA, "nrc_create: shared-memory attribute refused");
     }
     c->nrcs.push_back(m);
     int occ_i = 0, occ_t = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_nrc_mlp<false>, 128, kSmemInfer);
+    // resident inference CTAs per SM: shared memory (the kernel prefers the
+    // largest carveout) and 512 tensor-memory columns, 128 per CTA; the
+    // occupancy query is taken as a floor only, since it assumes the default
+    // carveout
+    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaFuncSetAttribute(k_nrc_mlp<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_nrc_infer, 128 * kInferGroups, kSmemInfer) !=
+        cudaSuccess)
+        occ_i = 1;
+    int smem_sm = 0;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+    const int by_smem = smem_sm / int(kSmemInfer + 2048u);
+    occ_i = std::max(1, std::min(std::max(occ_i, by_smem), std::min(3, int(512 / kTmemInfer))));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, k_nrc_mlp<true>, 128, kSmemTrain);
-    // tensor memory: 512 columns per SM; inference CTAs take 64, training 512
-    occ_i = std::max(1, std::min(occ_i, int(512 / kTmemInfer)));
+    cudaGetLastError();
     occ_t = 1;
     m->grid_infer = c->num_sms * occ_i;
     m->grid_train = c->num_sms * occ_t;

@@ -668,7 +668,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
 // rays and live entry for trace pass 0 / shade pass 1 — the frame's largest
 // shade pass never round-trips the path state through memory.
 template <bool COUNT, bool FUSED>
-__global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
+__global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     __shared__ DepSlot dep[FUSED ? 256 : 1];
     const uint32_t tile = blockIdx.x;
     const uint32_t vi = find_view(a.views, a.n_views, tile);
@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(256) k_primary(FrameArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
     const uint32_t* live_in = a.live[pass & 1u];
