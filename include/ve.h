@@ -192,7 +192,23 @@ int ve_ctx_synchronize(ve_ctx* ctx);
  * a device pass fills every leaf's normal field (3x3x3 occupancy gradient). */
 int ve_scene_upload(ve_ctx* ctx, const uint32_t* words, uint64_t n_words, uint32_t depth, uint32_t flags,
                     int32_t* scene_id);
+/* GPU bulk build (no counterpart in the reference): the node words that
+ * OctreeCPU::insert of every voxel followed by Octree::set produce, built on
+ * the device from n host rows (x, y, z, material 1..127) — a repeated
+ * position keeps its last row — and uploaded as a scene like
+ * ve_scene_upload.  *n_words (may be NULL) receives the array size. */
+int ve_scene_build(ve_ctx* ctx, const uint32_t* xyzm, uint64_t n, uint32_t depth, uint32_t flags,
+                   int32_t* scene_id, uint64_t* n_words);
 int ve_scene_release(ve_ctx* ctx, int32_t scene_id);
+/* Targeted refresh after an edit, the counterpart of the reference's
+ * findGpuSlot-driven invalidation (octree.cpp:317-341): for every voxel in
+ * the 3x3x3 neighbourhood of each of the n edited positions (x, y, z), the
+ * leaf normal field is recomputed (same values as the full pass) and, unless
+ * VE_REFRESH_KEEP_CACHE, the voxel's radiance-cache entry is cleared.  Use
+ * after ve_scene_apply_edits(..., VE_SCENE_KEEP_NORMALS) in place of the full
+ * normal pass. */
+#define VE_REFRESH_KEEP_CACHE 1u
+int ve_scene_refresh(ve_ctx* ctx, int32_t scene_id, const uint32_t* xyz, uint64_t n, uint32_t flags);
 /* Octree::applyEdits upload (octree.cpp:228-314 UpdateNode): scatter
  * words[i] to slots[i]; normals of affected leaves are recomputed unless
  * VE_SCENE_KEEP_NORMALS.  The scene's radiance cache is kept. */

@@ -183,6 +183,8 @@ _SIGNATURES = {
     "ve_nrc_gradients": ([_P, _P, _P, _U32, _P, _P, _PTR(ctypes.c_float)], ctypes.c_int),
     "ve_nrc_train": ([_P, _P, _P, _U32, _PTR(ctypes.c_float)], ctypes.c_int),
     "ve_scene_set_nrc": ([_P, ctypes.c_int, _P], ctypes.c_int),
+    "ve_scene_build": ([_P, _P, _U64, _U32, _U32, _PTR(ctypes.c_int32), _PTR(_U64)], ctypes.c_int),
+    "ve_scene_refresh": ([_P, ctypes.c_int32, _P, _U64, _U32], ctypes.c_int),
     "ve_nrc_stats": ([_P, _PTR(ctypes.c_float), _PTR(_U64), _PTR(_U64)], ctypes.c_int),
     "ve_server_create": ([_P, _PTR(ServerConfigC), _PTR(_P)], ctypes.c_int),
     "ve_server_submit": ([_P, _PTR(ViewC), _P, _P, _PTR(_U64)], ctypes.c_int),
@@ -500,6 +502,16 @@ class Renderer:
                                          ctypes.byref(sid)))
         return sid.value
 
+    def build_scene(self, xyzm: np.ndarray, depth: int, keep_normals: bool = False) -> int:
+        """GPU bulk build from (x, y, z, material) rows: the words of
+        OctreeCPU.insert_many + Octree.set, built on the device."""
+        v = np.ascontiguousarray(np.asarray(xyzm, np.uint32).reshape(-1, 4))
+        sid = ctypes.c_int32()
+        nw = _U64()
+        _check(self._lib.ve_scene_build(self._h, _ptr(v) if v.size else None, v.shape[0], depth,
+                                        1 if keep_normals else 0, ctypes.byref(sid), ctypes.byref(nw)))
+        return sid.value
+
     def release_scene(self, scene_id: int) -> None:
         _check(self._lib.ve_scene_release(self._h, scene_id))
 
@@ -508,6 +520,14 @@ class Renderer:
         w = np.ascontiguousarray(words, np.uint32)
         _check(self._lib.ve_scene_apply_edits(self._h, scene_id, _ptr(s), _ptr(w), s.size,
                                               SCENE_KEEP_NORMALS if keep_normals else 0))
+
+    def refresh_scene(self, scene_id: int, positions: np.ndarray, keep_cache: bool = False) -> None:
+        """Targeted refresh around edited positions (n x 3): leaf normals of
+        their 3x3x3 neighbourhoods and, unless keep_cache, their radiance-cache
+        entries."""
+        p = np.ascontiguousarray(np.asarray(positions, np.uint32).reshape(-1, 3))
+        _check(self._lib.ve_scene_refresh(self._h, scene_id, _ptr(p) if p.size else None, p.shape[0],
+                                          1 if keep_cache else 0))
 
     def download_scene(self, scene_id: int) -> np.ndarray:
         n = _U64()

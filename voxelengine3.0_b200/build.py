@@ -26,7 +26,8 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 
 CU_SOURCES = ["render.cu"]
 CXX_SOURCES = ["host/octree_cpu.cpp", "host/terrain.cpp", "host/host_api.cpp"]
-HEADERS = ["ve_device.cuh", "raycast.cuh", "serve.cuh", "tc.cuh", "nrc.cuh", "nrc_host.cuh", "host/scene_host.h"]
+HEADERS = ["ve_device.cuh", "raycast.cuh", "serve.cuh", "tc.cuh", "nrc.cuh", "nrc_host.cuh", "builder.cuh",
+           "host/scene_host.h"]
 
 
 def _newer(target, deps):

@@ -435,12 +435,78 @@ __device__ __forceinline__ void group_sync(uint32_t g) {
     asm volatile("bar.sync %0, 128;" ::"r"(1u + g) : "memory");
 }
 
-// Inference: two warpgroups per CTA run independent tile streams, each with
-// its own operand tile, tensor-memory columns (M = 128 accumulator, lanes
-// 0-127) and mbarrier, so one group's gathers and epilogues overlap the
-// other's tensor-core work; three CTAs per SM (shared memory and 384 of the
-// 512 tensor-memory columns).
-__global__ void __launch_bounds__(256, 3) k_nrc_infer(Args a) {
+// Inference, step 1: the input rows of the queries, in the operand-tile
+// image (tile t at X + 16 KB * t, row r at tile_off(r, .)).  The hash-grid
+// gathers are latency-bound; this kernel runs at full occupancy so enough of
+// them are in flight, and the MLP kernel then copies finished tiles.
+// `pre(row, r)` may stage per-row data for the MLP kernel's epilogue (the
+// frame form gathers the query path's state here, so the epilogue reads it
+// coalesced).
+struct NoStage {
+    __device__ __forceinline__ void operator()(uint32_t, const QRec&) const {}
+};
+
+template <class Pre>
+__global__ void __launch_bounds__(256, 4) k_nrc_encode(Args a, uint8_t* __restrict__ X, Pre pre) {
+    const uint32_t n = a.count ? min(*a.count, a.n) : a.n;
+    const uint32_t T = 1u << a.grid.log2T;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const QRec r = a.q[row];
+        pre(row, r);
+        uint8_t* tile = X + size_t(row / kRows) * kTileBytes;
+        const uint32_t t = row % kRows;
+        // columns 8j..8j+7 = levels 4j..4j+3, streamed out one 16-byte chunk at a time
+#pragma unroll 1
+        for (uint32_t j = 0; j < 4; j++) {
+            uint32_t pk[4];
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k += 2) {
+                uint32_t idx[2][8], h[2][8];
+                float w[2][8];
+                level_corners(a.grid, 4u * j + k, r.px, r.py, r.pz, idx[0], w[0]);
+                level_corners(a.grid, 4u * j + k + 1u, r.px, r.py, r.pz, idx[1], w[1]);
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+#pragma unroll
+                    for (int c = 0; c < 8; c++) h[e][c] = __ldg(a.table + size_t(4u * j + k + e) * T + idx[e][c]);
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[e][c]));
+                        f0 += w[e][c] * f.x;
+                        f1 += w[e][c] * f.y;
+                    }
+                    pk[k + e] = tc::pack_bf16(f0, f1);
+                }
+            }
+            *reinterpret_cast<uint4*>(tile + tc::tile_off(t, 8u * j)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        *reinterpret_cast<uint4*>(tile + tc::tile_off(t, 32u)) =
+            make_uint4(tc::pack_bf16(r.nx, r.ny), tc::pack_bf16(r.vx, r.vy), tc::pack_bf16(1.0f, 0.0f), 0u);
+        for (uint32_t j = 5; j < 8; j++)
+            *reinterpret_cast<uint4*>(tile + tc::tile_off(t, 8u * j)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+// Output of one inference row: the host-API form stores the prediction.
+struct StoreOut {
+    float4* out;
+    __device__ __forceinline__ void operator()(uint8_t*, uint32_t row, bool valid, const float (&y)[3]) const {
+        if (valid) out[row] = make_float4(y[0], y[1], y[2], 0.0f);
+    }
+};
+
+// Inference, step 2: two warpgroups per CTA run independent tile streams,
+// each with its own operand tile, tensor-memory columns (M = 128
+// accumulator, lanes 0-127) and mbarrier, so one group's tile copy and
+// epilogue overlap the other's tensor-core work; three CTAs per SM (shared
+// memory, and 384 of the 512 tensor-memory columns).  `epi(scratch, row,
+// valid, y)` is called by all 128 threads of a group with the row's
+// prediction; `scratch` is 4 KB of shared memory free during the call.
+template <class Epi>
+__global__ void __launch_bounds__(256, 3) k_nrc_infer(Args a, const uint8_t* __restrict__ X, Epi epi) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t mbar[kInferGroups];
     __shared__ uint32_t tmem_base;
@@ -470,12 +536,11 @@ __global__ void __launch_bounds__(256, 3) k_nrc_infer(Args a) {
          tile += gridDim.x * kInferGroups) {
         const uint32_t row = tile * kRows + t;
         const bool valid = row < n;
-        QRec r{};
-        if (valid) r = a.q[row];
-        {
-            uint32_t x[32];
-            encode_row(a, r, valid, x);
-            store_row(sh, t, x);
+        {   // the tile image, 16 KB contiguous: coalesced 16-byte copies
+            const uint4* src = reinterpret_cast<const uint4*>(X + size_t(tile) * kTileBytes);
+#pragma unroll
+            for (uint32_t j = 0; j < kTileBytes / 16u / 128u; j++)
+                reinterpret_cast<uint4*>(sh)[j * 128u + t] = __ldg(src + j * 128u + t);
         }
         tc::fence_async_smem();
         tc::fence_before();
@@ -522,7 +587,7 @@ __global__ void __launch_bounds__(256, 3) k_nrc_infer(Args a) {
             }
         }
         if (timed_out) break;
-        if (valid) a.out[row] = make_float4(y[0], y[1], y[2], 0.0f);
+        epi(sh, row, valid, y);  // the last layer's operands are consumed: sh is scratch
         tc::fence_before();
         group_sync(g);
     }

@@ -24,8 +24,9 @@ struct ve_nrc {
     // learned-frame buffers: queries (paths terminated at vertex 1) and
     // training samples
     ve::DevBuf<ve::nrc::QRec> fq, fs;
+    ve::DevBuf<float4> fstage;   // per query: the path state its deposit needs (3 x float4)
+    ve::DevBuf<uint8_t> fx, x;   // encoded input tiles (frames, host API)
     ve::DevBuf<ve::nrc::TRec> ftr;
-    ve::DevBuf<float4> fout;
     int grid_infer = 0, grid_train = 0;
     uint64_t trained_steps = 0;
     float last_loss = 0.0f;
@@ -85,7 +86,7 @@ static int launch_train(ve_nrc* m, cudaStream_t st, const QRec* q, const TRec* t
     return VE_OK;
 }
 
-static void launch_infer(ve_nrc* m, cudaStream_t st, const QRec* q, const uint32_t* count, uint32_t n, float4* out) {
+static Args infer_args(ve_nrc* m, const QRec* q, const uint32_t* count, uint32_t n) {
     Args a{};
     a.q = q;
     a.count = count;
@@ -93,9 +94,25 @@ static void launch_infer(ve_nrc* m, cudaStream_t st, const QRec* q, const uint32
     a.table = m->th.p;
     a.wimg = reinterpret_cast<const uint4*>(m->wimg.p);
     a.grid = m->grid;
-    a.out = out;
     a.status = m->status.p;
-    k_nrc_infer<<<m->grid_infer, 128 * kInferGroups, kSmemInfer, st>>>(a);
+    return a;
+}
+
+// Inference over `count` (device) or n rows: encode (+ stage), then the MLP
+// with the epilogue `epi` (X holds n rows rounded up to whole tiles).
+template <class Pre, class Epi>
+static void launch_infer(ve_nrc* m, cudaStream_t st, const Args& a, uint8_t* X, Pre pre, Epi epi) {
+    k_nrc_encode<Pre><<<m->c->num_sms * 8, 256, 0, st>>>(a, X, pre);
+    k_nrc_infer<Epi><<<m->grid_infer, 128 * kInferGroups, kSmemInfer, st>>>(a, X, epi);
+}
+
+template <class Epi>
+static int set_infer_attributes() {
+    if (cudaFuncSetAttribute(k_nrc_infer<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemInfer)) !=
+        cudaSuccess)
+        return VE_ERR_CUDA;
+    cudaFuncSetAttribute(k_nrc_infer<Epi>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return VE_OK;
 }
 
 static void launch_adam(ve_nrc* m, cudaStream_t st) {
@@ -120,13 +137,14 @@ static int zero_grads(ve_nrc* m, cudaStream_t st) {
 // Frame buffers of a learned frame: queries and predictions for every path,
 // the per-frame training sample set.  Returns whether a buffer moved.
 static int prepare_frame(ve_nrc* m, uint64_t paths, bool* moved) {
-    const void* before[] = {m->fq.p, m->fout.p, m->fs.p, m->ftr.p};
+    const void* before[] = {m->fq.p, m->fx.p, m->fstage.p, m->fs.p, m->ftr.p};
     int rc;
-    if ((rc = m->fq.ensure(paths)) || (rc = m->fout.ensure(paths)) || (rc = m->fs.ensure(m->cfg.train_samples)) ||
+    if ((rc = m->fq.ensure(paths)) || (rc = m->fx.ensure(size_t((paths + kRows - 1) / kRows) * kTileBytes)) ||
+        (rc = m->fstage.ensure(3 * paths)) || (rc = m->fs.ensure(m->cfg.train_samples)) ||
         (rc = m->ftr.ensure(m->cfg.train_samples)))
         return rc;
-    const void* after[] = {m->fq.p, m->fout.p, m->fs.p, m->ftr.p};
-    for (int i = 0; i < 4; i++) *moved |= before[i] != after[i];
+    const void* after[] = {m->fq.p, m->fx.p, m->fstage.p, m->fs.p, m->ftr.p};
+    for (int i = 0; i < 5; i++) *moved |= before[i] != after[i];
     return VE_OK;
 }
 
@@ -210,8 +228,7 @@ int ve_nrc_create(ve_ctx* c, const ve_nrc_config* cfg, ve_nrc** out) {
     static_assert(kSmemTrain <= 227u * 1024u, "training tile set exceeds shared memory");
     if (cudaFuncSetAttribute(k_nrc_mlp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemTrain)) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemInfer)) !=
-            cudaSuccess) {
+        set_infer_attributes<StoreOut>() != VE_OK || set_frame_infer_attributes() != VE_OK) {
         ve_nrc_destroy(m);
         return fail(VE_ERR_CUDA, "nrc_create: shared-memory attribute refused");
     }
@@ -221,10 +238,9 @@ int ve_nrc_create(ve_ctx* c, const ve_nrc_config* cfg, ve_nrc** out) {
     // largest carveout) and 512 tensor-memory columns, 128 per CTA; the
     // occupancy query is taken as a floor only, since it assumes the default
     // carveout
-    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaFuncSetAttribute(k_nrc_mlp<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_nrc_infer, 128 * kInferGroups, kSmemInfer) !=
-        cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_nrc_infer<StoreOut>, 128 * kInferGroups,
+                                                      kSmemInfer) != cudaSuccess)
         occ_i = 1;
     int smem_sm = 0;
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
@@ -248,7 +264,9 @@ int ve_nrc_destroy(ve_nrc* m) {
     auto& v = m->c->nrcs;
     v.erase(std::remove(v.begin(), v.end(), m), v.end());
     for (auto* b : {&m->tp, &m->tm, &m->tv, &m->tg}) b->release();
-    m->fout.release();
+    m->fstage.release();
+    m->fx.release();
+    m->x.release();
     m->th.release();
     for (auto* b : {&m->w, &m->wm, &m->wv, &m->wg, &m->loss}) b->release();
     m->val.release();
@@ -330,7 +348,8 @@ int ve_nrc_infer(ve_nrc* m, const ve_nrc_input* in, uint32_t n, float* rgb) {
     int rc;
     if ((rc = nrc::stage_inputs(m, in, nullptr, n)) || (rc = m->out.ensure(n))) return rc;
     cudaStream_t st = m->c->stream;
-    nrc::launch_infer(m, st, m->q.p, nullptr, n, m->out.p);
+    if ((rc = m->x.ensure(size_t((n + nrc::kRows - 1) / nrc::kRows) * nrc::kTileBytes))) return rc;
+    nrc::launch_infer(m, st, nrc::infer_args(m, m->q.p, nullptr, n), m->x.p, nrc::NoStage{}, nrc::StoreOut{m->out.p});
     std::vector<float4> o(n);
     VE_CUDA(cudaMemcpyAsync(o.data(), m->out.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
     VE_CUDA(cudaStreamSynchronize(st));

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/ve.h"
+#include "builder.cuh"
 #include "nrc.cuh"
 #include "raycast.cuh"
 #include "ve_device.cuh"
@@ -133,7 +134,7 @@ struct FrameArgs {
     uint32_t* remaining;   // per view slot: paths not yet deposited (serving), or null
     // learned radiance cache (views with VE_FRAME_LEARNED / _TERMINATE_HASH / _TRAIN)
     nrc::QRec* nq;         // queries: paths ended at their second vertex by the network
-    float4* nq_out;        // network predictions per query
+    float4* nstage;        // per query: {tp, path}, {direct, vid}, {indirect, scene | path-rgb flag}
     nrc::QRec* ns;         // training sample inputs
     nrc::TRec* nt;         // training sample targets
     uint32_t nq_cap, ns_cap;
@@ -800,38 +801,53 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
 }
 
-// Paths the learned cache ended at their second vertex: add throughput x the
-// network's prediction (negative channels read as zero) to the indirect
-// radiance, then deposit like any finished path.
-__global__ void __launch_bounds__(256) k_nrc_apply(FrameArgs a) {
-    __shared__ DepSlot dep[256];
-    const uint32_t n = min(a.counters[CNT_NRC_Q], a.nq_cap);
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const bool valid = i < n;
+// Staging of a learned-cache query in a frame (runs in the encode kernel, at
+// full occupancy): the path state its deposit needs, gathered from the
+// path's random slot into the query's own row.
+struct StagePath {
+    FrameArgs a;
+    __device__ __forceinline__ void operator()(uint32_t row, const nrc::QRec& q) const {
+        const uint32_t p = q.path;
+        const uint4 meta = a.p_meta[p];
+        const DevView& v = a.views[meta.z & 0xFFFFu];
+        const float4 tp = a.p_tp[p], di = a.p_direct[p], in = a.p_indirect[p];
+        const uint32_t sc = v.scene | ((v.flags & VE_FRAME_PATH_RGB) ? 0x80000000u : 0u);
+        a.nstage[3ull * row + 0] = make_float4(tp.x, tp.y, tp.z, __uint_as_float(p));
+        a.nstage[3ull * row + 1] = make_float4(di.x, di.y, di.z, __uint_as_float(meta.x));
+        a.nstage[3ull * row + 2] = make_float4(in.x, in.y, in.z, __uint_as_float(sc));
+    }
+};
+
+// Epilogue of the learned cache's inference in a frame: the query's path
+// gets throughput x prediction (negative channels read as zero) added to its
+// indirect radiance and is deposited like any finished path.  Runs inside
+// k_nrc_infer, on the 128 threads of a warpgroup (warp-aggregated deposits
+// through the group's free operand tile).
+struct ApplyDeposit {
+    FrameArgs a;
+    __device__ __forceinline__ void operator()(uint8_t* scratch, uint32_t row, bool valid, const float (&y)[3]) const {
         float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
         uint32_t dvid = 0, dscene = 0;
         if (valid) {
-            const uint32_t p = a.nq[i].path;
-            const uint4 meta = a.p_meta[p];
-            const DevView& v = a.views[meta.z & 0xFFFFu];
-            const float4 y = a.nq_out[i];
-            const f3 pred = mk(y.x > 0.0f ? y.x : 0.0f, y.y > 0.0f ? y.y : 0.0f, y.z > 0.0f ? y.z : 0.0f);
-            const f3 tp = ld3(a.p_tp[p]);
-            const f3 direct = ld3(a.p_direct[p]);
-            const f3 indirect = add(ld3(a.p_indirect[p]), mul(tp, pred));
-            deposit_value(direct, indirect, dr, dg, db, dl2);
-            dvid = meta.x;
-            dscene = v.scene;
-            if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
+            const float4 s0 = a.nstage[3ull * row + 0], s1 = a.nstage[3ull * row + 1], s2 = a.nstage[3ull * row + 2];
+            const f3 pred = mk(y[0] > 0.0f ? y[0] : 0.0f, y[1] > 0.0f ? y[1] : 0.0f, y[2] > 0.0f ? y[2] : 0.0f);
+            const f3 tp = ld3(s0);
+            const f3 indirect = add(ld3(s2), mul(tp, pred));
+            deposit_value(ld3(s1), indirect, dr, dg, db, dl2);
+            dvid = __float_as_uint(s1.w);
+            const uint32_t sc = __float_as_uint(s2.w);
+            dscene = sc & 0x7FFFFFFFu;
+            if (a.path_rgb && (sc & 0x80000000u)) {
+                const uint32_t p = __float_as_uint(s0.w);
                 a.path_rgb[3ull * p + 0] = dr;
                 a.path_rgb[3ull * p + 1] = dg;
                 a.path_rgb[3ull * p + 2] = db;
             }
         }
-        warp_deposit(valid, dscene, dvid, dr, dg, db, dl2, dep + (threadIdx.x & ~31u), a.scenes, a.stats);
+        DepSlot* dep = reinterpret_cast<DepSlot*>(scratch) + (threadIdx.x & 96u);
+        warp_deposit(valid, dscene, dvid, dr, dg, db, dl2, dep, a.scenes, a.stats);
     }
-}
+};
 
 __device__ __forceinline__ float aces(float x) {  // final.frag:11-18
     const float v = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
@@ -1185,6 +1201,18 @@ struct ve_ctx {
     uint32_t last_launches = 0, last_trace_launches = 0;
 };
 
+namespace ve {
+namespace nrc {
+static int set_frame_infer_attributes() {
+    if (cudaFuncSetAttribute(k_nrc_infer<ApplyDeposit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kSmemInfer)) != cudaSuccess)
+        return VE_ERR_CUDA;
+    cudaFuncSetAttribute(k_nrc_infer<ApplyDeposit>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return VE_OK;
+}
+}  // namespace nrc
+}  // namespace ve
+
 #include "nrc_host.cuh"
 
 namespace ve {
@@ -1227,6 +1255,74 @@ __global__ void k_build_top(const uint32_t* __restrict__ nodes, uint64_t n_words
             base = raw >> 4;
         }
         top[i] = terminal ? ent : ((base << 1) | 1u);
+    }
+}
+
+// Octree::applyEdits upload (octree.cpp:228-314): words[i] -> nodes[slots[i]].
+__global__ void k_scatter_words(uint32_t* __restrict__ nodes, const uint32_t* __restrict__ slots,
+                                const uint32_t* __restrict__ words, uint64_t n) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        nodes[slots[i]] = words[i];
+}
+
+// Slot of the voxel leaf at (x, y, z) when it holds a material, else ~0u:
+// the descent of the DDA (internal words down to level D, leaf word there).
+__device__ __forceinline__ uint32_t leaf_slot(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                              uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t L = 1u << D;
+    uint32_t base = 0;
+    for (uint32_t k = 0; k < D; k++) {
+        const uint32_t raw = dev::fetch_node(nodes, n_words, base + locate(x, y, z, L >> k));
+        if (!(raw & 1u)) return ~0u;
+        base = raw >> 4;
+    }
+    const uint32_t slot = base + locate(x, y, z, 1u);
+    const uint32_t raw = dev::fetch_node(nodes, n_words, slot);
+    return (!(raw & 1u) && ((raw >> 1) & 0x7Fu) != 0u) ? slot : ~0u;
+}
+
+// Targeted refresh after an edit: for every voxel of the 3x3x3 neighbourhood
+// of each edited position, the leaf normal field (the full pass's 26-
+// neighbour gradient of the occupancy, k_leaf_pass) and, when `cache` is
+// given, the radiance-cache entry (sums, weight and count cleared, key kept
+// so probe chains stay intact).  Normal writes keep bits 0-7, the only bits
+// the concurrent occupancy lookups read.
+__global__ void k_refresh(uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, const uint32_t* __restrict__ xyz,
+                          uint64_t n, CacheEntry* cache, uint32_t cache_log2, uint32_t probes) {
+    const int L = int(1u << D);
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n * 27u;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t e = i / 27u;
+        const int o = int(i % 27u);
+        const int x = int(xyz[3 * e]) + o / 9 - 1, y = int(xyz[3 * e + 1]) + (o / 3) % 3 - 1, z = int(xyz[3 * e + 2]) + o % 3 - 1;
+        if (x < 0 || y < 0 || z < 0 || x >= L || y >= L || z >= L) continue;
+        if (cache) {
+            const int c = cache_find(cache, cache_log2, probes, voxel_key(uint32_t(x), uint32_t(y), uint32_t(z)) + 1u);
+            if (c >= 0) {
+                cache[c].count = 0u;
+                cache[c].l2 = 0.0f;
+                cache[c].rgbw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+        }
+        const uint32_t slot = leaf_slot(nodes, n_words, D, uint32_t(x), uint32_t(y), uint32_t(z));
+        if (slot == ~0u) continue;
+        int ax = 0, ay = 0, az = 0;
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dz = -1; dz <= 1; dz++) {
+                    if (dx == 0 && dy == 0 && dz == 0) continue;
+                    const int nx = x + dx, ny = y + dy, nz = z + dz;
+                    bool occd = false;
+                    if (nx >= 0 && ny >= 0 && nz >= 0 && nx < L && ny < L && nz < L)
+                        occd = leaf_slot(nodes, n_words, D, uint32_t(nx), uint32_t(ny), uint32_t(nz)) != ~0u;
+                    if (!occd) {
+                        ax += dx;
+                        ay += dy;
+                        az += dz;
+                    }
+                }
+        const uint32_t lw = nodes[slot];
+        nodes[slot] = (lw & 0xFFu) | encode_normal_field(ax, ay, az);
     }
 }
 
@@ -1517,7 +1613,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     const bool train = nrc && (flags & VE_FRAME_TRAIN);
     if (nrc) {
         a.nq = learned ? nrc->fq.p : nullptr;
-        a.nq_out = nrc->fout.p;
+        a.nstage = nrc->fstage.p;
         a.nq_cap = uint32_t(paths);
         a.ns = train ? nrc->fs.p : nullptr;
         a.nt = nrc->ftr.p;
@@ -1568,8 +1664,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         if (learned || train) {
             if (learned) {
-                nrc::launch_infer(nrc, st, nrc->fq.p, c->counters.p + CNT_NRC_Q, a.nq_cap, nrc->fout.p);
-                k_nrc_apply<<<c->grid_shade, 256, 0, st>>>(a);
+                nrc::launch_infer(nrc, st, nrc::infer_args(nrc, nrc->fq.p, c->counters.p + CNT_NRC_Q, a.nq_cap),
+                                  nrc->fx.p, StagePath{a}, ApplyDeposit{a});
                 launches += 2;
             }
             if (train) {
@@ -1837,6 +1933,226 @@ int ve_ctx_synchronize(ve_ctx* c) {
     return VE_OK;
 }
 
+}  // extern "C"
+
+namespace ve {
+
+// Device scratch of the bulk builder, freed on every exit path.
+struct BuildScratch {
+    std::vector<void*> ptrs;
+    ~BuildScratch() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+};
+
+#define VE_BUILD_ALLOC(ptr, T, n)                                    \
+    T* ptr = scratch.alloc<T>(n);                                   \
+    if (!ptr) return fail(VE_ERR_NOMEM, "scene_build: device allocation failed")
+
+// Node words of OctreeCPU::insert (all voxels) + Octree::set, built on the
+// device (builder.cuh).  `xyzm` is a device array of n (x, y, z, material).
+// On success *words is a cudaMalloc'd array of *n_words words placed 7 words
+// into the allocation (*alloc), like an uploaded scene.
+static int build_scene_words(ve_ctx* c, const uint32_t* xyzm, uint64_t n, uint32_t D, void** alloc,
+                             uint32_t** words, uint64_t* n_words) {
+    using namespace build;
+    cudaStream_t st = c->stream;
+    BuildScratch scratch;
+    const int grid = c->num_sms * 8;
+    auto run_cub = [&](auto&& fn) -> int {  // size query, then the run
+        size_t bytes = 0;
+        if (fn(nullptr, bytes) != cudaSuccess) return fail(VE_ERR_CUDA, "scene_build: cub size query failed");
+        void* tmp = scratch.alloc<uint8_t>(bytes);
+        if (!tmp) return fail(VE_ERR_NOMEM, "scene_build: device allocation failed");
+        if (fn(tmp, bytes) != cudaSuccess) return fail(VE_ERR_CUDA, "scene_build: cub call failed");
+        return VE_OK;
+    };
+    auto empty_scene = [&]() -> int {  // no voxel: OctreeCPU has no root, Octree::set keeps 8 zero words
+        void* a = nullptr;
+        if (cudaMalloc(&a, 16 * 4) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene_build: allocation failed");
+        VE_CUDA(cudaMemsetAsync(a, 0, 16 * 4, st));
+        VE_CUDA(cudaStreamSynchronize(st));
+        *alloc = a;
+        *words = reinterpret_cast<uint32_t*>(a) + 7;
+        *n_words = 8;
+        return VE_OK;
+    };
+    if (n == 0) return empty_scene();
+    int rc;
+    // 1. keys, stable sort, last voxel per position
+    VE_BUILD_ALLOC(keys, uint64_t, n);
+    VE_BUILD_ALLOC(keys_s, uint64_t, n);
+    VE_BUILD_ALLOC(idx, uint32_t, n);
+    VE_BUILD_ALLOC(idx_s, uint32_t, n);
+    VE_BUILD_ALLOC(flag, uint8_t, n);
+    VE_BUILD_ALLOC(nsel, uint64_t, 1);
+    k_keys<<<grid, 256, 0, st>>>(xyzm, n, D, keys, idx);
+    if ((rc = run_cub([&](void* t, size_t& b) {
+             return cub::DeviceRadixSort::SortPairs(t, b, keys, keys_s, idx, idx_s, n, 0, int(3 * D), st);
+         })))
+        return rc;
+    k_last_of_run<<<grid, 256, 0, st>>>(keys_s, n, flag);
+    VE_BUILD_ALLOC(leaf_key, uint64_t, n);
+    VE_BUILD_ALLOC(leaf_idx, uint32_t, n);
+    if ((rc = run_cub([&](void* t, size_t& b) {
+             return cub::DeviceSelect::Flagged(t, b, keys_s, flag, leaf_key, nsel, n, st);
+         })) ||
+        (rc = run_cub([&](void* t, size_t& b) {
+             return cub::DeviceSelect::Flagged(t, b, idx_s, flag, leaf_idx, nsel, n, st);
+         })))
+        return rc;
+    uint64_t nu = 0;
+    VE_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
+    VE_CUDA(cudaStreamSynchronize(st));
+    if (nu == 0) return empty_scene();
+    VE_BUILD_ALLOC(leaf_mat, uint32_t, nu);
+    k_gather_material<<<grid, 256, 0, st>>>(xyzm, leaf_idx, nu, leaf_mat);
+    // 2. internal levels D .. 2 (level l: prefixes of l-1 digits)
+    struct Level {
+        uint64_t* prefix = nullptr;
+        uint32_t* count = nullptr;
+        uint32_t* parent_of = nullptr;  // 1-based index of each node's parent in level l-1 (l >= 3)
+        uint64_t m = 0;
+    };
+    std::vector<Level> lv(D + 2);
+    lv[D + 1].prefix = leaf_key;
+    lv[D + 1].m = nu;
+    for (uint32_t l = D + 1; l >= 3; l--) {
+        const uint64_t m = lv[l].m;
+        VE_BUILD_ALLOC(par, uint64_t, m);
+        VE_BUILD_ALLOC(head, uint32_t, m);
+        VE_BUILD_ALLOC(scan, uint32_t, m);
+        VE_BUILD_ALLOC(uniq, uint64_t, m);
+        VE_BUILD_ALLOC(cnt, uint32_t, m);
+        k_prefix_heads<<<grid, 256, 0, st>>>(lv[l].prefix, m, 3u, par, head);
+        if ((rc = run_cub([&](void* t, size_t& b) {
+                 return cub::DeviceRunLengthEncode::Encode(t, b, par, uniq, cnt, nsel, m, st);
+             })) ||
+            (rc = run_cub([&](void* t, size_t& b) { return cub::DeviceScan::InclusiveSum(t, b, head, scan, m, st); })))
+            return rc;
+        lv[l].parent_of = scan;
+        uint64_t mp = 0;
+        VE_CUDA(cudaMemcpyAsync(&mp, nsel, 8, cudaMemcpyDeviceToHost, st));
+        VE_CUDA(cudaStreamSynchronize(st));
+        lv[l - 1].prefix = uniq;
+        lv[l - 1].count = cnt;
+        lv[l - 1].m = mp;
+    }
+    uint64_t M = 0;
+    std::vector<uint64_t> base(D + 2, 0);
+    for (uint32_t l = 2; l <= D; l++) {
+        base[l] = M;
+        M += lv[l].m;
+    }
+    if (9ull + 8ull * M >= (1ull << 28)) return fail(VE_ERR_CAPACITY, "scene_build: node array exceeds 2^28 words");
+    // 3. blocks: rank of every internal node (levels 2..D) in the stack order
+    VE_BUILD_ALLOC(block, uint32_t, M);
+    if (M) {
+        VE_BUILD_ALLOC(okey, uint64_t, M);
+        VE_BUILD_ALLOC(okey_s, uint64_t, M);
+        VE_BUILD_ALLOC(oval, uint32_t, M);
+        VE_BUILD_ALLOC(oval_s, uint32_t, M);
+        for (uint32_t l = 2; l <= D; l++)
+            k_order_keys<<<grid, 256, 0, st>>>(lv[l].prefix, lv[l].m, l - 1u, uint32_t(base[l]), okey + base[l],
+                                                oval + base[l]);
+        if ((rc = run_cub([&](void* t, size_t& b) {
+                 return cub::DeviceRadixSort::SortPairs(t, b, okey, okey_s, oval, oval_s, M, 0, 64, st);
+             })))
+            return rc;
+        k_scatter_rank<<<grid, 256, 0, st>>>(oval_s, M, block);
+    }
+    // 4. words
+    const uint64_t size = 9ull + 8ull * M;
+    void* a = nullptr;
+    if (cudaMalloc(&a, (size + 8) * 4) != cudaSuccess)
+        return fail(VE_ERR_NOMEM, "scene_build: node array allocation failed");
+    uint32_t* w = reinterpret_cast<uint32_t*>(a) + 7;
+    cudaMemsetAsync(a, 0, (size + 8) * 4, st);
+    k_root_word<<<1, 1, 0, st>>>(uint32_t(lv[2].m), w);
+    for (uint32_t l = 2; l <= D + 1; l++) {
+        const bool leaf = l == D + 1;
+        const uint32_t* pb = l >= 3 ? block + base[l - 1] - 1 : nullptr;  // parent_of is 1-based
+        k_level_words<<<grid, 256, 0, st>>>(lv[l].prefix, lv[l].m, lv[l].parent_of, pb,
+                                             leaf ? nullptr : block + base[l], lv[l].count, leaf ? leaf_mat : nullptr, w);
+    }
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(a);
+        return fail(VE_ERR_CUDA, std::string("scene_build: ") + cudaGetErrorString(e));
+    }
+    *alloc = a;
+    *words = w;
+    *n_words = size;
+    return VE_OK;
+}
+
+}  // namespace ve
+
+extern "C" {
+
+int ve_scene_build(ve_ctx* c, const uint32_t* xyzm, uint64_t n, uint32_t depth, uint32_t flags, int32_t* scene_id,
+                   uint64_t* n_words) {
+    if (!c || (!xyzm && n) || !scene_id) return fail(VE_ERR_INVALID, "scene_build: null argument");
+    if (depth < 1 || depth > 16) return fail(VE_ERR_INVALID, "scene_build: depth must be in [1, 16]");
+    if (n >= (1ull << 32)) return fail(VE_ERR_CAPACITY, "scene_build: at most 2^32 - 1 voxels");
+    const uint64_t L = 1ull << depth;
+    for (uint64_t i = 0; i < n; i++) {
+        if (xyzm[4 * i] >= L || xyzm[4 * i + 1] >= L || xyzm[4 * i + 2] >= L)
+            return fail(VE_ERR_INVALID, "scene_build: voxel outside the 2^depth cube");
+        if (xyzm[4 * i + 3] == 0u || xyzm[4 * i + 3] > 127u)
+            return fail(VE_ERR_INVALID, "scene_build: materials are 1..127");
+    }
+    cudaSetDevice(c->device);
+    uint32_t* d_in = nullptr;
+    if (cudaMalloc(&d_in, std::max<uint64_t>(n, 1) * 16) != cudaSuccess)
+        return fail(VE_ERR_NOMEM, "scene_build: device allocation failed");
+    if (n) VE_CUDA(cudaMemcpyAsync(d_in, xyzm, n * 16, cudaMemcpyHostToDevice, c->stream));
+    SceneSlot s;
+    s.depth = depth;
+    int rc = build_scene_words(c, d_in, n, depth, &s.alloc, &s.nodes, &s.n_words);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(d_in);
+    if (rc) return rc;
+    const size_t cache_bytes = sizeof(CacheEntry) << c->cfg.hash_log2;
+    if (cudaMalloc(&s.cache, cache_bytes) != cudaSuccess) {
+        cudaFree(s.alloc);
+        return fail(VE_ERR_NOMEM, "scene_build: radiance cache allocation failed");
+    }
+    VE_CUDA(cudaMemsetAsync(s.cache, 0, cache_bytes, c->stream));
+    s.live = true;
+    if ((rc = build_top(c, s)) || (!(flags & VE_SCENE_KEEP_NORMALS) && (rc = compute_normals(c, s)))) {
+        cudaFree(s.alloc);
+        cudaFree(s.cache);
+        if (s.top) cudaFree(s.top);
+        return rc;
+    }
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    int32_t id = -1;
+    for (size_t i = 0; i < c->scenes.size(); i++)
+        if (!c->scenes[i].live) {
+            id = int32_t(i);
+            break;
+        }
+    if (id < 0) {
+        id = int32_t(c->scenes.size());
+        c->scenes.push_back(s);
+    } else {
+        c->scenes[id] = s;
+    }
+    c->scenes_dirty = true;
+    c->gen++;
+    *scene_id = id;
+    if (n_words) *n_words = s.n_words;
+    return VE_OK;
+}
+
 int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t depth, uint32_t flags,
                     int32_t* scene_id) {
     if (!c || !words || !scene_id) return fail(VE_ERR_INVALID, "scene_upload: null argument");
@@ -1915,14 +2231,45 @@ int ve_scene_apply_edits(ve_ctx* c, int32_t id, const uint32_t* slots, const uin
     for (uint64_t i = 0; i < n; i++)
         if (slots[i] >= s.n_words) return fail(VE_ERR_CAPACITY, "scene_apply_edits: slot beyond the uploaded array");
     cudaSetDevice(c->device);
-    for (uint64_t i = 0; i < n; i++)
-        VE_CUDA(cudaMemcpyAsync(s.nodes + slots[i], words + i, 4, cudaMemcpyHostToDevice, c->stream));
+    if (n) {  // one copy of the (slot, word) lists, one scatter
+        uint32_t* d = nullptr;
+        if (cudaMalloc(&d, n * 8) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene_apply_edits: allocation failed");
+        cudaMemcpyAsync(d, slots, n * 4, cudaMemcpyHostToDevice, c->stream);
+        cudaMemcpyAsync(d + n, words, n * 4, cudaMemcpyHostToDevice, c->stream);
+        k_scatter_words<<<c->num_sms * 4, 256, 0, c->stream>>>(s.nodes, d, d + n, n);
+        const cudaError_t e = cudaStreamSynchronize(c->stream);
+        cudaFree(d);
+        if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("scene_apply_edits: ") + cudaGetErrorString(e));
+    }
     if (int rc = build_top(c, s)) return rc;
     if (!(flags & VE_SCENE_KEEP_NORMALS)) {
         int rc = compute_normals(c, s);
         if (rc) return rc;
     }
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_scene_refresh(ve_ctx* c, int32_t id, const uint32_t* xyz, uint64_t n, uint32_t flags) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_refresh: unknown scene");
+    if (n && !xyz) return fail(VE_ERR_INVALID, "scene_refresh: null positions");
+    if (n > (1ull << 26)) return fail(VE_ERR_CAPACITY, "scene_refresh: at most 2^26 positions per call");
+    SceneSlot& s = c->scenes[id];
+    const uint32_t L = 1u << s.depth;
+    for (uint64_t i = 0; i < 3 * n; i++)
+        if (xyz[i] >= L) return fail(VE_ERR_INVALID, "scene_refresh: position outside the scene");
+    if (n == 0) return VE_OK;
+    cudaSetDevice(c->device);
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, n * 12) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene_refresh: allocation failed");
+    cudaMemcpyAsync(d, xyz, n * 12, cudaMemcpyHostToDevice, c->stream);
+    k_refresh<<<c->num_sms * 8, 256, 0, c->stream>>>(s.nodes, s.n_words, s.depth, d, n,
+                                                     (flags & VE_REFRESH_KEEP_CACHE) ? nullptr : s.cache,
+                                                     c->cfg.hash_log2, c->cfg.hash_probes);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("scene_refresh: ") + cudaGetErrorString(e));
     return VE_OK;
 }
 
