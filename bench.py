@@ -586,6 +586,65 @@ def run_learned(args, rank, world):
     return 0
 
 
+def run_build(args, rank, world):
+    """GPU bulk octree build (voxel list -> Octree::set words on the device)
+    against the host paths: OctreeCPU.insert + Octree.set (the reference's
+    algorithm, restated) on a bounded depth, and the terrain bulk builder.
+    Seconds per build; the words of every path are compared."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    torch.cuda.set_device(local)
+    W = wl.LARGE
+    r = ve.Renderer(device=local, hash_log2=12)
+    out = {}
+    for depth in (8, W.depth):
+        vox = ve.terrain_voxels(depth, W.variant, W.seed)
+        words, _ = ve.terrain_words(depth, W.variant, W.seed)
+        sid = r.build_scene(vox, depth, keep_normals=True)  # warm-up (module load, first allocations)
+        r.release_scene(sid)
+        ts = []
+        for _ in range(max(args.steps, 3)):
+            t0 = time.perf_counter()
+            sid = r.build_scene(vox, depth, keep_normals=True)
+            ts.append(time.perf_counter() - t0)
+            got = r.download_scene(sid) if not ts[1:] else None
+            r.release_scene(sid)
+            if got is not None:
+                assert np.array_equal(got, words), "GPU build differs from the bulk builder"
+        t0 = time.perf_counter()
+        ve.terrain_words(depth, W.variant, W.seed)
+        t_bulk = time.perf_counter() - t0
+        rec = {"voxels": int(len(vox)), "words": int(words.size), "gpu_build_s": statistics.median(ts),
+               "host_bulk_builder_s": t_bulk}
+        if depth <= 8:
+            t0 = time.perf_counter()
+            cpu = ve.OctreeCPU(depth)
+            cpu.insert_many(vox)
+            tree = ve.Octree(depth)
+            tree.set(cpu)
+            rec["host_octree_cpu_set_s"] = time.perf_counter() - t0
+            assert np.array_equal(tree.words()[: tree.size], words)
+        out[f"depth{depth}"] = rec
+    r.close()
+    big = out[f"depth{W.depth}"]
+    line = {"metric": "GPU octree build, Mvoxels/s (voxel list -> Octree::set words)",
+            "value": big["voxels"] / big["gpu_build_s"] / 1e6, "unit": "Mvoxels/s", "n_gpus": 1,
+            "steps": max(args.steps, 3), "warmup": 1, "ms_per_step": 1e3 * big["gpu_build_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded terrain voxel lists)",
+            "config": {"workload": "build: depth-8 and depth-10 terrain + overhangs, host voxel list in, "
+                                   "device words out (host copy of the list included)"},
+            "builds": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -594,7 +653,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "build"], default="large")
     ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
     ap.add_argument("--eq-frames", type=int, default=4, help="learned: plain frames setting the time budget")
     ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
@@ -620,6 +679,8 @@ def main():
         return run_serving(args, rank, world)
     if args.workload == "learned":
         return run_learned(args, rank, world)
+    if args.workload == "build":
+        return run_build(args, rank, world)
 
     import torch
 

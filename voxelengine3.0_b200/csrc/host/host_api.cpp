@@ -161,7 +161,7 @@ int ve_words_free(ve_words* w) {
     return VE_OK;
 }
 int ve_terrain_voxels(uint32_t depth, uint32_t variant, uint64_t seed, uint32_t* xyzm, uint64_t cap, uint64_t* n) {
-    if (depth < 1 || depth > 9) return hfail(VE_ERR_INVALID, "terrain_voxels: depth must be in [1, 9]");
+    if (depth < 1 || depth > 10) return hfail(VE_ERR_INVALID, "terrain_voxels: depth must be in [1, 10]");
     std::vector<uint32_t> v = ve::terrain_voxels(ve::TerrainParams{depth, variant, seed});
     if (n) *n = v.size() / 4;
     if (xyzm) std::memcpy(xyzm, v.data(), std::min<uint64_t>(cap, v.size() / 4) * 16);

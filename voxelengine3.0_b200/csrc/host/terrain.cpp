@@ -140,9 +140,14 @@ uint32_t TerrainField::material(uint32_t x, uint32_t y, uint32_t z) const {
 std::vector<uint32_t> terrain_voxels(const TerrainParams& p) {
     TerrainField f(p);
     const uint32_t L = f.length();
+    // no voxel is solid at or above the highest column top plus the band
+    double top = 0.0;
+    for (uint32_t z = 0; z < L; z++)
+        for (uint32_t x = 0; x < L; x++) top = std::max(top, double(f.height(x, z)));
+    const uint32_t ymax = uint32_t(std::min<double>(L, std::max(0.0, std::ceil(top + f.band())) + 1.0));
     std::vector<uint32_t> out;
     for (uint32_t x = 0; x < L; x++)
-        for (uint32_t y = 0; y < L; y++)
+        for (uint32_t y = 0; y < ymax; y++)
             for (uint32_t z = 0; z < L; z++)
                 if (f.solid(x, y, z)) {
                     out.push_back(x);
