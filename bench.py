@@ -477,75 +477,57 @@ def run_serving(args, rank, world):
     return 0
 
 
-def run_learned(args, rank, world):
-    """rMSE at equal time against a 64-spp plain render (16 frames x 4 spp,
-    fresh cache, decay 1) on the depth-10 scene at 1080p, fixed camera:
-    the plain method, the hashed per-voxel cache ending paths at their second
-    vertex, and the learned cache (trained online on 2^16 samples per frame
-    over `--train-frames` plain frames, then ending paths at their second
-    vertex, falling back to the hashed cache per cell).  Each method renders
-    4-spp frames from a fresh radiance cache until its device time reaches
-    that of the plain method's `--eq-frames` frames."""
-    import torch
+class _EqualTime:
+    """Image quality at equal device time on the depth-10 scene at 1080p,
+    fixed camera: the reference image is a 64-spp plain render (16 frames x
+    4 spp through the per-voxel cache, decay 1); each method renders frames
+    from a fresh radiance cache until its device time (CUDA events inside the
+    library, host copies excluded) reaches the budget, and its last image is
+    scored by the relative MSE (img - ref)^2 / (ref^2 + 0.01) over hit pixels."""
 
-    import ve_b200.dist as vd
-    import ve_b200.workloads as wl
+    STATS = ("nrc_queries", "nrc_hash_terminated", "paths", "ms_learned", "ms_trace", "ms_shade", "ms_primary",
+             "rays_bounce", "rays_shadow", "scheduled_voxels", "scheduled_paths")
 
-    ve = load_package()
-    rank, world, local = vd.env_rank()
-    dist = vd.init("nccl", timeout_s=600.0, device=local)
-    torch.cuda.set_device(local)
-    W = wl.LARGE
-    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
-    r = ve.Renderer(device=local, hash_log2=W.hash_log2)
-    r.set_materials(ve.terrain_materials(W.seed))
-    sid = r.upload_scene(words, W.depth)
-    eye, d = wl.orbit_camera(0, W.frames, W.seed)
-    cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
-    stream = torch.cuda.ExternalStream(r.stream, device=local)
+    def __init__(self, ve, wl, local):
+        W = self.W = wl.LARGE
+        self.ve = ve
+        words, _ = ve.terrain_words(W.depth, W.variant, W.seed)
+        r = self.r = ve.Renderer(device=local, hash_log2=W.hash_log2)
+        r.set_materials(ve.terrain_materials(W.seed))
+        self.sid = r.upload_scene(words, W.depth)
+        eye, d = wl.orbit_camera(0, W.frames, W.seed)
+        self.cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+        r.cache_reset(self.sid)
+        for k in range(15):
+            r.render(self.sid, self.cam, self.fc(90000 + k, 4), outputs=())
+        ref = r.render(self.sid, self.cam, self.fc(90015, 4), outputs=("voxel_id", "rgb"))
+        self.mask = ref["voxel_id"] != 0
+        self.refrgb = ref["rgb"]
 
-    def fc(frame, spp, flags=0):
-        return ve.FrameConfig(width=W.width, height=W.height, spp=spp, bounces=W.bounces, frame_index=frame,
-                              primary_controlchecks=W.primary_controlchecks,
-                              bounce_controlchecks=W.bounce_controlchecks, decay=1.0, flags=flags)
+    def fc(self, frame, spp, flags=0, **kw):
+        W = self.W
+        return self.ve.FrameConfig(width=W.width, height=W.height, spp=spp, bounces=W.bounces, frame_index=frame,
+                                   primary_controlchecks=W.primary_controlchecks,
+                                   bounce_controlchecks=W.bounce_controlchecks, decay=1.0, flags=flags, **kw)
 
-    def timed(frame, spp, flags, outputs=()):
-        """One frame; device time of its kernels (CUDA events inside the
-        library), host copies of the outputs excluded."""
-        out = r.render(sid, cam, fc(frame, spp, flags | ve.FRAME_TIMING), outputs=outputs)
-        return out, r.stats()["ms_total"]
+    def timed(self, frame, spp, flags, outputs=(), **kw):
+        out = self.r.render(self.sid, self.cam, self.fc(frame, spp, flags | self.ve.FRAME_TIMING, **kw),
+                            outputs=outputs)
+        return out, self.r.stats()["ms_total"]
 
-    # reference: 64 spp through the per-voxel cache
-    r.cache_reset(sid)
-    for k in range(15):
-        r.render(sid, cam, fc(90000 + k, 4), outputs=())
-    ref = r.render(sid, cam, fc(90015, 4), outputs=("voxel_id", "rgb"))
-    mask = ref["voxel_id"] != 0
-    refrgb = ref["rgb"]
+    def rmse(self, img):
+        e = (img - self.refrgb) ** 2 / (self.refrgb ** 2 + 0.01)
+        return float(e[self.mask].mean())
 
-    def rmse(img):
-        e = (img - refrgb) ** 2 / (refrgb ** 2 + 0.01)
-        return float(e[mask].mean())
-
-    # online training of the learned cache on plain frames
-    m = ve.LearnedCache(r, log2_table=19, train_samples=65536, seed=1)
-    m.attach(sid)
-    train_ms = 0.0
-    losses = []
-    for f in range(args.train_frames):
-        _, ms = timed(1000 + f, W.spp, ve.FRAME_TRAIN)
-        train_ms += ms
-        losses.append(m.stats()["loss"])
-
-    def run_method(flags, budget_ms, max_frames):
-        r.cache_reset(sid)
+    def run(self, flags, budget_ms, max_frames, **kw):
+        r = self.r
+        r.cache_reset(self.sid)
         t = 0.0
         n = 0
         img = None
-        stats = {"nrc_queries": 0, "nrc_hash_terminated": 0, "paths": 0, "ms_learned": 0.0, "ms_trace": 0.0,
-                 "ms_shade": 0.0, "ms_primary": 0.0, "rays_bounce": 0, "rays_shadow": 0}
+        stats = {k: 0 for k in self.STATS}
         while n < max_frames:
-            out, ms = timed(20000 + n, W.spp, flags, outputs=("rgb",))
+            out, ms = self.timed(20000 + n, self.W.spp, flags, outputs=("rgb",), **kw)
             if budget_ms is not None and n > 0 and t + ms > budget_ms * 1.0001:
                 break
             t += ms
@@ -556,14 +538,43 @@ def run_learned(args, rank, world):
                 stats[k] += st[k]
             if budget_ms is None and n >= max_frames:
                 break
-        return {"rmse": rmse(img), "frames": n, "ms": t, "spp": n * W.spp, **stats}
+        return {"rmse": self.rmse(img), "frames": n, "ms": t, "spp": n * self.W.spp, **stats}
 
-    plain = run_method(0, None, args.eq_frames)
+
+def run_learned(args, rank, world):
+    """rMSE at equal time against a 64-spp plain render: the plain method,
+    the hashed per-voxel cache ending paths at their second vertex, and the
+    learned cache (trained online on 2^16 samples per frame over
+    `--train-frames` plain frames, then ending paths at their second vertex,
+    falling back to the hashed cache per cell).  The budget is the plain
+    method's `--eq-frames` frames."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=600.0, device=local)
+    torch.cuda.set_device(local)
+    H = _EqualTime(ve, wl, local)
+    W, r = H.W, H.r
+
+    # online training of the learned cache on plain frames
+    m = ve.LearnedCache(r, log2_table=19, train_samples=65536, seed=1)
+    m.attach(H.sid)
+    train_ms = 0.0
+    losses = []
+    for f in range(args.train_frames):
+        _, ms = H.timed(1000 + f, W.spp, ve.FRAME_TRAIN)
+        train_ms += ms
+        losses.append(m.stats()["loss"])
+
+    plain = H.run(0, None, args.eq_frames)
     budget = plain["ms"]
-    stream.synchronize()
-    hashed = run_method(ve.FRAME_TERMINATE_HASH, budget, 64)
-    learned_frozen = run_method(ve.FRAME_LEARNED, budget, 64)
-    learned = run_method(ve.FRAME_LEARNED | ve.FRAME_TRAIN, budget, 64)
+    hashed = H.run(ve.FRAME_TERMINATE_HASH, budget, 64)
+    learned_frozen = H.run(ve.FRAME_LEARNED, budget, 64)
+    learned = H.run(ve.FRAME_LEARNED | ve.FRAME_TRAIN, budget, 64)
     line = {"metric": "rMSE at equal time vs 64-spp plain render (learned cache)", "value": learned["rmse"],
             "unit": "relative MSE", "n_gpus": world, "steps": learned["frames"], "warmup": args.train_frames,
             "ms_per_step": learned["ms"] / max(learned["frames"], 1), "higher_is_better": False,
@@ -582,6 +593,47 @@ def run_learned(args, rank, world):
         print(json.dumps(line), flush=True)
     m.close()
     r.close()
+    vd.shutdown(dist)
+    return 0
+
+
+def run_scheduled(args, rank, world):
+    """Importance-aware voxel scheduling (rank/threshold/emit) against the
+    plain per-pixel method at equal device time: rMSE against the 64-spp
+    plain render, frames and paths per frame, for the default weights
+    (pixels 0.1, variance 0.9, top 30 %, middle 40 %) at two shading budgets
+    (131072, the reference's default, and 2 x pixels)."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=600.0, device=local)
+    torch.cuda.set_device(local)
+    H = _EqualTime(ve, wl, local)
+    W = H.W
+    plain = H.run(0, None, args.eq_frames)
+    budget = plain["ms"]
+    out = {}
+    for name, sb in (("budget_131072", 131072), ("budget_2x_pixels", 2 * W.width * W.height)):
+        res = H.run(ve.FRAME_SCHEDULED, budget, 4096, shading_budget=sb)
+        res["ms_per_frame"] = res["ms"] / max(res["frames"], 1)
+        res["paths_per_frame"] = res["paths"] / max(res["frames"], 1)
+        out[name] = res
+    best = min(out.values(), key=lambda x: x["rmse"])
+    line = {"metric": "rMSE at equal time vs 64-spp plain render (importance scheduling)", "value": best["rmse"],
+            "unit": "relative MSE", "n_gpus": world, "steps": best["frames"], "warmup": 0,
+            "ms_per_step": best["ms_per_frame"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain, fixed orbit camera)",
+            "config": {"workload": "scheduled: depth-10 terrain 1920x1080, 3 bounces, 64-spp reference, "
+                                   "equal device time with the plain method's frames",
+                       "plain_frames": args.eq_frames, "budget_ms": budget},
+            "plain": plain, **out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    H.r.close()
     vd.shutdown(dist)
     return 0
 
@@ -653,9 +705,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "build"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "build"], default="large")
     ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
-    ap.add_argument("--eq-frames", type=int, default=4, help="learned: plain frames setting the time budget")
+    ap.add_argument("--eq-frames", type=int, default=4, help="learned, scheduled: plain frames setting the time budget")
     ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
     ap.add_argument("--capacity-requests", type=int, default=400, help="serving: closed-loop capacity sample")
     ap.add_argument("--serial-requests", type=int, default=400, help="serving: serial plain comparison sample")
@@ -679,6 +731,8 @@ def main():
         return run_serving(args, rank, world)
     if args.workload == "learned":
         return run_learned(args, rank, world)
+    if args.workload == "scheduled":
+        return run_scheduled(args, rank, world)
     if args.workload == "build":
         return run_build(args, rank, world)
 

@@ -46,6 +46,8 @@ extern "C" {
 #define VE_FRAME_LEARNED 8u       /* end paths at their second vertex with the scene's learned cache */
 #define VE_FRAME_TERMINATE_HASH 16u /* end paths at their second vertex with the hashed per-voxel cache */
 #define VE_FRAME_TRAIN 32u        /* record training samples and train the scene's learned cache */
+#define VE_FRAME_SCHEDULED 64u    /* importance-aware voxel scheduling (schedule/rank/threshold.comp)
+                                     in place of spp paths per pixel; single-view calls */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
                                      replaying a CUDA graph of the frame's kernel sequence */
 
@@ -74,8 +76,16 @@ typedef struct ve_frame_config {
     float sun_intensity;
     float sky[3];                   /* constant sky radiance */
     float decay;                    /* temporal decay of the cache per frame */
-    float variance_norm;            /* core.hpp:109 (VARIANCE view scale) */
+    float variance_norm;            /* core.hpp:109 (VARIANCE view and rank.comp variance scale) */
     uint32_t flags;                 /* VE_FRAME_* */
+    /* importance-aware scheduling (VE_FRAME_SCHEDULED), core.hpp:95-112 */
+    float weight_pixels;            /* 0.1 */
+    float weight_variance;          /* 0.9 */
+    float pixels_norm;              /* 100 */
+    float top_fraction;             /* 0.30: voxels given 2 paths */
+    float mid_fraction;             /* 0.40: voxels given 1 path */
+    uint32_t min_samples;           /* 1: paths of the remaining voxels */
+    uint32_t shading_budget;        /* 131072: cap on paths per frame */
 } ve_frame_config;
 
 /* One render request: scene, Camera::UBO (camera.hpp:24-29: position,
@@ -97,7 +107,9 @@ typedef struct ve_frame_outputs {
     float* rgb;         /* 3 x f32 per pixel */
     float* mapped;      /* 3 x f32 per pixel */
     float* path_rgb;    /* 3 x f32 per path (pixel * spp + sample); VE_FRAME_PATH_RGB;
-                           zero for pixels without a primary hit (no path) */
+                           zero for pixels without a primary hit (no path).  With
+                           VE_FRAME_SCHEDULED: one per shade-list entry, room for
+                           min(shading_budget, 2 * width * height) paths */
 } ve_frame_outputs;
 
 /* FrameStats (src/renderer/core.hpp:164-185) and the profiler's stage
@@ -117,6 +129,8 @@ typedef struct ve_frame_stats {
     uint64_t nrc_queries;         /* paths ended by the learned cache */
     uint64_t nrc_hash_terminated; /* paths ended by the hashed per-voxel cache */
     uint64_t nrc_samples;         /* training samples recorded */
+    uint64_t scheduled_voxels;    /* VE_FRAME_SCHEDULED: distinct visible voxels */
+    uint64_t scheduled_paths;     /* VE_FRAME_SCHEDULED: shade-list entries (paths) */
     float ms_learned;             /* learned-cache inference + training (VE_FRAME_TIMING) */
     uint32_t reserved;
 } ve_frame_stats;
@@ -215,6 +229,18 @@ int ve_scene_refresh(ve_ctx* ctx, int32_t scene_id, const uint32_t* xyz, uint64_
 int ve_scene_apply_edits(ve_ctx* ctx, int32_t scene_id, const uint32_t* slots, const uint32_t* words, uint64_t n,
                          uint32_t flags);
 int ve_scene_download(ve_ctx* ctx, int32_t scene_id, uint32_t* out, uint64_t cap, uint64_t* n_words);
+
+/* A batch of independent rays through the device DDA that the frame kernels
+ * run (Raycast / RaycastCounted, src/shd/internal.glsl:297-400; the GPU
+ * counterpart of OctreeCPU::raycast, src/octree_cpu.cpp:128-215, for
+ * picking and for checking the traversal ray by ray).  origins, dirs: 3 f32
+ * per ray, host memory; out: 8 u32 per ray {status (0 hit, 1 left the
+ * volume, 2 out of controlchecks), hit node slot, material, x, y, z, node
+ * size, checks}.  flags: VE_RAYCAST_FULL_WALK descends every octree level
+ * per step instead of starting from the scene's top table.  Synchronous. */
+#define VE_RAYCAST_FULL_WALK 1u
+int ve_raycast_batch(ve_ctx* ctx, int32_t scene_id, const float* origins, const float* dirs, uint64_t n,
+                     uint32_t controlchecks, uint32_t flags, uint32_t* out);
 /* device bytes held by a scene (node array + radiance cache) */
 int ve_scene_footprint(ve_ctx* ctx, int32_t scene_id, uint64_t* bytes);
 

@@ -30,12 +30,16 @@ class FrameParams(ctypes.Structure):
                 ("primary_controlchecks", _U32), ("bounce_controlchecks", _U32),
                 ("reconstruction_radius", _U32), ("render_type", _U32), ("frame_index", _U32),
                 ("sun_dir", ctypes.c_float * 3), ("sun_intensity", ctypes.c_float), ("sky", ctypes.c_float * 3),
-                ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", _U32)]
+                ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", _U32),
+                ("weight_pixels", ctypes.c_float), ("weight_variance", ctypes.c_float),
+                ("pixels_norm", ctypes.c_float), ("top_fraction", ctypes.c_float), ("mid_fraction", ctypes.c_float),
+                ("min_samples", _U32), ("shading_budget", _U32)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("rays_primary", _U64), ("rays_bounce", _U64), ("rays_shadow", _U64), ("fetch_restart", _U64),
-                ("fetch_min", _U64), ("paths", _U64), ("deposits", _U64), ("steps", _U64)]
+                ("fetch_min", _U64), ("paths", _U64), ("deposits", _U64), ("steps", _U64),
+                ("scheduled_voxels", _U64), ("scheduled_paths", _U64)]
 
 
 def build_oracle(force: bool = False) -> str:
@@ -70,6 +74,8 @@ class Oracle:
                                         _np(np.float32)]
         L.oracle_raycast.argtypes = [_np(np.uint32), _U64, _U32, _np(np.float32), _np(np.float32), _U32,
                                      _np(np.uint32), _P]
+        L.oracle_raycast_batch.argtypes = [_np(np.uint32), _U64, _U32, _np(np.float32), _np(np.float32), _U64, _U32,
+                                           _U32, _np(np.uint32)]
         L.oracle_voxel_key.restype = _U32
         L.oracle_voxel_key.argtypes = [_U32, _U32, _U32]
         L.oracle_rand_seq.restype = _U32
@@ -119,6 +125,16 @@ class Oracle:
                                 ctypes.cast(cnt, _P))
         return out, (cnt[0], cnt[1])
 
+    def raycast_batch(self, words, depth, origins, dirs, controlchecks, threads=8):
+        """(n, 8) u32 rows {status, id, material, x, y, z, size, checks}."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        w = np.ascontiguousarray(words, np.uint32)
+        out = np.zeros((o.shape[0], 8), np.uint32)
+        self.lib.oracle_raycast_batch(w, w.size, depth, o.reshape(-1), d.reshape(-1), o.shape[0], controlchecks,
+                                      threads, out.reshape(-1))
+        return out
+
     def voxel_key(self, x, y, z) -> int:
         return self.lib.oracle_voxel_key(x, y, z)
 
@@ -158,7 +174,8 @@ class OracleRenderer:
         gbuf = np.zeros((H, W, 4), np.uint32)
         rgb = np.zeros((H, W, 3), np.float32) if want_rgb else None
         mapped = np.zeros((H, W, 3), np.float32) if want_rgb else None
-        path_rgb = np.zeros((W * H * params.spp, 3), np.float32) if want_path_rgb else None
+        n_paths = min(params.shading_budget, 2 * W * H) if params.flags & 64 else W * H * params.spp
+        path_rgb = np.zeros((n_paths, 3), np.float32) if want_path_rgb else None
         st = Stats()
         r0, r1 = rows if rows else (0, 0)
         w = np.ascontiguousarray(words, np.uint32)
@@ -280,4 +297,13 @@ def frame_params(fc) -> FrameParams:
     p.sun_intensity = float(fc.sun_intensity)
     p.decay = float(fc.decay)
     p.variance_norm = float(fc.variance_norm)
+    for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction"):
+        setattr(p, f, float(getattr(fc, f, FrameParams_defaults[f])))
+    for f in ("min_samples", "shading_budget"):
+        setattr(p, f, int(getattr(fc, f, FrameParams_defaults[f])))
     return p
+
+
+# core.hpp:95-112 scheduling defaults, for frame configs without those fields
+FrameParams_defaults = {"weight_pixels": 0.1, "weight_variance": 0.9, "pixels_norm": 100.0, "top_fraction": 0.30,
+                        "mid_fraction": 0.40, "min_samples": 1, "shading_budget": 131072}

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <stack>
@@ -529,11 +530,11 @@ struct PathOut {
 // next-event estimate in the place of the emissive NEE (shade.comp:631-836 is
 // dormant in scenes without emissive voxels).
 void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_frame_params& P,
-                const Hit& primary, f3 primary_dir, uint32_t pix_index, uint32_t sample, PathOut* out,
+                const Hit& primary, f3 primary_dir, uint32_t pix_index, uint32_t list_idx, PathOut* out,
                 ov_stats* st, RayCounters* rc) {
     const uint32_t max_bounces = P.bounces + 1u;  // MAX_BOUNCES (wavefront.glsl:23)
-    const uint32_t list_idx = pix_index * P.spp + sample;
-    // emit.comp:171-174
+    // emit.comp:171-174; list_idx is pixel * spp + sample in the per-pixel
+    // method and the shade-list index in the scheduled one
     const uint32_t sample_idx = P.frame_index + pix_index * 2654435761u + list_idx * 1442695040u;
     uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
     f3 tp = mk(1, 1, 1);
@@ -653,9 +654,132 @@ inline double aces(double x) {  // final.frag:11-18
     return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
 }
 
+// Scheduling thresholds carried from frame to frame (threshold.comp's
+// output, read by the next frame's rank.comp): +inf / -inf before the first
+// scheduled frame, which puts every voxel in the middle tier.
 struct Renderer {
     Cache cache;
+    float t_high = std::numeric_limits<float>::infinity();
+    float t_mid = -std::numeric_limits<float>::infinity();
 };
+
+constexpr uint32_t kRankBins = 256;
+constexpr uint32_t kFrameScheduled = 64;  // VE_FRAME_SCHEDULED
+
+inline f3 pixel_dir(const float cam[16], uint32_t px, uint32_t py, uint32_t W, uint32_t H) {
+    // generate_primary.comp:44-52
+    const f3 plane = mk(cam[4], cam[5], cam[6]);
+    const f3 right = mk(cam[8], cam[9], cam[10]);
+    const f3 up = mk(cam[12], cam[13], cam[14]);
+    const float ndx = (float(px) + 0.5f) / float(W) * 2.0f - 1.0f;
+    const float ndy = (float(py) + 0.5f) / float(H) * 2.0f - 1.0f;
+    return normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
+}
+
+// One scheduled frame's paths (schedule.comp, rank.comp, threshold.comp,
+// emit.comp), written as sequential loops over pixels:
+//   schedule  every hit pixel claims its voxel; the voxel keeps its pixel
+//             count and its smallest pixel index (the representative)
+//   rank      importance = w_pix * clamp(pixels / pixels_norm)
+//                        + w_var * clamp(var * 255^2 / variance_norm)
+//             (var: the cache's luminance variance, 0 below two samples);
+//             2 paths at or above t_high, 1 at or above t_mid, else
+//             min_samples; a 256-bin histogram of the importances
+//   list      entries {vid, pixel} in representative-pixel order, cut at
+//             min(shading_budget, 2 * pixels)
+//   threshold the next frame's t_high / t_mid: the bins where the reverse
+//             cumulative count reaches top_fraction and top + mid fractions
+//   emit      one path per entry from the representative pixel's primary
+//             hit, the entry index seeding the path.
+// The device implementation follows the same deterministic order (smallest
+// pixel as the representative, list ordered by pixel); the reference keeps
+// the first pixel to claim and appends with atomics.
+void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t n_mats, const float cam[16],
+                    const ov_frame_params* P, uint32_t threads, const std::vector<Hit>& hits,
+                    const std::vector<uint32_t>& vids, float* path_rgb,
+                    std::vector<std::vector<std::vector<Deposit>>>& deps, std::vector<ov_stats>& tstats,
+                    std::vector<RayCounters>& trc) {
+    const uint32_t W = P->width, H = P->height, npix = W * H;
+    struct Claim { uint32_t pix, count; };
+    std::unordered_map<uint32_t, Claim> claims;
+    for (uint32_t pix = 0; pix < npix; pix++) {
+        const uint32_t vid = vids[pix];
+        if (!vid) continue;
+        auto it = claims.find(vid);
+        if (it == claims.end()) claims.emplace(vid, Claim{pix, 1u});
+        else it->second.count++;
+    }
+    std::vector<uint32_t> hist(kRankBins, 0u);
+    std::vector<std::pair<uint32_t, uint32_t>> list;  // {vid, pixel}
+    const uint64_t cap = std::min<uint64_t>(P->shading_budget, 2ull * npix);
+    uint64_t nvox = 0;
+    for (uint32_t pix = 0; pix < npix; pix++) {
+        const uint32_t vid = vids[pix];
+        if (!vid) continue;
+        const Claim& cl = claims[vid];
+        if (cl.pix != pix) continue;
+        nvox++;
+        const Avg a = lookup_avg(R->cache, vid);
+        const float var = a.count >= 2u ? float(a.var) : 0.0f;
+        const float pn = gclamp(float(cl.count) / gmax(P->pixels_norm, 1.0f), 0.0f, 1.0f);
+        const float vn = gclamp(var * (255.0f * 255.0f) / gmax(P->variance_norm, 1.0f), 0.0f, 1.0f);
+        const float imp = P->weight_pixels * pn + P->weight_variance * vn;
+        const uint32_t n = imp >= R->t_high ? 2u : (imp >= R->t_mid ? 1u : P->min_samples);
+        uint32_t bin = uint32_t(imp * float(kRankBins));
+        if (bin >= kRankBins) bin = kRankBins - 1u;
+        hist[bin]++;
+        for (uint32_t j = 0; j < n && list.size() < cap; j++) list.emplace_back(vid, pix);
+    }
+    // threshold.comp
+    uint32_t total = 0;
+    for (uint32_t b = 0; b < kRankBins; b++) total += hist[b];
+    if (total == 0u) {
+        R->t_high = std::numeric_limits<float>::infinity();
+        R->t_mid = -std::numeric_limits<float>::infinity();
+    } else {
+        const float top = gclamp(P->top_fraction, 0.0f, 1.0f);
+        const float mid = gclamp(P->mid_fraction, 0.0f, 1.0f - top);
+        const uint32_t top_n = uint32_t(top * float(total)), topmid_n = uint32_t((top + mid) * float(total));
+        uint32_t cum = 0, hb = kRankBins, mb = kRankBins;
+        for (int b = int(kRankBins) - 1; b >= 0; b--) {
+            cum += hist[b];
+            if (hb == kRankBins && cum >= top_n) hb = uint32_t(b);
+            if (mb == kRankBins && cum >= topmid_n) mb = uint32_t(b);
+        }
+        if (hb == kRankBins) hb = kRankBins - 1u;
+        if (mb == kRankBins) mb = kRankBins - 1u;
+        R->t_high = float(hb) / float(kRankBins);
+        R->t_mid = float(mb) / float(kRankBins);
+    }
+    tstats[0].scheduled_voxels += nvox;
+    tstats[0].scheduled_paths += list.size();
+    // emit + bounce loop, entries interleaved over threads
+    auto work = [&](uint32_t t) {
+        ov_stats& st = tstats[t];
+        for (size_t i = t; i < list.size(); i += threads) {
+            const uint32_t vid = list[i].first, pix = list[i].second;
+            const f3 dir = pixel_dir(cam, pix % W, pix / W, W, H);
+            PathOut po;
+            trace_path(s, mats, n_mats, *P, hits[pix], dir, pix, uint32_t(i), &po, &st, &trc[t]);
+            st.paths++;
+            Deposit dp;
+            dp.vid = vid;
+            deposit_value(po, dp.rgb);
+            if (path_rgb) {
+                float* o = path_rgb + 3 * uint64_t(i);
+                o[0] = dp.rgb[0]; o[1] = dp.rgb[1]; o[2] = dp.rgb[2];
+            }
+            deps[t][shard_of(vid)].push_back(dp);
+        }
+    };
+    if (threads == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < threads; t++) th.emplace_back(work, t);
+        for (auto& x : th) x.join();
+    }
+}
 
 }  // namespace
 
@@ -789,6 +913,28 @@ void oracle_raycast(const uint32_t* words, uint64_t n, uint32_t depth, const flo
     if (fetch) { fetch[0] += rc.fetch_restart; fetch[1] += rc.fetch_min; }
 }
 
+// oracle_raycast over n rays (3 f32 origin / direction per ray, 8 u32 out
+// per ray), rays split across `threads` std::threads.
+void oracle_raycast_batch(const uint32_t* words, uint64_t n_words, uint32_t depth, const float* o, const float* d,
+                          uint64_t n, uint32_t controlchecks, uint32_t threads, uint32_t* out) {
+    Scene s{words, n_words, depth};
+    if (threads == 0) threads = 1;
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < threads; t++)
+        th.emplace_back([&, t] {
+            RayCounters rc;
+            for (uint64_t i = t; i < n; i += threads) {
+                const Hit h = raycast(s, mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]), mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]),
+                                      controlchecks, &rc);
+                uint32_t* w = out + 8 * i;
+                w[0] = uint32_t(h.status); w[1] = h.id; w[2] = h.material;
+                w[3] = h.pos[0]; w[4] = h.pos[1]; w[5] = h.pos[2];
+                w[6] = h.size; w[7] = h.checks;
+            }
+        });
+    for (auto& x : th) x.join();
+}
+
 uint32_t oracle_voxel_key(uint32_t x, uint32_t y, uint32_t z) {
     const uint32_t p[3] = {x, y, z};
     return voxel_key(p);
@@ -859,6 +1005,10 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     if (row_end == 0 || row_end > H) row_end = H;
     if (row_begin > row_end) row_begin = row_end;
     if (threads == 0) threads = 1;
+    const bool sched = (P->flags & kFrameScheduled) != 0;
+    if (sched && (row_begin != 0 || row_end != H)) return -1;  // the schedule spans the whole view
+    std::vector<Hit> hits(sched ? size_t(W) * H : 0);
+    std::vector<uint32_t> vids(sched ? size_t(W) * H : 0, 0u);
 
     // temporal decay of the cache before this frame's deposits
     run_parallel(kShards, threads, [&](uint32_t sh) {
@@ -901,10 +1051,15 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                     gbuf[4 * uint64_t(pix) + 2] = h.status == ST_HIT ? h.id : 0u;
                     gbuf[4 * uint64_t(pix) + 3] = vid;
                 }
+                if (sched) {
+                    hits[pix] = h;
+                    vids[pix] = vid;
+                    continue;
+                }
                 if (vid == 0) continue;
                 for (uint32_t smp = 0; smp < P->spp; smp++) {
                     PathOut po;
-                    trace_path(s, mats, n_mats, *P, h, dir, pix, smp, &po, &st, &trc[t]);
+                    trace_path(s, mats, n_mats, *P, h, dir, pix, pix * P->spp + smp, &po, &st, &trc[t]);
                     st.paths++;
                     Deposit dp;
                     dp.vid = vid;
@@ -925,6 +1080,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         for (uint32_t t = 0; t < threads; t++) th.emplace_back(work, t);
         for (auto& x : th) x.join();
     }
+    if (sched) schedule_frame(R, s, mats, n_mats, cam, P, threads, hits, vids, path_rgb, deps, tstats, trc);
     ov_stats total{};
     for (uint32_t t = 0; t < threads; t++) {
         total.rays_primary += tstats[t].rays_primary;
@@ -934,6 +1090,8 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         total.fetch_restart += trc[t].fetch_restart;
         total.fetch_min += trc[t].fetch_min;
         total.steps += trc[t].steps;
+        total.scheduled_voxels += tstats[t].scheduled_voxels;
+        total.scheduled_paths += tstats[t].scheduled_paths;
         for (uint32_t sh = 0; sh < kShards; sh++) total.deposits += deps[t][sh].size();
     }
     run_parallel(kShards, threads, [&](uint32_t sh) {

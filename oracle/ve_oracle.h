@@ -31,6 +31,9 @@ struct ov_frame_params {
     float decay;
     float variance_norm;
     uint32_t flags;
+    /* importance-aware scheduling (flags & 64), core.hpp:95-112 */
+    float weight_pixels, weight_variance, pixels_norm, top_fraction, mid_fraction;
+    uint32_t min_samples, shading_budget;
 };
 
 struct ov_stats {
@@ -39,6 +42,7 @@ struct ov_stats {
     uint64_t fetch_min;       // distinct (level, node) words per ray (summed)
     uint64_t paths, deposits;
     uint64_t steps;           // DDA outer iterations (all rays)
+    uint64_t scheduled_voxels, scheduled_paths;  // scheduled frames
 };
 
 }  // extern "C"

@@ -46,6 +46,8 @@ FRAME_PATH_RGB = 4
 FRAME_LEARNED = 8
 FRAME_TERMINATE_HASH = 16
 FRAME_TRAIN = 32
+FRAME_SCHEDULED = 64
+RAYCAST_FULL_WALK = 1
 CFG_NO_GRAPHS = 1
 
 
@@ -69,7 +71,10 @@ class FrameConfigC(ctypes.Structure):
                 ("bounce_controlchecks", ctypes.c_uint32), ("reconstruction_radius", ctypes.c_uint32),
                 ("render_type", ctypes.c_uint32), ("frame_index", ctypes.c_uint32),
                 ("sun_dir", ctypes.c_float * 3), ("sun_intensity", ctypes.c_float), ("sky", ctypes.c_float * 3),
-                ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", ctypes.c_uint32)]
+                ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", ctypes.c_uint32),
+                ("weight_pixels", ctypes.c_float), ("weight_variance", ctypes.c_float),
+                ("pixels_norm", ctypes.c_float), ("top_fraction", ctypes.c_float), ("mid_fraction", ctypes.c_float),
+                ("min_samples", ctypes.c_uint32), ("shading_budget", ctypes.c_uint32)]
 
 
 class ViewC(ctypes.Structure):
@@ -97,6 +102,7 @@ class FrameStatsC(ctypes.Structure):
                 ("trace_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
                 ("cache_capacity", ctypes.c_uint64), ("nrc_queries", ctypes.c_uint64),
                 ("nrc_hash_terminated", ctypes.c_uint64), ("nrc_samples", ctypes.c_uint64),
+                ("scheduled_voxels", ctypes.c_uint64), ("scheduled_paths", ctypes.c_uint64),
                 ("ms_learned", ctypes.c_float), ("reserved", ctypes.c_uint32)]
 
 
@@ -165,6 +171,7 @@ _SIGNATURES = {
     "ve_scene_apply_edits": ([_P, _I32, _P, _P, _U64, _U32], ctypes.c_int),
     "ve_scene_download": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
     "ve_scene_footprint": ([_P, _I32, _PTR(_U64)], ctypes.c_int),
+    "ve_raycast_batch": ([_P, _I32, _P, _P, _U64, _U32, _U32, _P], ctypes.c_int),
     "ve_set_materials": ([_P, _P, _U32], ctypes.c_int),
     "ve_cache_reset": ([_P, _I32], ctypes.c_int),
     "ve_cache_dump": ([_P, _I32, _P, _P, _P, _U64, _PTR(_U64)], ctypes.c_int),
@@ -419,11 +426,19 @@ class FrameConfig:
     decay: float = 0.95
     variance_norm: float = 10000.0
     flags: int = 0
+    # importance-aware scheduling (FRAME_SCHEDULED), core.hpp:95-112 defaults
+    weight_pixels: float = 0.1
+    weight_variance: float = 0.9
+    pixels_norm: float = 100.0
+    top_fraction: float = 0.30
+    mid_fraction: float = 0.40
+    min_samples: int = 1
+    shading_budget: int = 131072
 
     def to_c(self) -> FrameConfigC:
         c = FrameConfigC()
         for f in ("width", "height", "spp", "bounces", "primary_controlchecks", "bounce_controlchecks",
-                  "reconstruction_radius", "render_type", "frame_index", "flags"):
+                  "reconstruction_radius", "render_type", "frame_index", "flags", "min_samples", "shading_budget"):
             setattr(c, f, int(getattr(self, f)))
         for i in range(3):
             c.sun_dir[i] = float(self.sun_dir[i])
@@ -431,6 +446,8 @@ class FrameConfig:
         c.sun_intensity = float(self.sun_intensity)
         c.decay = float(self.decay)
         c.variance_norm = float(self.variance_norm)
+        for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction"):
+            setattr(c, f, float(getattr(self, f)))
         return c
 
 
@@ -448,7 +465,8 @@ def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
         elif k in ("rgb", "mapped"):
             arrays[k] = np.zeros((fc.height, fc.width, 3), np.float32)
         elif k == "path_rgb":
-            arrays[k] = np.zeros((npx * fc.spp, 3), np.float32)
+            n = min(fc.shading_budget, 2 * npx) if fc.flags & FRAME_SCHEDULED else npx * fc.spp
+            arrays[k] = np.zeros((n, 3), np.float32)
         else:
             raise ValueError(f"unknown output {k!r}")
     o = FrameOutputsC()
@@ -528,6 +546,19 @@ class Renderer:
         p = np.ascontiguousarray(np.asarray(positions, np.uint32).reshape(-1, 3))
         _check(self._lib.ve_scene_refresh(self._h, scene_id, _ptr(p) if p.size else None, p.shape[0],
                                           1 if keep_cache else 0))
+
+    def raycast_batch(self, scene_id: int, origins: np.ndarray, dirs: np.ndarray, controlchecks: int = 300,
+                      full_walk: bool = False) -> np.ndarray:
+        """Rays through the device DDA; (n, 8) u32 rows {status, hit node,
+        material, x, y, z, size, checks}."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        if o.shape != d.shape:
+            raise ValueError("origins and dirs differ in shape")
+        out = np.zeros((o.shape[0], 8), np.uint32)
+        _check(self._lib.ve_raycast_batch(self._h, scene_id, _ptr(o), _ptr(d), o.shape[0], controlchecks,
+                                          RAYCAST_FULL_WALK if full_walk else 0, _ptr(out)))
+        return out
 
     def download_scene(self, scene_id: int) -> np.ndarray:
         n = _U64()

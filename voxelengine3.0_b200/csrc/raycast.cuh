@@ -82,7 +82,8 @@ __device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlche
 
 // Top-table entry of the cell containing (x, y, z): (offset << 1) | 1 when
 // levels 0..T0-1 are internal (offset = child block of the level-T0 node),
-// else (terminal level << 1).
+// else (terminal level << 1).  The table covers positions below 2^D on every
+// axis (root child 0, which level 0's bit-D test selects for them).
 __device__ __forceinline__ uint32_t top_index(uint32_t x, uint32_t y, uint32_t z, uint32_t D, uint32_t T0) {
     const uint32_t sh = D - T0 + 1u, b = T0 - 1u;
     return ((((x >> sh) << b) | (y >> sh)) << b) | (z >> sh);
@@ -124,7 +125,10 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
         bool found = false;
         uint32_t off = 0;
         k = start;
-        if (!COUNT && start < T0) {
+        // inBounds admits a coordinate equal to 2^D; level 0 then selects
+        // another root child than the table's, so such a position walks
+        // every level as the reference's descent does
+        if (!COUNT && start < T0 && !((ux | uy | uz) & L)) {
             const uint32_t ent = __ldg(top + top_index(ux, uy, uz, D, T0));
             if (ent & 1u) {
                 s.base[T0] = ent >> 1;

@@ -75,10 +75,15 @@ struct DevView {
     uint32_t tile_base;
     uint32_t pad0;
     unsigned long long path_base;
+    // importance-aware scheduling (rank.comp knobs)
+    float w_pix, w_var, pix_norm, top_frac, mid_frac;
+    uint32_t min_samples, budget, pad1;
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
-enum : uint32_t { CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_TOTAL = 64 };
+enum : uint32_t {
+    CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_TOTAL = 64
+};
 enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
     ST_RAYS_BOUNCE,
@@ -93,6 +98,8 @@ enum : uint32_t {
     ST_NRC_QUERIES,  // paths ended at their second vertex by the learned cache
     ST_NRC_HASH,     // ... by the hashed per-voxel cache
     ST_NRC_SAMPLES,  // training samples recorded
+    ST_SCHED_VOXELS, // scheduled frames: distinct visible voxels
+    ST_SCHED_PATHS,  // scheduled frames: shade-list entries
     ST_TOTAL = 16
 };
 enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u };
@@ -144,7 +151,21 @@ struct FrameArgs {
     uint32_t val_mask;
     uint32_t nrc_ready;     // cells without validation samples use the network
     uint32_t* p_aux;        // per path: training sample slot
+    // importance-aware scheduling (VE_FRAME_SCHEDULED, single view)
+    uint4* hitinfo;         // per pixel: {leaf slot, x | y << 16, z | material << 16, 0} of the primary hit
+    uint32_t* claim_key;    // per-frame voxel claim table (vid, 0 = free)
+    uint32_t* claim_pix;    // canonical (smallest) pixel of the voxel
+    uint32_t* claim_cnt;    // pixels that see the voxel
+    uint32_t claim_mask;
+    uint32_t* sched_n;      // per pixel: paths of its voxel when it is the canonical pixel
+    uint32_t* sched_off;    // exclusive prefix sum of sched_n
+    uint2* shade_list;      // {vid, pixel} per path
+    uint32_t shade_cap;
+    float* rank;            // the scene's {t_high, t_mid, histogram[256]} (thresholds from the previous frame)
 };
+
+constexpr uint32_t kRankBins = 256;
+constexpr uint32_t kClaimProbes = 64;
 
 // ---------------------------------------------------------------------------
 // warp helpers
@@ -697,9 +718,11 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
         const uint32_t pix = py * v.W + px;
         a.gbuf[v.pix_base + pix] = make_uint4(h.checks, h.status == kHit ? h.material : 0u,
                                               h.status == kHit ? h.id : 0u, vid);
+        if (v.flags & VE_FRAME_SCHEDULED)  // paths come from the shade list: keep the hit
+            a.hitinfo[v.pix_base + pix] = make_uint4(h.id, h.x | (h.y << 16), h.z | (h.material << 16), 0u);
     }
-    const bool spawn = inside && vid != 0u;
-    if (FUSED) {
+    const bool spawn = inside && vid != 0u && !(v.flags & VE_FRAME_SCHEDULED);
+    if (FUSED && !(v.flags & VE_FRAME_SCHEDULED)) {
         // the warp's (pixel, sample) pairs in chunks of 32, pixel-major: the
         // lanes of one chunk hold consecutive path slots (a row of the warp's
         // 8 x 4 pixel block), so path-state stores and queue entries stay
@@ -799,6 +822,168 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
     }
     warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+}
+
+// ---------------------------------------------------------------------------
+// Importance-aware voxel scheduling (schedule.comp, rank.comp, threshold.comp,
+// emit.comp), one view per frame.  Differences from the reference, for
+// determinism: a voxel's representative pixel is its smallest pixel index
+// (the reference keeps the first pixel to claim it, in a scrambled
+// workgroup order), the shade list is ordered by representative pixel
+// (prefix sum over pixels instead of atomic appends), and paths start from
+// the stored primary hit instead of re-casting the primary ray.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t claim_hash(uint32_t vid) {  // schedule.comp claimHash
+    uint32_t x = vid;
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    return x;
+}
+
+// schedule.comp: claim the voxel of every hit pixel, count its pixels and
+// keep its smallest pixel index.
+__global__ void __launch_bounds__(256) k_sched_claim(FrameArgs a) {
+    const DevView& v = a.views[0];
+    const uint32_t npix = v.W * v.H;
+    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
+        const uint32_t vid = a.gbuf[v.pix_base + pix].w;
+        if (vid == 0u) continue;
+        uint32_t h = claim_hash(vid) & a.claim_mask;
+        for (uint32_t q = 0; q < kClaimProbes; q++, h = (h + 1u) & a.claim_mask) {
+            const uint32_t prev = atomicCAS(&a.claim_key[h], 0u, vid);
+            if (prev == 0u || prev == vid) {
+                atomicMin(&a.claim_pix[h], pix);
+                atomicAdd(&a.claim_cnt[h], 1u);
+                break;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int claim_find(const FrameArgs& a, uint32_t vid) {
+    uint32_t h = claim_hash(vid) & a.claim_mask;
+    for (uint32_t q = 0; q < kClaimProbes; q++, h = (h + 1u) & a.claim_mask) {
+        const uint32_t k = a.claim_key[h];
+        if (k == vid) return int(h);
+        if (k == 0u) return -1;
+    }
+    return -1;
+}
+
+// rank.comp: importance = w_pix * coverage + w_var * variance (the voxel's
+// radiance-cache variance from the previous frames, on the VARIANCE view's
+// scale), tiers from the previous frame's thresholds, histogram for the
+// next ones.  sched_n[pix] = paths of the voxel at its representative pixel.
+__global__ void __launch_bounds__(256) k_sched_rank(FrameArgs a) {
+    const DevView& v = a.views[0];
+    const DevScene S = a.scenes[v.scene];
+    const uint32_t npix = v.W * v.H;
+    const float t_high = a.rank[0], t_mid = a.rank[1];
+    uint32_t* hist = reinterpret_cast<uint32_t*>(a.rank + 2);
+    uint32_t nvox = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < npix; base += gridDim.x * blockDim.x) {
+        const uint32_t pix = base + threadIdx.x;
+        uint32_t n = 0;
+        if (pix < npix) {
+            const uint32_t vid = a.gbuf[v.pix_base + pix].w;
+            const int c = vid ? claim_find(a, vid) : -1;
+            if (c >= 0 && a.claim_pix[c] == pix) {
+                nvox++;
+                const Avg av = lookup_avg(S, vid);
+                const float var = av.count >= 2u ? av.var : 0.0f;
+                const float pn = gclamp(float(a.claim_cnt[c]) / gmax(v.pix_norm, 1.0f), 0.0f, 1.0f);
+                const float vn = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
+                const float imp = v.w_pix * pn + v.w_var * vn;
+                n = imp >= t_high ? 2u : (imp >= t_mid ? 1u : v.min_samples);
+                uint32_t bin = uint32_t(imp * float(kRankBins));
+                if (bin >= kRankBins) bin = kRankBins - 1u;
+                atomicAdd(&hist[bin], 1u);
+            }
+            a.sched_n[pix] = n;
+        }
+    }
+    warp_add_stat(&a.stats[ST_SCHED_VOXELS], nvox);
+}
+
+// The shade list: n entries {vid, pixel} at the pixel's prefix-sum offset,
+// cut at the shading budget; the last pixel publishes the entry count.
+__global__ void __launch_bounds__(256) k_sched_list(FrameArgs a) {
+    const DevView& v = a.views[0];
+    const uint32_t npix = v.W * v.H;
+    const uint32_t cap = min(a.shade_cap, v.budget);
+    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
+        const uint32_t n = a.sched_n[pix], off = a.sched_off[pix];
+        if (pix + 1u == npix) a.counters[CNT_SCHED] = min(off + n, cap);
+        if (n == 0u) continue;
+        const uint32_t vid = a.gbuf[v.pix_base + pix].w;
+        for (uint32_t j = 0; j < n && off + j < cap; j++) a.shade_list[off + j] = make_uint2(vid, pix);
+    }
+}
+
+// threshold.comp: the next frame's thresholds from this frame's histogram
+// (top_frac of the voxels above t_high, the next mid_frac above t_mid).
+__global__ void k_sched_threshold(float* rank, const DevView* views) {
+    uint32_t* hist = reinterpret_cast<uint32_t*>(rank + 2);
+    uint32_t total = 0;
+    for (uint32_t b = 0; b < kRankBins; b++) total += hist[b];
+    if (total == 0u) {
+        rank[0] = __int_as_float(0x7f800000);   // +inf
+        rank[1] = __int_as_float(0xff800000);   // -inf
+        return;
+    }
+    const float top = gclamp(views[0].top_frac, 0.0f, 1.0f);
+    const float mid = gclamp(views[0].mid_frac, 0.0f, 1.0f - top);
+    const uint32_t top_n = uint32_t(top * float(total)), topmid_n = uint32_t((top + mid) * float(total));
+    uint32_t cum = 0, hb = kRankBins, mb = kRankBins;
+    for (int b = int(kRankBins) - 1; b >= 0; b--) {
+        cum += hist[b];
+        if (hb == kRankBins && cum >= top_n) hb = uint32_t(b);
+        if (mb == kRankBins && cum >= topmid_n) mb = uint32_t(b);
+        if (hb != kRankBins && mb != kRankBins) break;
+    }
+    if (hb == kRankBins) hb = kRankBins - 1u;
+    if (mb == kRankBins) mb = kRankBins - 1u;
+    rank[0] = float(hb) / float(kRankBins);
+    rank[1] = float(mb) / float(kRankBins);
+}
+
+// emit.comp: one path per shade-list entry, from the representative pixel's
+// primary hit, list index i seeding the RNG; its first shading step runs
+// here as in the fused primary pass.
+__global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
+    __shared__ DepSlot dep[256];
+    const DevView& v = a.views[0];
+    const uint32_t n = a.counters[CNT_SCHED];
+    const f3 plane = mk(v.cam[4], v.cam[5], v.cam[6]);
+    const f3 right = mk(v.cam[8], v.cam[9], v.cam[10]);
+    const f3 up = mk(v.cam[12], v.cam[13], v.cam[14]);
+    uint32_t n_ext = 0, n_sh = 0, n_paths = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t p = uint32_t(v.path_base) + i;
+        ShadeOut o;
+        if (i < n) {
+            const uint2 e = a.shade_list[i];
+            const uint32_t pix = e.y, px = pix % v.W, py = pix / v.W;
+            const float ndx = (float(px) + 0.5f) / float(v.W) * 2.0f - 1.0f;
+            const float ndy = (float(py) + 0.5f) / float(v.H) * 2.0f - 1.0f;
+            const f3 dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
+            const uint4 hi = a.hitinfo[v.pix_base + pix];
+            // emit.comp:171-174 with listIdx = the shade-list index
+            const uint32_t sample_idx = v.frame_index + pix * 2654435761u + i * 1442695040u;
+            const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+            shade_step(a, p, make_uint4(e.x, rng, 0u + a.view_offset, pix), mk(1.0f, 1.0f, 1.0f), mk(0.0f, 0.0f, 0.0f),
+                       mk(0.0f, 0.0f, 0.0f), dir, make_uint4(kHit, hi.x, hi.y, hi.z), o);
+            n_paths++;
+        }
+        shade_emit(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
+                   n_ext, n_sh);
+    }
+    warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
+    warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+    warp_add_stat(&a.stats[ST_PATHS], n_paths);
+    warp_add_stat(&a.stats[ST_SCHED_PATHS], n_paths);
 }
 
 // Staging of a learned-cache query in a frame (runs in the encode kernel, at
@@ -1107,6 +1292,7 @@ struct SceneSlot {
     uint32_t top_level = 0;
     bool live = false;
     ve_nrc* nrc = nullptr;  // learned radiance cache attached to the scene
+    float* rank = nullptr;  // scheduling state: {t_high, t_mid, histogram[256]}
 };
 
 template <typename T>
@@ -1154,6 +1340,13 @@ struct ve_ctx {
     ve::DevBuf<uint4> p_hit, p_meta;
     ve::DevBuf<uint8_t> p_vis;
     ve::DevBuf<uint32_t> p_aux;  // training sample slot per path (learned-cache training frames)
+    // importance-aware scheduling: primary hits, voxel claim table (key,
+    // representative pixel, pixel count), per-pixel path counts and their
+    // prefix sums, shade list, scan scratch
+    ve::DevBuf<uint4> hitinfo;
+    ve::DevBuf<uint32_t> claim, sched_n;
+    ve::DevBuf<uint2> shade_list;
+    ve::DevBuf<uint8_t> scan_tmp;
     ve::DevBuf<uint32_t> live0, live1, rayq;
     ve::DevBuf<uint32_t> counters;
     ve::DevBuf<unsigned long long> stats;
@@ -1168,6 +1361,8 @@ struct ve_ctx {
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
+    ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
+    ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
     int occ_trace = 1, occ_trace_count = 1, occ_shade = 1;  // occupancy maxima (blocks/SM)
     ve_launch_config launch{0, 0, 8, 0};
@@ -1385,6 +1580,17 @@ static int compute_normals(ve_ctx* c, SceneSlot& s) {
     return VE_OK;
 }
 
+// Scheduling thresholds {t_high = +inf, t_mid = -inf} and an empty histogram:
+// every voxel of the next scheduled frame falls in the middle tier.
+static int reset_rank(ve_ctx* c, float* rank) {
+    std::vector<uint32_t> init(2 + kRankBins, 0u);
+    init[0] = 0x7f800000u;
+    init[1] = 0xff800000u;
+    VE_CUDA(cudaMemcpyAsync(rank, init.data(), init.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
 static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_views) {
     int rc = 0;
     const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->p_ray_o.p,
@@ -1502,10 +1708,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         const uint32_t tx = (f.width + 15) / 16, ty = (f.height + 15) / 16;
         tiles += tx * ty;
         pixels += uint64_t(f.width) * f.height;
-        paths += uint64_t(f.width) * f.height * f.spp;
+        paths += (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2ull * f.width * f.height)
+                                                : uint64_t(f.width) * f.height * f.spp;
         max_b = std::max(max_b, f.bounces);
         flags |= f.flags;
     }
+    if ((flags & VE_FRAME_SCHEDULED) && nv != 1)
+        return fail(VE_ERR_INVALID, "render: VE_FRAME_SCHEDULED renders one view per call");
+    if ((flags & VE_FRAME_SCHEDULED) && (flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN)))
+        return fail(VE_ERR_INVALID, "render: VE_FRAME_SCHEDULED does not combine with the learned cache");
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
     // learned radiance cache: one per batch, attached to the views' scenes
     ve_nrc* nrc = nullptr;
@@ -1518,6 +1729,28 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     }
     int rc = ensure_frame(c, pixels, paths, nv);
     if (rc) return rc;
+    const bool sched = (flags & VE_FRAME_SCHEDULED) != 0;
+    uint32_t claim_size = 0;
+    size_t scan_bytes = 0;
+    if (sched) {
+        SceneSlot& sc = c->scenes[views[0].scene_id];
+        const void* before[] = {c->hitinfo.p, c->claim.p, c->sched_n.p, c->shade_list.p, c->scan_tmp.p, sc.rank};
+        claim_size = 1024u;
+        while (claim_size < 2ull * pixels) claim_size <<= 1;
+        cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, c->sched_n.p, c->sched_n.p, int(pixels), c->stream);
+        if ((rc = c->hitinfo.ensure(pixels)) || (rc = c->claim.ensure(3ull * claim_size)) ||
+            (rc = c->sched_n.ensure(2 * pixels)) || (rc = c->shade_list.ensure(paths)) ||
+            (rc = c->scan_tmp.ensure(scan_bytes)))
+            return rc;
+        if (!sc.rank) {
+            if (cudaMalloc(&sc.rank, (2 + kRankBins) * 4) != cudaSuccess)
+                return fail(VE_ERR_NOMEM, "render: scheduling state allocation failed");
+            if ((rc = reset_rank(c, sc.rank))) return rc;
+        }
+        const void* after[] = {c->hitinfo.p, c->claim.p, c->sched_n.p, c->shade_list.p, c->scan_tmp.p, sc.rank};
+        for (int i = 0; i < 6; i++)
+            if (before[i] != after[i]) c->gen++;
+    }
     if (nrc) {
         bool moved = false;
         if ((rc = nrc::prepare_frame(nrc, paths, &moved))) return rc;
@@ -1557,12 +1790,20 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         d.sun_intensity = f.sun_intensity;
         d.decay = f.decay;
         d.variance_norm = f.variance_norm;
+        d.w_pix = f.weight_pixels;
+        d.w_var = f.weight_variance;
+        d.pix_norm = f.pixels_norm;
+        d.top_frac = f.top_fraction;
+        d.mid_frac = f.mid_fraction;
+        d.min_samples = std::min<uint32_t>(f.min_samples, 2u);
+        d.budget = f.shading_budget;
         d.pix_base = uint32_t(pix_base);
         d.tile_base = tile_base;
         d.path_base = path_base;
         tile_base += d.tiles_x * ((f.height + 15) / 16);
         pix_base += uint64_t(f.width) * f.height;
-        path_base += uint64_t(f.width) * f.height * f.spp;
+        path_base += (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2ull * f.width * f.height)
+                                                    : uint64_t(f.width) * f.height * f.spp;
     }
     cudaStream_t st = c->stream;
     const bool timing = (flags & VE_FRAME_TIMING) != 0;
@@ -1628,6 +1869,18 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         a.nrc_ready = nrc->trained_steps >= nrc::kReadySteps ? 1u : 0u;
         a.p_aux = train ? c->p_aux.p : nullptr;
     }
+    if (sched) {
+        a.hitinfo = c->hitinfo.p;
+        a.claim_key = c->claim.p;
+        a.claim_pix = c->claim.p + claim_size;
+        a.claim_cnt = c->claim.p + 2ull * claim_size;
+        a.claim_mask = claim_size - 1u;
+        a.sched_n = c->sched_n.p;
+        a.sched_off = c->sched_n.p + pixels;
+        a.shade_list = c->shade_list.p;
+        a.shade_cap = uint32_t(paths);
+        a.rank = c->scenes[views[0].scene_id].rank;
+    }
     // the frame's kernel sequence (no host synchronisation inside)
     auto enqueue = [&]() {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
@@ -1647,6 +1900,21 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (count) k_primary<true, true><<<tiles, 256, 0, st>>>(a);
         else k_primary<false, true><<<tiles, 256, 0, st>>>(a);
         launches++;
+        if (sched) {  // schedule -> rank -> shade list -> thresholds -> emit
+            cudaMemsetAsync(a.claim_key, 0, 4ull * claim_size, st);
+            cudaMemsetAsync(a.claim_pix, 0xFF, 4ull * claim_size, st);
+            cudaMemsetAsync(a.claim_cnt, 0, 4ull * claim_size, st);
+            cudaMemsetAsync(a.rank + 2, 0, 4ull * kRankBins, st);
+            const int g = c->num_sms * 8;
+            k_sched_claim<<<g, 256, 0, st>>>(a);
+            k_sched_rank<<<g, 256, 0, st>>>(a);
+            size_t b = scan_bytes;
+            cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, b, a.sched_n, a.sched_off, int(pixels), st);
+            k_sched_list<<<g, 256, 0, st>>>(a);
+            k_sched_threshold<<<1, 1, 0, st>>>(a.rank, a.views);
+            k_sched_emit<<<c->grid_shade, 256, 0, st>>>(a);
+            launches += 6;
+        }
         rec();
         for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
             if (pass > 0) {  // pass 0 runs inside the fused primary
@@ -1689,7 +1957,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     } else {
         std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
                                      flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
-                                              VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN),
+                                              VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED),
                                      paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
                                      uint64_t(c->launch.refill_threshold), uint64_t(uintptr_t(nrc)),
                                      uint64_t(a.nrc_ready)};
@@ -1754,7 +2022,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         for (uint32_t i = 0; i < nv; i++) {
             const ve_frame_config& f = views[i].frame;
             const uint64_t np = uint64_t(f.width) * f.height;
-            const uint64_t nq = np * f.spp;
+            const uint64_t nq = (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2 * np)
+                                                               : np * f.spp;
             ve_frame_outputs& o = outs[i];
             if (o.gbuffer) { VE_CUDA(cudaMemcpyAsync(o.gbuffer, c->gbuf.p + pb, np * 16, cudaMemcpyDeviceToHost, st)); d2h += np * 16; }
             if (o.voxel_id) { VE_CUDA(cudaMemcpyAsync(o.voxel_id, c->out_vid.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
@@ -1779,6 +2048,26 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     c->tot_trace_launches += trace_launches;
     if (train) nrc->trained_steps++;
     return VE_OK;
+}
+
+// Batch of independent rays through the device DDA (the same raycast the
+// frame kernels run): 8 words per ray {status, hit node, material, x, y, z,
+// size, checks} as Raycast / RaycastCounted (internal.glsl:297-400) reports
+// them.  VE_RAYCAST_FULL_WALK descends every level per step (the
+// fetch-counting variant) instead of starting from the top table.
+template <bool FULL>
+__global__ void __launch_bounds__(256) k_raycast_batch(DevScene S, const float* __restrict__ in, uint64_t n,
+                                                       uint32_t cc, uint32_t* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const f3 o = mk(in[3 * i + 0], in[3 * i + 1], in[3 * i + 2]);
+        const f3 d = mk(in[3 * (n + i) + 0], in[3 * (n + i) + 1], in[3 * (n + i) + 2]);
+        RayCount rc;
+        const Hit h = raycast<FULL>(S.nodes, S.n_words, S.depth, S.top, S.top_level, o, d, cc, rc);
+        uint32_t* w = out + 8 * i;
+        w[0] = h.status; w[1] = h.id; w[2] = h.material;
+        w[3] = h.x; w[4] = h.y; w[5] = h.z;
+        w[6] = h.size; w[7] = h.checks;
+    }
 }
 
 }  // namespace ve
@@ -1897,14 +2186,16 @@ int ve_ctx_destroy(ve_ctx* c) {
         if (s.alloc) cudaFree(s.alloc);
         if (s.cache) cudaFree(s.cache);
         if (s.top) cudaFree(s.top);
+        if (s.rank) cudaFree(s.rank);
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
     c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
     c->p_indirect.release(); c->p_pend.release(); c->p_hit.release(); c->p_meta.release(); c->p_vis.release();
     c->live0.release(); c->live1.release(); c->rayq.release(); c->counters.release(); c->stats.release();
     c->p_aux.release();
+    c->hitinfo.release(); c->claim.release(); c->sched_n.release(); c->shade_list.release(); c->scan_tmp.release();
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
-    c->out_mapped.release(); c->path_rgb.release();
+    c->out_mapped.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
         if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
         if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
@@ -2216,6 +2507,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     cudaFree(s.alloc);
     cudaFree(s.cache);
     if (s.top) cudaFree(s.top);
+    if (s.rank) cudaFree(s.rank);
     s = SceneSlot();
     c->scenes_dirty = true;
     c->gen++;
@@ -2285,6 +2577,33 @@ int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64
     return VE_OK;
 }
 
+// ve_raycast_batch: rays from host memory through k_raycast_batch.
+int ve_raycast_batch(ve_ctx* c, int32_t id, const float* origins, const float* dirs, uint64_t n,
+                     uint32_t controlchecks, uint32_t flags, uint32_t* out) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "raycast_batch: unknown scene");
+    if (n == 0) return VE_OK;
+    if (!origins || !dirs || !out) return fail(VE_ERR_INVALID, "raycast_batch: null argument");
+    if (n > (1ull << 28)) return fail(VE_ERR_CAPACITY, "raycast_batch: at most 2^28 rays per call");
+    if (controlchecks > kMaxControlChecks) return fail(VE_ERR_INVALID, "raycast_batch: controlchecks must be <= 65536");
+    int rc;
+    if ((rc = c->ray_in.ensure(6 * n)) || (rc = c->ray_out.ensure(8 * n))) return rc;
+    const SceneSlot& sl = c->scenes[id];
+    const DevScene S{sl.nodes, sl.n_words, sl.cache, sl.depth, c->cfg.hash_log2, c->cfg.hash_probes, sl.top_level, sl.top};
+    cudaStream_t st = c->stream;
+    VE_CUDA(cudaMemcpyAsync(c->ray_in.p, origins, 12 * n, cudaMemcpyHostToDevice, st));
+    VE_CUDA(cudaMemcpyAsync(c->ray_in.p + 3 * n, dirs, 12 * n, cudaMemcpyHostToDevice, st));
+    const uint32_t grid = uint32_t(std::min<uint64_t>((n + 255) / 256, uint64_t(c->num_sms) * 16));
+    if (flags & VE_RAYCAST_FULL_WALK)
+        k_raycast_batch<true><<<grid, 256, 0, st>>>(S, c->ray_in.p, n, controlchecks, c->ray_out.p);
+    else
+        k_raycast_batch<false><<<grid, 256, 0, st>>>(S, c->ray_in.p, n, controlchecks, c->ray_out.p);
+    VE_CUDA(cudaGetLastError());
+    VE_CUDA(cudaMemcpyAsync(out, c->ray_out.p, 32 * n, cudaMemcpyDeviceToHost, st));
+    VE_CUDA(cudaStreamSynchronize(st));
+    return VE_OK;
+}
+
 int ve_scene_footprint(ve_ctx* c, int32_t id, uint64_t* bytes) {
     if (!c || !bytes || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_footprint: unknown scene");
@@ -2318,6 +2637,11 @@ int ve_cache_reset(ve_ctx* c, int32_t id) {
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "cache_reset: unknown scene");
     VE_CUDA(cudaMemsetAsync(c->scenes[id].cache, 0, sizeof(CacheEntry) << c->cfg.hash_log2, c->stream));
+    // the scheduling thresholds derive from the cache: forget them too
+    if (c->scenes[id].rank) {
+        const int rc = reset_rank(c, c->scenes[id].rank);
+        if (rc) return rc;
+    }
     VE_CUDA(cudaStreamSynchronize(c->stream));
     return VE_OK;
 }
@@ -2442,6 +2766,8 @@ static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
     r.nrc_queries = h[ST_NRC_QUERIES];
     r.nrc_hash_terminated = h[ST_NRC_HASH];
     r.nrc_samples = h[ST_NRC_SAMPLES];
+    r.scheduled_voxels = h[ST_SCHED_VOXELS];
+    r.scheduled_paths = h[ST_SCHED_PATHS];
 }
 
 int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
