@@ -685,15 +685,17 @@ inline f3 pixel_dir(const float cam[16], uint32_t px, uint32_t py, uint32_t W, u
 //             (var: the cache's luminance variance, 0 below two samples);
 //             2 paths at or above t_high, 1 at or above t_mid, else
 //             min_samples; a 256-bin histogram of the importances
-//   list      entries {vid, pixel} in representative-pixel order, cut at
-//             min(shading_budget, 2 * pixels)
+//   list      entries {vid, pixel} in representative-pixel order starting
+//             at pixel (frame * 0x9E3779B9 mod 2^32) mod pixels and wrapping,
+//             cut at min(shading_budget, 2 * pixels)
 //   threshold the next frame's t_high / t_mid: the bins where the reverse
 //             cumulative count reaches top_fraction and top + mid fractions
 //   emit      one path per entry from the representative pixel's primary
 //             hit, the entry index seeding the path.
 // The device implementation follows the same deterministic order (smallest
-// pixel as the representative, list ordered by pixel); the reference keeps
-// the first pixel to claim and appends with atomics.
+// pixel as the representative, list ordered by rotated pixel); the reference
+// keeps the first pixel to claim and appends with atomics, so its budget cut
+// falls on whichever voxels rank last in that frame's workgroup order.
 void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t n_mats, const float cam[16],
                     const ov_frame_params* P, uint32_t threads, const std::vector<Hit>& hits,
                     const std::vector<uint32_t>& vids, float* path_rgb,
@@ -712,8 +714,10 @@ void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t 
     std::vector<uint32_t> hist(kRankBins, 0u);
     std::vector<std::pair<uint32_t, uint32_t>> list;  // {vid, pixel}
     const uint64_t cap = std::min<uint64_t>(P->shading_budget, 2ull * npix);
+    const uint32_t rot = uint32_t(uint64_t(P->frame_index * 0x9E3779B9u) % npix);
     uint64_t nvox = 0;
-    for (uint32_t pix = 0; pix < npix; pix++) {
+    for (uint32_t j = 0; j < npix; j++) {
+        const uint32_t pix = (j + rot) % npix;
         const uint32_t vid = vids[pix];
         if (!vid) continue;
         const Claim& cl = claims[vid];

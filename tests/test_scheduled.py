@@ -88,6 +88,21 @@ def test_oracle_schedule_budget(ve, oracle):
     assert (o["path_rgb"] > 0).any()
 
 
+def test_oracle_budget_cut_rotates(ve, oracle):
+    """Over budget, the list starts at a per-frame rotation of the pixel
+    order, so the voxels left out change from frame to frame."""
+    words, depth, mats, cam, fc = helpers.small_setup()
+    words = oracle.fill_normals(words, depth)
+    fc = sched_config(ve, fc, shading_budget=1000)
+    orc = OracleRenderer(oracle)
+    for f in range(6):
+        fc.frame_index = f
+        o = orc.render(words, depth, mats, cam, frame_params(fc), threads=4)
+        assert o["stats"]["scheduled_paths"] == 1000
+    vids, counts, _ = orc.cache()
+    assert vids.size > 2000  # without the rotation the same <= 1000 voxels would be shaded every frame
+
+
 def test_oracle_schedule_thread_invariant(ve, oracle):
     words, depth, mats, cam, fc = helpers.small_setup()
     words = oracle.fill_normals(words, depth)
@@ -206,10 +221,17 @@ def test_shading_budget(ve, oracle, renderer, small):
     sid, words, depth, mats, cam, fc = small
     renderer.cache_reset(sid)
     fc = sched_config(ve, fc, flags=ve.FRAME_SCHEDULED | ve.FRAME_PATH_RGB, shading_budget=1000)
-    g, st, o = frame_pair(renderer, OracleRenderer(oracle), sid, words, depth, mats, cam, fc)
-    assert_frame_exact(g, st, o)
-    assert st["scheduled_paths"] == 1000 == st["paths"]
-    assert g["path_rgb"].shape == (1000, 3)
+    orc = OracleRenderer(oracle)
+    for f in (0, 5, 6):  # rotation 0 and two others
+        fc.frame_index = f
+        g, st, o = frame_pair(renderer, orc, sid, words, depth, mats, cam, fc)
+        assert_frame_exact(g, st, o)
+        assert st["scheduled_paths"] == 1000 == st["paths"]
+        assert g["path_rgb"].shape == (1000, 3)
+    vids, counts, _ = renderer.cache_dump(sid)
+    ovids, ocounts, _ = orc.cache()
+    assert np.array_equal(vids, ovids)
+    assert np.array_equal(counts.astype(np.uint64), ocounts)
 
 
 @pytest.mark.gpu

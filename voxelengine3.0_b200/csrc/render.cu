@@ -830,8 +830,13 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
 // determinism: a voxel's representative pixel is its smallest pixel index
 // (the reference keeps the first pixel to claim it, in a scrambled
 // workgroup order), the shade list is ordered by representative pixel
-// (prefix sum over pixels instead of atomic appends), and paths start from
-// the stored primary hit instead of re-casting the primary ray.
+// starting at a per-frame rotation of the pixel index (a prefix sum instead
+// of atomic appends; the rotation spreads the shading budget's cut over the
+// image from frame to frame), and paths start from the stored primary hit
+// instead of re-casting the primary ray.
+__device__ __forceinline__ uint32_t sched_rotation(uint32_t frame, uint32_t npix) {
+    return uint32_t((unsigned long long)(frame * 0x9E3779B9u) % npix);
+}
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t claim_hash(uint32_t vid) {  // schedule.comp claimHash
     uint32_t x = vid;
@@ -874,12 +879,14 @@ __device__ __forceinline__ int claim_find(const FrameArgs& a, uint32_t vid) {
 // rank.comp: importance = w_pix * coverage + w_var * variance (the voxel's
 // radiance-cache variance from the previous frames, on the VARIANCE view's
 // scale), tiers from the previous frame's thresholds, histogram for the
-// next ones.  sched_n[pix] = paths of the voxel at its representative pixel.
+// next ones.  sched_n[j] = paths of the voxel whose representative pixel
+// is pix, j = (pix - rotation) mod pixels.
 __global__ void __launch_bounds__(256) k_sched_rank(FrameArgs a) {
     const DevView& v = a.views[0];
     const DevScene S = a.scenes[v.scene];
     const uint32_t npix = v.W * v.H;
     const float t_high = a.rank[0], t_mid = a.rank[1];
+    const uint32_t rot = sched_rotation(v.frame_index, npix);
     uint32_t* hist = reinterpret_cast<uint32_t*>(a.rank + 2);
     uint32_t nvox = 0;
     for (uint32_t base = blockIdx.x * blockDim.x; base < npix; base += gridDim.x * blockDim.x) {
@@ -900,24 +907,27 @@ __global__ void __launch_bounds__(256) k_sched_rank(FrameArgs a) {
                 if (bin >= kRankBins) bin = kRankBins - 1u;
                 atomicAdd(&hist[bin], 1u);
             }
-            a.sched_n[pix] = n;
+            a.sched_n[pix >= rot ? pix - rot : pix + (npix - rot)] = n;
         }
     }
     warp_add_stat(&a.stats[ST_SCHED_VOXELS], nvox);
 }
 
-// The shade list: n entries {vid, pixel} at the pixel's prefix-sum offset,
-// cut at the shading budget; the last pixel publishes the entry count.
+// The shade list: n entries {vid, pixel} at the rotated pixel's prefix-sum
+// offset, cut at the shading budget; the last position publishes the entry
+// count.
 __global__ void __launch_bounds__(256) k_sched_list(FrameArgs a) {
     const DevView& v = a.views[0];
     const uint32_t npix = v.W * v.H;
     const uint32_t cap = min(a.shade_cap, v.budget);
-    for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
-        const uint32_t n = a.sched_n[pix], off = a.sched_off[pix];
-        if (pix + 1u == npix) a.counters[CNT_SCHED] = min(off + n, cap);
+    const uint32_t rot = sched_rotation(v.frame_index, npix);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < npix; j += gridDim.x * blockDim.x) {
+        const uint32_t n = a.sched_n[j], off = a.sched_off[j];
+        if (j + 1u == npix) a.counters[CNT_SCHED] = min(off + n, cap);
+        const uint32_t pix = j < npix - rot ? j + rot : j - (npix - rot);
         if (n == 0u) continue;
         const uint32_t vid = a.gbuf[v.pix_base + pix].w;
-        for (uint32_t j = 0; j < n && off + j < cap; j++) a.shade_list[off + j] = make_uint2(vid, pix);
+        for (uint32_t e = 0; e < n && off + e < cap; e++) a.shade_list[off + e] = make_uint2(vid, pix);
     }
 }
 
