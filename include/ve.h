@@ -265,7 +265,7 @@ int ve_render(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
 int ve_render_batch(ve_ctx* ctx, const ve_view* views, uint32_t n_views, ve_frame_outputs* outs);
 /* Launch shape of the persistent bounce kernels: resident blocks per SM of
  * the trace and shade kernels (0 = occupancy maximum) and the number of idle
- * lanes at which a trace warp refills itself with new rays. */
+ * lanes at which a trace warp refills itself with new rays (0 = default, 24). */
 typedef struct ve_launch_config {
     uint32_t trace_blocks_per_sm;
     uint32_t shade_blocks_per_sm;
