@@ -302,7 +302,7 @@ int ve_reset_total_stats(ve_ctx* ctx);
 typedef struct ve_server ve_server;
 typedef struct ve_server_config {
     uint64_t pixel_capacity; /* pooled pixels: GBuffer + outputs, 48 B each */
-    uint64_t path_capacity;  /* pooled path states, 145 B each */
+    uint64_t path_capacity;  /* pooled path states, 144 B each */
     uint32_t max_requests;   /* view slots (requests on the GPU at once) */
     uint32_t flags;
 } ve_server_config;

@@ -89,7 +89,9 @@ __device__ __forceinline__ uint32_t top_index(uint32_t x, uint32_t y, uint32_t z
     return ((((x >> sh) << b) | (y >> sh)) << b) | (z >> sh);
 }
 
-template <bool COUNT>
+// WORD: a hit reports the leaf's node word in h.id instead of its slot (the
+// bounce trace keeps the word for shading; the slot is the GBuffer's field).
+template <bool COUNT, bool WORD = false>
 __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
                                          const uint32_t* __restrict__ top, uint32_t T0, Hit& h, RayCount& rc) {
     const uint32_t L = 1u << D;
@@ -156,7 +158,7 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
             const uint32_t mat = (raw & 254u) >> 1;
             if (mat != 0u) {
                 h.status = kHit;
-                h.id = off;
+                h.id = WORD ? raw : off;
                 h.material = mat;
                 h.x = ux; h.y = uy; h.z = uz;
                 h.size = 1u;

@@ -123,10 +123,9 @@ struct FrameArgs {
     float4* p_tp;        // throughput
     float4* p_direct;    // direct radiance (sun at bounce 0, bounce-0 emission)
     float4* p_indirect;  // indirect radiance
-    float4* p_pend;      // pending sun contribution, w = channel (0 direct, 1 indirect)
-    uint4* p_hit;        // {status, node slot, x | y<<16, z | material<<16}
+    float4* p_pend;      // pending sun contribution; w = 0, set to 1 by the shadow trace when the sun is visible
+    uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
-    uint8_t* p_vis;      // sun visibility from the shadow trace
     uint32_t* live[2];
     uint32_t* rayq;
     uint32_t* counters;
@@ -308,7 +307,7 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
 // serves all idle lanes of the warp, once `refill` of them are idle or none is
 // busy), so warps stay full although ray lengths differ by 100x.
 template <bool COUNT>
-__global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
@@ -318,9 +317,12 @@ __global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t* top = nullptr;
     uint64_t n_words = 0;
     Dda s;
-    Hit h;
     RayCount rc;
     for (;;) {
+        // the result lives one iteration: written and stored when a ray ends
+        Hit h;
+        h.status = kEscaped;
+        h.id = h.material = h.x = h.y = h.z = 0u;
         const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
         const unsigned busy = __ballot_sync(0xffffffffu, active);
         if (idle == 0u && busy == 0u) break;
@@ -353,13 +355,18 @@ __global__ void __launch_bounds__(256, 5) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_step<COUNT>(s, nodes, n_words, D, top, T0, h, rc);
+            finished = dda_step<COUNT, true>(s, nodes, n_words, D, top, T0, h, rc);
             if (finished) active = false;
         }
         if (finished) {
             const uint32_t p = e & 0x7FFFFFFFu;
-            if (e >> 31) a.p_vis[p] = h.status == kEscaped ? 1u : 0u;
-            else a.p_hit[p] = make_uint4(h.status, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+            if (e >> 31) {
+                if (h.status == kEscaped) reinterpret_cast<float*>(a.p_pend + p)[3] = 1.0f;
+            } else {
+                // h.id holds the hit leaf's word: the shade pass needs no
+                // dependent load from the node array
+                a.p_hit[p] = make_uint4(h.status, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+            }
         }
     }
     if (COUNT) {
@@ -479,7 +486,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
             const f3 albedo = mk(m.albedo_rough.x, m.albedo_rough.y, m.albedo_rough.z);
             const float roughness = m.albedo_rough.w, metallic = m.params.x, spec = m.params.y;
             const bool emissive = m.params.z != 0.0f;
-            const f3 N = shading_normal(fetch_node(S.nodes, S.n_words, hit.y), dir);
+            const f3 N = shading_normal(hit.y, dir);
             if (emissive) {  // shade.comp:576-583
                 const float k = m.params.w;
                 f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
@@ -565,7 +572,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                 const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
                 f3 c = muls(brdf, v.sun_intensity);
                 c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
-                a.p_pend[p] = st3(mul(tp, c), b == 0u ? 0.0f : 1.0f);
+                a.p_pend[p] = st3(mul(tp, c), 0.0f);
                 nf |= F_PENDING;
                 o.app_sh = true;
             }
@@ -705,7 +712,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     h.checks = 0;
     f3 dir = mk(0.0f, 0.0f, 0.0f);
     RayCount rc;
-    uint32_t vid = 0;
+    uint32_t vid = 0, word = 0;
     if (inside) {
         const float ndx = (float(px) + 0.5f) / float(v.W) * 2.0f - 1.0f;
         const float ndy = (float(py) + 0.5f) / float(v.H) * 2.0f - 1.0f;
@@ -715,12 +722,15 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
         dir = normalize(sub(add(plane, muls(right, ndx)), muls(up, ndy)));
         h = raycast<COUNT>(S.nodes, S.n_words, S.depth, S.top, S.top_level, mk(v.cam[0], v.cam[1], v.cam[2]), dir,
                            v.cc_primary, rc);
-        if (h.status == kHit) vid = voxel_key(h.x, h.y, h.z) + 1u;
+        if (h.status == kHit) {
+            vid = voxel_key(h.x, h.y, h.z) + 1u;
+            word = __ldg(S.nodes + h.id);  // the hit leaf's word, for shading
+        }
         const uint32_t pix = py * v.W + px;
         a.gbuf[v.pix_base + pix] = make_uint4(h.checks, h.status == kHit ? h.material : 0u,
                                               h.status == kHit ? h.id : 0u, vid);
         if (v.flags & VE_FRAME_SCHEDULED)  // paths come from the shade list: keep the hit
-            a.hitinfo[v.pix_base + pix] = make_uint4(h.id, h.x | (h.y << 16), h.z | (h.material << 16), 0u);
+            a.hitinfo[v.pix_base + pix] = make_uint4(word, h.x | (h.y << 16), h.z | (h.material << 16), 0u);
     }
     const bool spawn = inside && vid != 0u && !(v.flags & VE_FRAME_SCHEDULED);
     if (FUSED && !(v.flags & VE_FRAME_SCHEDULED)) {
@@ -739,7 +749,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
             const bool sp = __shfl_sync(0xffffffffu, spawn ? 1 : 0, int(src)) != 0;
             const uint32_t svid = __shfl_sync(0xffffffffu, vid, int(src));
             const uint32_t spix = __shfl_sync(0xffffffffu, pix, int(src));
-            const uint32_t sid = __shfl_sync(0xffffffffu, h.id, int(src));
+            const uint32_t sword = __shfl_sync(0xffffffffu, word, int(src));
             const uint32_t sxy = __shfl_sync(0xffffffffu, hxy, int(src));
             const uint32_t szm = __shfl_sync(0xffffffffu, hzm, int(src));
             const f3 sdir = mk(__shfl_sync(0xffffffffu, dir.x, int(src)), __shfl_sync(0xffffffffu, dir.y, int(src)),
@@ -752,7 +762,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
                 const uint32_t sample_idx = v.frame_index + spix * 2654435761u + list_idx * 1442695040u;
                 const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
                 shade_step(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
-                           mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sid, sxy, szm), o);
+                           mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o);
             }
             shade_emit(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
                        dep + (threadIdx.x & ~31u), n_ext, n_sh);
@@ -773,7 +783,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
             a.p_tp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
             a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.p_hit[p] = make_uint4(kHit, h.id, h.x | (h.y << 16), h.z | (h.material << 16));
+            a.p_hit[p] = make_uint4(kHit, word, h.x | (h.y << 16), h.z | (h.material << 16));
             a.p_meta[p] = make_uint4(vid, rng, vi + a.view_offset, pix);
             a.live[0][q + s] = uint32_t(p);
         }
@@ -806,15 +816,16 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
         ShadeOut o;
         if (valid) {
             const uint4 meta = a.p_meta[p];
+            const float4 pe = a.p_pend[p];  // read with the rest: no load waits on the flags
             const uint32_t flags = meta.z >> 24;
             f3 direct = ld3(a.p_direct[p]);
             f3 indirect = ld3(a.p_indirect[p]);
-            if (flags & F_PENDING) {
-                if (a.p_vis[p]) {
-                    const float4 pe = a.p_pend[p];
-                    if (pe.w == 0.0f) direct = add(direct, ld3(pe));
-                    else indirect = add(indirect, ld3(pe));
-                }
+            if ((flags & F_PENDING) && pe.w != 0.0f) {
+                // the sun term belongs to the bounce that cast the shadow ray:
+                // the stored one when the path ended there, else the one before
+                const uint32_t b = (meta.z >> 16) & 0xFFu;
+                if (((flags & F_TERM) ? b : b - 1u) == 0u) direct = add(direct, ld3(pe));
+                else indirect = add(indirect, ld3(pe));
             }
             const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
             shade_step(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
@@ -1349,7 +1360,6 @@ struct ve_ctx {
     int staging_next = 0;
     ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
     ve::DevBuf<uint4> p_hit, p_meta;
-    ve::DevBuf<uint8_t> p_vis;
     ve::DevBuf<uint32_t> p_aux;  // training sample slot per path (learned-cache training frames)
     // importance-aware scheduling: primary hits, voxel claim table (key,
     // representative pixel, pixel count), per-pixel path counts and their
@@ -1606,14 +1616,14 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
     int rc = 0;
     const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->p_ray_o.p,
                             c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p, c->p_pend.p, c->p_hit.p,
-                            c->p_meta.p, c->p_vis.p, c->live0.p, c->live1.p, c->rayq.p, c->d_views.p};
+                            c->p_meta.p, c->live0.p, c->live1.p, c->rayq.p, c->d_views.p};
     struct GenBump {
         ve_ctx* c;
         const void* const* before;
         ~GenBump() {
             const void* after[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p,
                                    c->p_ray_o.p, c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p,
-                                   c->p_pend.p, c->p_hit.p, c->p_meta.p, c->p_vis.p, c->live0.p, c->live1.p,
+                                   c->p_pend.p, c->p_hit.p, c->p_meta.p, c->live0.p, c->live1.p,
                                    c->rayq.p, c->d_views.p};
             for (size_t i = 0; i < sizeof(after) / sizeof(after[0]); i++)
                 if (after[i] != before[i]) { c->gen++; break; }
@@ -1624,7 +1634,7 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
         return rc;
     if ((rc = c->p_ray_o.ensure(paths)) || (rc = c->p_ray_d.ensure(paths)) || (rc = c->p_tp.ensure(paths)) ||
         (rc = c->p_direct.ensure(paths)) || (rc = c->p_indirect.ensure(paths)) || (rc = c->p_pend.ensure(paths)) ||
-        (rc = c->p_hit.ensure(paths)) || (rc = c->p_meta.ensure(paths)) || (rc = c->p_vis.ensure(paths)) ||
+        (rc = c->p_hit.ensure(paths)) || (rc = c->p_meta.ensure(paths)) ||
         (rc = c->live0.ensure(paths)) || (rc = c->live1.ensure(paths)) || (rc = c->rayq.ensure(paths * 2)))
         return rc;
     if ((rc = c->d_views.ensure(n_views))) return rc;
@@ -1855,7 +1865,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.mats = c->d_mats.p;
     a.p_ray_o = c->p_ray_o.p; a.p_ray_d = c->p_ray_d.p; a.p_tp = c->p_tp.p;
     a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
-    a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p; a.p_vis = c->p_vis.p;
+    a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p;
     a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p;
     a.counters = c->counters.p; a.stats = c->stats.p;
     a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
@@ -2204,7 +2214,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
     c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
-    c->p_indirect.release(); c->p_pend.release(); c->p_hit.release(); c->p_meta.release(); c->p_vis.release();
+    c->p_indirect.release(); c->p_pend.release(); c->p_hit.release(); c->p_meta.release();
     c->live0.release(); c->live1.release(); c->rayq.release(); c->counters.release(); c->stats.release();
     c->p_aux.release();
     c->hitinfo.release(); c->claim.release(); c->sched_n.release(); c->shade_list.release(); c->scan_tmp.release();

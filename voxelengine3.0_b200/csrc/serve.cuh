@@ -139,7 +139,7 @@ static FrameArgs serve_args(ve_server* s) {
     a.mats = c->d_mats.p;
     a.p_ray_o = c->p_ray_o.p; a.p_ray_d = c->p_ray_d.p; a.p_tp = c->p_tp.p;
     a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
-    a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p; a.p_vis = c->p_vis.p;
+    a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p;
     a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p;
     a.counters = c->counters.p; a.stats = c->stats.p;
     a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
@@ -407,7 +407,7 @@ int ve_server_get_stats(ve_server* s, ve_server_stats* out) {
     out->in_flight = s->active.size();
     out->max_in_flight = s->max_inflight;
     out->steps = s->steps_run;
-    out->pool_bytes = s->pix_pool.capacity() * 48ull + s->path_pool.capacity() * 145ull;
+    out->pool_bytes = s->pix_pool.capacity() * 48ull + s->path_pool.capacity() * 144ull;
     uint64_t scene_bytes = 0;
     for (const auto& sc : s->c->scenes)
         if (sc.live)
