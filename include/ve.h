@@ -46,6 +46,8 @@ extern "C" {
 #define VE_FRAME_LEARNED 8u       /* end paths at their second vertex with the scene's learned cache */
 #define VE_FRAME_TERMINATE_HASH 16u /* end paths at their second vertex with the hashed per-voxel cache */
 #define VE_FRAME_TRAIN 32u        /* record training samples and train the scene's learned cache */
+#define VE_FRAME_EMISSIVE 128u    /* NEE toward the scene's emissive voxels instead of the sun: light
+                                     registry, single-pick RIS and ReSTIR DI (shade.comp:576-836) */
 #define VE_FRAME_SCHEDULED 64u    /* importance-aware voxel scheduling (schedule/rank/threshold.comp)
                                      in place of spp paths per pixel; single-view calls */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
@@ -86,7 +88,17 @@ typedef struct ve_frame_config {
     float mid_fraction;             /* 0.40: voxels given 1 path */
     uint32_t min_samples;           /* 1: paths of the remaining voxels */
     uint32_t shading_budget;        /* 131072: cap on paths per frame */
+    /* emissive NEE (VE_FRAME_EMISSIVE), ReSTIR DI knobs of core.hpp:138-144 */
+    uint32_t restir;                  /* VE_RESTIR_* bits; all three by default */
+    uint32_t restir_m;                /* 4: initial RIS candidates (<= 64) */
+    uint32_t restir_spatial_neighbors;/* 1 (at most 6 are used) */
+    uint32_t restir_max_m;            /* 24: history cap on reuse */
+    float restir_spatial_radius;      /* 2.75: neighbour offset in voxels */
 } ve_frame_config;
+
+#define VE_RESTIR_ENABLE 1u   /* ReSTIR DI at bounce 0 (else single-pick RIS there too) */
+#define VE_RESTIR_TEMPORAL 2u /* reuse the voxel's reservoir from earlier frames */
+#define VE_RESTIR_SPATIAL 4u  /* reuse neighbour voxels' reservoirs */
 
 /* One render request: scene, Camera::UBO (camera.hpp:24-29: position,
  * cameraPlane, cameraPlaneRight, cameraPlaneUp as 4 x vec4) and frame knobs. */
@@ -133,6 +145,9 @@ typedef struct ve_frame_stats {
     uint64_t scheduled_paths;     /* VE_FRAME_SCHEDULED: shade-list entries (paths) */
     float ms_learned;             /* learned-cache inference + training (VE_FRAME_TIMING) */
     uint32_t reserved;
+    uint64_t emissive_lights;     /* VE_FRAME_EMISSIVE: registered lights after the call */
+    uint64_t nee_emissive;        /* VE_FRAME_EMISSIVE: NEE shadow rays toward lights */
+    uint64_t restir_commits;      /* VE_FRAME_EMISSIVE: voxel reservoirs stored */
 } ve_frame_stats;
 
 typedef struct ve_ctx ve_ctx;

@@ -33,13 +33,16 @@ class FrameParams(ctypes.Structure):
                 ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", _U32),
                 ("weight_pixels", ctypes.c_float), ("weight_variance", ctypes.c_float),
                 ("pixels_norm", ctypes.c_float), ("top_fraction", ctypes.c_float), ("mid_fraction", ctypes.c_float),
-                ("min_samples", _U32), ("shading_budget", _U32)]
+                ("min_samples", _U32), ("shading_budget", _U32),
+                ("restir", _U32), ("restir_m", _U32), ("restir_spatial_neighbors", _U32), ("restir_max_m", _U32),
+                ("restir_spatial_radius", ctypes.c_float)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("rays_primary", _U64), ("rays_bounce", _U64), ("rays_shadow", _U64), ("fetch_restart", _U64),
                 ("fetch_min", _U64), ("paths", _U64), ("deposits", _U64), ("steps", _U64),
-                ("scheduled_voxels", _U64), ("scheduled_paths", _U64)]
+                ("scheduled_voxels", _U64), ("scheduled_paths", _U64),
+                ("emissive_lights", _U64), ("nee_emissive", _U64), ("restir_commits", _U64)]
 
 
 def build_oracle(force: bool = False) -> str:
@@ -76,6 +79,7 @@ class Oracle:
                                      _np(np.uint32), _P]
         L.oracle_raycast_batch.argtypes = [_np(np.uint32), _U64, _U32, _np(np.float32), _np(np.float32), _U64, _U32,
                                            _U32, _np(np.uint32)]
+        L.oracle_pow_unit.argtypes = [_np(np.float32), _np(np.float32), _U64, _np(np.float32)]
         L.oracle_voxel_key.restype = _U32
         L.oracle_voxel_key.argtypes = [_U32, _U32, _U32]
         L.oracle_rand_seq.restype = _U32
@@ -133,6 +137,13 @@ class Oracle:
         out = np.zeros((o.shape[0], 8), np.uint32)
         self.lib.oracle_raycast_batch(w, w.size, depth, o.reshape(-1), d.reshape(-1), o.shape[0], controlchecks,
                                       threads, out.reshape(-1))
+        return out
+
+    def pow_unit(self, x, e) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        e = np.ascontiguousarray(e, np.float32)
+        out = np.zeros_like(x)
+        self.lib.oracle_pow_unit(x, e, x.size, out)
         return out
 
     def voxel_key(self, x, y, z) -> int:
@@ -299,11 +310,15 @@ def frame_params(fc) -> FrameParams:
     p.variance_norm = float(fc.variance_norm)
     for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction"):
         setattr(p, f, float(getattr(fc, f, FrameParams_defaults[f])))
-    for f in ("min_samples", "shading_budget"):
+    for f in ("min_samples", "shading_budget", "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m"):
         setattr(p, f, int(getattr(fc, f, FrameParams_defaults[f])))
+    p.restir_spatial_radius = float(getattr(fc, "restir_spatial_radius", FrameParams_defaults["restir_spatial_radius"]))
     return p
 
 
 # core.hpp:95-112 scheduling defaults, for frame configs without those fields
 FrameParams_defaults = {"weight_pixels": 0.1, "weight_variance": 0.9, "pixels_norm": 100.0, "top_fraction": 0.30,
-                        "mid_fraction": 0.40, "min_samples": 1, "shading_budget": 131072}
+                        "mid_fraction": 0.40, "min_samples": 1, "shading_budget": 131072,
+                        # core.hpp:138-144 ReSTIR defaults (enable | temporal | spatial)
+                        "restir": 7, "restir_m": 4, "restir_spatial_neighbors": 1, "restir_max_m": 24,
+                        "restir_spatial_radius": 2.75}

@@ -30,6 +30,7 @@
 #include <thread>
 #include <tuple>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 namespace {
@@ -283,6 +284,49 @@ struct Material {
 };
 static_assert(sizeof(Material) == 64, "material stride");
 
+// x^e for x in (0, 1], e > 0: exp2(e log2 x) with the atanh series of the
+// mantissa's logarithm and the Taylor series of 2^f (explicit fma), the same
+// operation sequence as the device's pow_unit; results below 2^-125 are 0.
+inline float pow_unit(float x, float e) {
+    if (x != x) return x;  // NaN stays NaN
+    uint32_t bits;
+    std::memcpy(&bits, &x, 4);
+    int ex = int(bits >> 23) - 127;
+    const uint32_t mb = (bits & 0x007FFFFFu) | 0x3F800000u;
+    float m;
+    std::memcpy(&m, &mb, 4);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        ex += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = std::fmaf(s2, 0.0769230769f, 0.0909090909f);
+    p = std::fmaf(s2, p, 0.111111111f);
+    p = std::fmaf(s2, p, 0.142857143f);
+    p = std::fmaf(s2, p, 0.2f);
+    p = std::fmaf(s2, p, 0.333333333f);
+    const float lnm = 2.0f * std::fmaf(s * s2, p, s);
+    const float y = e * (float(ex) + lnm * 1.44269504f);
+    if (!(y > -125.0f)) return 0.0f;
+    const float n = std::floor(y + 0.5f);
+    const float t = (y - n) * 0.693147181f;
+    float q = std::fmaf(t, 2.48015873e-5f, 1.98412698e-4f);
+    q = std::fmaf(t, q, 1.38888889e-3f);
+    q = std::fmaf(t, q, 8.33333333e-3f);
+    q = std::fmaf(t, q, 4.16666667e-2f);
+    q = std::fmaf(t, q, 0.166666667f);
+    q = std::fmaf(t, q, 0.5f);
+    q = std::fmaf(t, q, 1.0f);
+    q = std::fmaf(t, q, 1.0f);
+    uint32_t qb;
+    std::memcpy(&qb, &q, 4);
+    qb += uint32_t(int(n)) << 23;
+    float r;
+    std::memcpy(&r, &qb, 4);
+    return r;
+}
+
 // EvaluateBRDF (internal.glsl:120-149)
 inline f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float roughness, float metallic,
                         float specular_intensity) {
@@ -293,7 +337,7 @@ inline f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float roughness, float meta
     const f3 H = normalize(sub(L, V));
     const float NdotH = gmax(dot(N, H), 0.001f);
     const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
-    const float specular = spec_norm * std::pow(NdotH, spec_exp);
+    const float specular = spec_norm * pow_unit(NdotH, spec_exp);
     const float kS = specular_intensity * metallic;
     const float kD = 1.0f - kS * 0.5f;
     const f3 diffuse = muls(muls(albedo, kD), 0.31831f);
@@ -525,13 +569,295 @@ struct PathOut {
     f3 direct{0, 0, 0}, indirect{0, 0, 0};
 };
 
+// ---------------------------------------------------------------------------
+// Emissive NEE (shade.comp:576-836): the light registry, the single-pick RIS
+// estimator and ReSTIR DI with per-voxel reservoirs, under the product's
+// deterministic rules: lights seen by a frame's primary hits join the
+// registry at the end of the frame (sorted by vid, up to 4096), reservoirs
+// are read as committed by earlier frames and each voxel keeps the reservoir
+// of its frame's largest path slot.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kEmCapacity = 4096;  // EMISSIVE_CAPACITY (wavefront.glsl:109)
+constexpr uint32_t kFrameEmissive = 128;  // VE_FRAME_EMISSIVE
+constexpr uint32_t kRestirEnable = 1, kRestirTemporal = 2, kRestirSpatial = 4;
+
+struct EmLight {  // EmissiveVoxel (wavefront.glsl:91-96)
+    float e[3];
+    uint32_t vid;
+    uint32_t pos[3];
+    uint32_t size;
+};
+struct Reservoir {  // shade.comp:296-303
+    uint32_t light_idx = 0, light_vid = 0, seed = 0;
+    float wsum = 0.0f;
+    uint32_t m = 0;
+    float target = 0.0f;
+};
+struct ResRecord {
+    uint32_t vid, slot;
+    Reservoir r;
+};
+// A frame's emissive-NEE inputs (the registry and reservoirs as the frame
+// began) and one thread's outputs.
+struct EmFrame {
+    const std::vector<EmLight>* lights = nullptr;
+    const std::unordered_map<uint32_t, Reservoir>* res = nullptr;
+    std::vector<EmLight> staged;
+    std::vector<ResRecord> records;
+    uint64_t nee = 0;
+};
+
+inline float luminance(const float e[3]) { return (e[0] * 0.2126f + e[1] * 0.7152f) + e[2] * 0.0722f; }
+
+// rUpdate / rCombine / rCapHistory (shade.comp:316-370)
+inline void r_update(Reservoir& r, uint32_t li, uint32_t lv, uint32_t seed, float target, float w, uint32_t& rng) {
+    if (w <= 0.0f) {
+        r.m += 1u;
+        return;
+    }
+    r.wsum += w;
+    r.m += 1u;
+    if (rand01(rng) * r.wsum < w) {
+        r.light_idx = li;
+        r.light_vid = lv;
+        r.seed = seed;
+        r.target = target;
+    }
+}
+inline void r_combine(Reservoir& a, const Reservoir& b, float target_at_us, uint32_t& rng) {
+    if (b.m == 0u || b.target <= 0.0f || target_at_us <= 0.0f) return;
+    const float w = target_at_us * b.wsum / b.target;
+    a.wsum += w;
+    a.m += b.m;
+    if (rand01(rng) * a.wsum < w) {
+        a.light_idx = b.light_idx;
+        a.light_vid = b.light_vid;
+        a.seed = b.seed;
+        a.target = target_at_us;
+    }
+}
+inline void r_cap(Reservoir& r, uint32_t max_m) {
+    if (r.m > max_m && max_m > 0u) {
+        r.wsum = r.wsum * float(max_m) / float(r.m);
+        r.m = max_m;
+    }
+}
+// packFaceSeed (shade.comp:376-380)
+inline uint32_t pack_face_seed(uint32_t face, float u, float v) {
+    const uint32_t ui = uint32_t(gclamp(u, 0.0f, 0.9999f) * 16383.0f);
+    const uint32_t vi = uint32_t(gclamp(v, 0.0f, 0.9999f) * 16383.0f);
+    return (face & 0xFu) | ((ui & 0x3FFFu) << 4) | ((vi & 0x3FFFu) << 18);
+}
+// face normal and tangents (shade.comp:397-407)
+inline void face_frame(uint32_t face, f3& n, f3& t, f3& b) {
+    if (face < 2u) {
+        n = mk(face == 0u ? 1.0f : -1.0f, 0, 0); t = mk(0, 1, 0); b = mk(0, 0, 1);
+    } else if (face < 4u) {
+        n = mk(0, face == 2u ? 1.0f : -1.0f, 0); t = mk(1, 0, 0); b = mk(0, 0, 1);
+    } else {
+        n = mk(0, 0, face == 4u ? 1.0f : -1.0f); t = mk(1, 0, 0); b = mk(0, 1, 0);
+    }
+}
+// fCenter + fNormal*halfSize + (u-0.5)*2*halfSize*fT + (v-0.5)*2*halfSize*fB
+// (shade.comp:408-414, 798-804)
+inline f3 face_point(const EmLight& L, f3 n, f3 t, f3 b, float u, float v) {
+    const float hs = float(L.size) * 0.5f;
+    const f3 c = add(mk(float(L.pos[0]), float(L.pos[1]), float(L.pos[2])), mk(hs, hs, hs));
+    const f3 p = add(c, muls(n, hs));
+    const f3 q = add(p, muls(t, ((u - 0.5f) * 2.0f) * hs));
+    return add(q, muls(b, ((v - 0.5f) * 2.0f) * hs));
+}
+// unpackLightSamplePoint (shade.comp:392-415)
+inline void light_sample_point(uint32_t seed, const EmLight& L, f3& P, f3& N) {
+    uint32_t face = seed & 0xFu;
+    const float u = float((seed >> 4) & 0x3FFFu) / 16383.0f;
+    const float v = float((seed >> 18) & 0x3FFFu) / 16383.0f;
+    if (face > 5u) face = 5u;
+    f3 t, b;
+    face_frame(face, N, t, b);
+    P = face_point(L, N, t, b, u, v);
+}
+// computeTargetPdf (shade.comp:420-435)
+inline float target_pdf(const EmLight& L, uint32_t seed, f3 sp, f3 n) {
+    f3 P, N;
+    light_sample_point(seed, L, P, N);
+    const f3 to = sub(P, sp);
+    const float d2 = dot(to, to);
+    if (d2 < 1e-6f) return 0.0f;
+    const float dist = std::sqrt(d2);
+    const f3 ld = divs(to, dist);
+    const float cx = dot(n, ld);
+    if (cx <= 0.0f) return 0.0f;
+    const float cy = dot(mk(-ld.x, -ld.y, -ld.z), N);
+    if (cy <= 0.0f) return 0.0f;
+    const float lum = gmax(luminance(L.e), 1e-6f);
+    const float area = 6.0f * float(L.size * L.size);
+    return ((lum * cy) * area) / d2;
+}
+// neighbourVid (shade.comp:521-531)
+inline uint32_t neighbour_vid(const uint32_t pos[3], uint32_t size, int ox, int oy, int oz) {
+    const int px = int(pos[0]) + ox * int(size), py = int(pos[1]) + oy * int(size), pz = int(pos[2]) + oz * int(size);
+    if (px < 0 || py < 0 || pz < 0) return 0u;
+    const uint32_t m = ~(size - 1u);
+    const uint32_t sx = uint32_t(px) & m, sy = uint32_t(py) & m, sz = uint32_t(pz) & m;
+    const uint32_t p = (sx & 0x3FFu) | ((sy & 0x3FFu) << 10) | ((sz & 0x3FFu) << 20);
+    return (hash32(p) & 0x7FFFFFFFu) + 1u;
+}
+// rBufferLoad + lightStillValid (shade.comp:441-515)
+inline bool res_load(const EmFrame& em, uint32_t vid, Reservoir& r) {
+    auto it = em.res->find(vid);
+    if (it == em.res->end()) return false;
+    r = it->second;
+    const uint32_t n = uint32_t(std::min<size_t>(em.lights->size(), kEmCapacity));
+    if (r.m == 0u || r.light_idx >= n) return false;
+    return (*em.lights)[r.light_idx].vid == r.light_vid;
+}
+inline f3 clamp_contrib(f3 c) { return mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f)); }
+
+// NEE toward the registered lights at a non-emissive hit of bounce b < 2;
+// the shadow ray must hit the light's voxel (RaycastVisibilityToVoxel,
+// internal.glsl:406-410).  Adds to direct (b == 0) or indirect radiance.
+void emissive_nee(const Scene& s, const ov_frame_params& P, EmFrame& em, uint32_t slot, uint32_t primary_vid,
+                  uint32_t b, const Hit& hit, f3 N, f3 sp, f3 dir, f3 tp, f3 albedo, const Material& m,
+                  uint32_t& rng, f3& direct, f3& indirect, ov_stats* st, RayCounters* rc) {
+    const std::vector<EmLight>& lights = *em.lights;
+    const uint32_t n_lights = uint32_t(std::min<size_t>(lights.size(), kEmCapacity));
+    if (n_lights == 0u) return;
+    bool have = false;
+    f3 contrib{0, 0, 0}, ld{0, 0, 0};
+    uint32_t target_vid = 0;
+    if ((P.restir & kRestirEnable) && b == 0u) {
+        Reservoir res;
+        const uint32_t n_m = std::max(P.restir_m, 1u);
+        const float inv_src = float(n_lights) * 6.0f;
+        for (uint32_t k = 0; k < n_m; k++) {
+            uint32_t pick = uint32_t(rand01(rng) * float(n_lights));
+            if (pick >= n_lights) pick = n_lights - 1u;
+            const EmLight& cand = lights[pick];
+            uint32_t face = uint32_t(rand01(rng) * 6.0f);
+            if (face >= 6u) face = 5u;
+            const float uu = rand01(rng);
+            const float vv = rand01(rng);
+            const uint32_t seed = pack_face_seed(face, uu, vv);
+            const float target = target_pdf(cand, seed, sp, N);
+            r_update(res, pick, cand.vid, seed, target, target * inv_src, rng);
+        }
+        if (P.restir & kRestirTemporal) {
+            Reservoir t;
+            if (res_load(em, primary_vid, t)) {
+                r_cap(t, P.restir_max_m);
+                r_combine(res, t, t.target, rng);
+            }
+        }
+        if ((P.restir & kRestirSpatial) && P.restir_spatial_neighbors > 0u) {
+            const f3 up = std::fabs(N.z) < 0.999f ? mk(0, 0, 1) : mk(1, 0, 0);
+            const f3 T = normalize(cross(up, N));
+            const f3 B = cross(N, T);
+            const uint32_t K = std::min(P.restir_spatial_neighbors, 6u);
+            for (uint32_t k = 0; k < K; k++) {
+                const float ua = rand01(rng);
+                const float rr = P.restir_spatial_radius * std::sqrt(rand01(rng));
+                float sn, cs;
+                sincos_turn(ua, &sn, &cs);
+                const f3 off = muls(add(muls(T, cs), muls(B, sn)), rr);
+                const int ox = int(std::round(off.x)), oy = int(std::round(off.y)), oz = int(std::round(off.z));
+                if (ox == 0 && oy == 0 && oz == 0) continue;
+                const uint32_t nvid = neighbour_vid(hit.pos, 1u, ox, oy, oz);
+                if (nvid == 0u || nvid == primary_vid) continue;
+                Reservoir nb;
+                if (!res_load(em, nvid, nb)) continue;
+                const float tu = target_pdf(lights[nb.light_idx], nb.seed, sp, N);
+                if (tu <= 0.0f) continue;
+                r_cap(nb, P.restir_max_m);
+                r_combine(res, nb, tu, rng);
+            }
+        }
+        if (res.m > 0u && res.target > 0.0f) {
+            const EmLight& L = lights[res.light_idx];
+            if (L.vid == res.light_vid) {
+                f3 LP, LN;
+                light_sample_point(res.seed, L, LP, LN);
+                const f3 to = sub(LP, sp);
+                const float d2 = dot(to, to);
+                const float dist = std::sqrt(gmax(d2, 1e-12f));
+                if (dist > 1e-3f) {
+                    const f3 l = divs(to, dist);
+                    const float cx = gmax(dot(N, l), 0.0f);
+                    const float cy = gmax(dot(mk(-l.x, -l.y, -l.z), LN), 0.0f);
+                    if (cx > 0.0f && cy > 0.0f) {
+                        const f3 brdf = evaluate_brdf(dir, l, N, albedo, m.roughness, m.metallic, m.specular);
+                        const float W = res.wsum / (float(res.m) * res.target);
+                        const float sz2 = float(L.size * L.size);
+                        const float geom = cy / gmax(d2, 1e-6f);
+                        contrib = clamp_contrib(muls(muls(muls(mul(mk(L.e[0], L.e[1], L.e[2]), brdf), geom), sz2), W));
+                        ld = l;
+                        target_vid = L.vid;
+                        have = true;
+                    }
+                }
+            }
+        }
+        if (res.m > 0u) em.records.push_back(ResRecord{primary_vid, slot, res});
+    } else {
+        float wsum = 0.0f, chosen_t = 0.0f;
+        uint32_t chosen = 0u;
+        for (int k = 0; k < 4; k++) {
+            uint32_t pick = uint32_t(rand01(rng) * float(n_lights));
+            if (pick >= n_lights) pick = n_lights - 1u;
+            const EmLight& cand = lights[pick];
+            const float lum = gmax(luminance(cand.e), 1e-6f);
+            const float target = lum * float(cand.size * cand.size);
+            wsum += target;
+            if (rand01(rng) * wsum < target) {
+                chosen = pick;
+                chosen_t = target;
+            }
+        }
+        const float avg_t = wsum / 4.0f;
+        const EmLight& L = lights[chosen];
+        uint32_t face = uint32_t(rand01(rng) * 6.0f);
+        if (face >= 6u) face = 5u;
+        f3 fn, ft, fb;
+        face_frame(face, fn, ft, fb);
+        const float u1 = rand01(rng);
+        const float u2 = rand01(rng);
+        const f3 lp = face_point(L, fn, ft, fb, u1, u2);
+        f3 l = sub(lp, sp);
+        const float d2 = dot(l, l);
+        const float dist = std::sqrt(d2);
+        if (dist > 1e-3f && chosen_t > 0.0f) {
+            l = divs(l, dist);
+            const float cx = gmax(dot(N, l), 0.0f);
+            const float cy = gmax(dot(mk(-l.x, -l.y, -l.z), fn), 0.0f);
+            if (cx > 0.0f && cy > 0.0f) {
+                const f3 brdf = evaluate_brdf(dir, l, N, albedo, m.roughness, m.metallic, m.specular);
+                const float area = 6.0f * float(L.size) * float(L.size);
+                const float ris = float(n_lights) * avg_t / gmax(chosen_t, 1e-6f);
+                const float geom = cy / gmax(d2, 1e-6f);
+                contrib = clamp_contrib(muls(muls(muls(mul(mk(L.e[0], L.e[1], L.e[2]), brdf), geom), area), ris));
+                ld = l;
+                target_vid = L.vid;
+                have = true;
+            }
+        }
+    }
+    if (!have) return;
+    const Hit sh = raycast(s, sp, ld, P.bounce_controlchecks, rc);
+    st->rays_shadow++;
+    em.nee++;
+    if (sh.status == ST_HIT && voxel_key(sh.pos) + 1u == target_vid) {
+        const f3 w = mul(tp, contrib);
+        if (b == 0) direct = add(direct, w); else indirect = add(indirect, w);
+    }
+}
+
 // The per-pixel plain method: one path of the bounce/shade loop
 // (shade.comp:543-575, 838-908) from a known primary hit, with the sun
 // next-event estimate in the place of the emissive NEE (shade.comp:631-836 is
 // dormant in scenes without emissive voxels).
 void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_frame_params& P,
                 const Hit& primary, f3 primary_dir, uint32_t pix_index, uint32_t list_idx, PathOut* out,
-                ov_stats* st, RayCounters* rc) {
+                ov_stats* st, RayCounters* rc, EmFrame* em = nullptr) {
     const uint32_t max_bounces = P.bounces + 1u;  // MAX_BOUNCES (wavefront.glsl:23)
     // emit.comp:171-174; list_idx is pixel * spp + sample in the per-pixel
     // method and the shade-list index in the scheduled one
@@ -558,12 +884,19 @@ void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_
             f3 e = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
             e = mk(gmin(e.x, 20.0f), gmin(e.y, 20.0f), gmin(e.z, 20.0f));
             if (b == 0) direct = add(direct, e); else indirect = add(indirect, e);
+            if (em && b == 0)  // a light seen by a primary ray (shade.comp:585-613)
+                em->staged.push_back(EmLight{{albedo.x * k, albedo.y * k, albedo.z * k}, voxel_key(hit.pos) + 1u,
+                                             {hit.pos[0], hit.pos[1], hit.pos[2]}, 1u});
         }
         const f3 hit_pos = mk(float(hit.pos[0]), float(hit.pos[1]), float(hit.pos[2]));
         const f3 shading_point = add(add(hit_pos, mk(0.5f, 0.5f, 0.5f)), N);  // shade.comp:635, 892
-        // NEE gate of shade.comp:631 (non-emissive surface, bounce < 2), with
-        // the sun's cosine test of shade.comp:811-815.
-        if (!m.emissive && b < 2u && dot(N, sun) > 0.0f) {
+        if (em) {
+            if (!m.emissive && b < 2u)
+                emissive_nee(s, P, *em, list_idx, voxel_key(primary.pos) + 1u, b, hit, N, shading_point, dir, tp,
+                             albedo, m, rng, direct, indirect, st, rc);
+        } else if (!m.emissive && b < 2u && dot(N, sun) > 0.0f) {
+            // NEE gate of shade.comp:631 (non-emissive surface, bounce < 2),
+            // with the sun's cosine test of shade.comp:811-815
             const Hit sh = raycast(s, shading_point, sun, P.bounce_controlchecks, rc);
             st->rays_shadow++;
             if (sh.status == ST_ESCAPED) {
@@ -661,7 +994,35 @@ struct Renderer {
     Cache cache;
     float t_high = std::numeric_limits<float>::infinity();
     float t_mid = -std::numeric_limits<float>::infinity();
+    // emissive frames: the light registry, the vids it has claimed (kept or
+    // dropped at capacity) and the committed per-voxel reservoirs
+    std::vector<EmLight> lights;
+    std::unordered_set<uint32_t> em_claimed;
+    std::unordered_map<uint32_t, Reservoir> res;
 };
+
+// End of an emissive frame: new lights in vid order fill the registry up to
+// its capacity (all of them stay claimed); each voxel keeps the reservoir of
+// its largest path slot.
+void commit_emissive(Renderer* R, std::vector<EmFrame>& ems, ov_stats* total) {
+    std::vector<EmLight> fresh;
+    for (auto& em : ems)
+        for (const EmLight& L : em.staged)
+            if (R->em_claimed.insert(L.vid).second) fresh.push_back(L);
+    std::sort(fresh.begin(), fresh.end(), [](const EmLight& a, const EmLight& b) { return a.vid < b.vid; });
+    for (const EmLight& L : fresh)
+        if (R->lights.size() < kEmCapacity) R->lights.push_back(L);
+    std::unordered_map<uint32_t, const ResRecord*> win;
+    for (auto& em : ems)
+        for (const ResRecord& r : em.records) {
+            auto it = win.find(r.vid);
+            if (it == win.end() || it->second->slot < r.slot) win[r.vid] = &r;
+        }
+    for (auto& kv : win) R->res[kv.first] = kv.second->r;
+    total->emissive_lights = R->lights.size();
+    total->restir_commits = win.size();
+    for (auto& em : ems) total->nee_emissive += em.nee;
+}
 
 constexpr uint32_t kRankBins = 256;
 constexpr uint32_t kFrameScheduled = 64;  // VE_FRAME_SCHEDULED
@@ -700,7 +1061,7 @@ void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t 
                     const ov_frame_params* P, uint32_t threads, const std::vector<Hit>& hits,
                     const std::vector<uint32_t>& vids, float* path_rgb,
                     std::vector<std::vector<std::vector<Deposit>>>& deps, std::vector<ov_stats>& tstats,
-                    std::vector<RayCounters>& trc) {
+                    std::vector<RayCounters>& trc, std::vector<EmFrame>& ems) {
     const uint32_t W = P->width, H = P->height, npix = W * H;
     struct Claim { uint32_t pix, count; };
     std::unordered_map<uint32_t, Claim> claims;
@@ -764,7 +1125,8 @@ void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t 
             const uint32_t vid = list[i].first, pix = list[i].second;
             const f3 dir = pixel_dir(cam, pix % W, pix / W, W, H);
             PathOut po;
-            trace_path(s, mats, n_mats, *P, hits[pix], dir, pix, uint32_t(i), &po, &st, &trc[t]);
+            trace_path(s, mats, n_mats, *P, hits[pix], dir, pix, uint32_t(i), &po, &st, &trc[t],
+                       ems.empty() ? nullptr : &ems[t]);
             st.paths++;
             Deposit dp;
             dp.vid = vid;
@@ -939,6 +1301,12 @@ void oracle_raycast_batch(const uint32_t* words, uint64_t n_words, uint32_t dept
     for (auto& x : th) x.join();
 }
 
+// The specular lobe's power function, element-wise (pinned in tests against
+// float64 pow).
+void oracle_pow_unit(const float* x, const float* e, uint64_t n, float* out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = pow_unit(x[i], e[i]);
+}
+
 uint32_t oracle_voxel_key(uint32_t x, uint32_t y, uint32_t z) {
     const uint32_t p[3] = {x, y, z};
     return voxel_key(p);
@@ -1011,6 +1379,8 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     if (threads == 0) threads = 1;
     const bool sched = (P->flags & kFrameScheduled) != 0;
     if (sched && (row_begin != 0 || row_end != H)) return -1;  // the schedule spans the whole view
+    // emissive frames commit lights and reservoirs once per whole frame
+    if ((P->flags & kFrameEmissive) && (row_begin != 0 || row_end != H)) return -1;
     std::vector<Hit> hits(sched ? size_t(W) * H : 0);
     std::vector<uint32_t> vids(sched ? size_t(W) * H : 0, 0u);
 
@@ -1031,6 +1401,12 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     std::vector<std::vector<std::vector<Deposit>>> deps(threads, std::vector<std::vector<Deposit>>(kShards));
     std::vector<ov_stats> tstats(threads);
     std::vector<RayCounters> trc(threads);
+    // emissive frames: the registry and reservoirs as the frame begins
+    std::vector<EmFrame> ems((P->flags & kFrameEmissive) ? threads : 0);
+    for (auto& em : ems) {
+        em.lights = &R->lights;
+        em.res = &R->res;
+    }
     const uint32_t rows = row_end - row_begin;
     // static interleaved rows (row r -> thread r mod threads): balanced and
     // deterministic; deposits merge in thread order below
@@ -1063,7 +1439,8 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                 if (vid == 0) continue;
                 for (uint32_t smp = 0; smp < P->spp; smp++) {
                     PathOut po;
-                    trace_path(s, mats, n_mats, *P, h, dir, pix, pix * P->spp + smp, &po, &st, &trc[t]);
+                    trace_path(s, mats, n_mats, *P, h, dir, pix, pix * P->spp + smp, &po, &st, &trc[t],
+                               ems.empty() ? nullptr : &ems[t]);
                     st.paths++;
                     Deposit dp;
                     dp.vid = vid;
@@ -1084,7 +1461,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         for (uint32_t t = 0; t < threads; t++) th.emplace_back(work, t);
         for (auto& x : th) x.join();
     }
-    if (sched) schedule_frame(R, s, mats, n_mats, cam, P, threads, hits, vids, path_rgb, deps, tstats, trc);
+    if (sched) schedule_frame(R, s, mats, n_mats, cam, P, threads, hits, vids, path_rgb, deps, tstats, trc, ems);
     ov_stats total{};
     for (uint32_t t = 0; t < threads; t++) {
         total.rays_primary += tstats[t].rays_primary;
@@ -1098,6 +1475,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         total.scheduled_paths += tstats[t].scheduled_paths;
         for (uint32_t sh = 0; sh < kShards; sh++) total.deposits += deps[t][sh].size();
     }
+    if (!ems.empty()) commit_emissive(R, ems, &total);
     run_parallel(kShards, threads, [&](uint32_t sh) {
         auto& m = R->cache.map[sh];
         for (uint32_t t = 0; t < threads; t++)

@@ -34,6 +34,9 @@ struct ov_frame_params {
     /* importance-aware scheduling (flags & 64), core.hpp:95-112 */
     float weight_pixels, weight_variance, pixels_norm, top_fraction, mid_fraction;
     uint32_t min_samples, shading_budget;
+    /* emissive NEE (flags & 128), core.hpp:138-144 */
+    uint32_t restir, restir_m, restir_spatial_neighbors, restir_max_m;
+    float restir_spatial_radius;
 };
 
 struct ov_stats {
@@ -43,6 +46,7 @@ struct ov_stats {
     uint64_t paths, deposits;
     uint64_t steps;           // DDA outer iterations (all rays)
     uint64_t scheduled_voxels, scheduled_paths;  // scheduled frames
+    uint64_t emissive_lights, nee_emissive, restir_commits;  // emissive frames
 };
 
 }  // extern "C"

@@ -47,6 +47,10 @@ FRAME_LEARNED = 8
 FRAME_TERMINATE_HASH = 16
 FRAME_TRAIN = 32
 FRAME_SCHEDULED = 64
+FRAME_EMISSIVE = 128
+RESTIR_ENABLE = 1
+RESTIR_TEMPORAL = 2
+RESTIR_SPATIAL = 4
 RAYCAST_FULL_WALK = 1
 CFG_NO_GRAPHS = 1
 
@@ -74,7 +78,10 @@ class FrameConfigC(ctypes.Structure):
                 ("decay", ctypes.c_float), ("variance_norm", ctypes.c_float), ("flags", ctypes.c_uint32),
                 ("weight_pixels", ctypes.c_float), ("weight_variance", ctypes.c_float),
                 ("pixels_norm", ctypes.c_float), ("top_fraction", ctypes.c_float), ("mid_fraction", ctypes.c_float),
-                ("min_samples", ctypes.c_uint32), ("shading_budget", ctypes.c_uint32)]
+                ("min_samples", ctypes.c_uint32), ("shading_budget", ctypes.c_uint32),
+                ("restir", ctypes.c_uint32), ("restir_m", ctypes.c_uint32),
+                ("restir_spatial_neighbors", ctypes.c_uint32), ("restir_max_m", ctypes.c_uint32),
+                ("restir_spatial_radius", ctypes.c_float)]
 
 
 class ViewC(ctypes.Structure):
@@ -103,7 +110,9 @@ class FrameStatsC(ctypes.Structure):
                 ("cache_capacity", ctypes.c_uint64), ("nrc_queries", ctypes.c_uint64),
                 ("nrc_hash_terminated", ctypes.c_uint64), ("nrc_samples", ctypes.c_uint64),
                 ("scheduled_voxels", ctypes.c_uint64), ("scheduled_paths", ctypes.c_uint64),
-                ("ms_learned", ctypes.c_float), ("reserved", ctypes.c_uint32)]
+                ("ms_learned", ctypes.c_float), ("reserved", ctypes.c_uint32),
+                ("emissive_lights", ctypes.c_uint64), ("nee_emissive", ctypes.c_uint64),
+                ("restir_commits", ctypes.c_uint64)]
 
 
 class ServerConfigC(ctypes.Structure):
@@ -434,11 +443,18 @@ class FrameConfig:
     mid_fraction: float = 0.40
     min_samples: int = 1
     shading_budget: int = 131072
+    # emissive NEE (FRAME_EMISSIVE), core.hpp:138-144 ReSTIR defaults
+    restir: int = RESTIR_ENABLE | RESTIR_TEMPORAL | RESTIR_SPATIAL
+    restir_m: int = 4
+    restir_spatial_neighbors: int = 1
+    restir_max_m: int = 24
+    restir_spatial_radius: float = 2.75
 
     def to_c(self) -> FrameConfigC:
         c = FrameConfigC()
         for f in ("width", "height", "spp", "bounces", "primary_controlchecks", "bounce_controlchecks",
-                  "reconstruction_radius", "render_type", "frame_index", "flags", "min_samples", "shading_budget"):
+                  "reconstruction_radius", "render_type", "frame_index", "flags", "min_samples", "shading_budget",
+                  "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m"):
             setattr(c, f, int(getattr(self, f)))
         for i in range(3):
             c.sun_dir[i] = float(self.sun_dir[i])
@@ -446,7 +462,8 @@ class FrameConfig:
         c.sun_intensity = float(self.sun_intensity)
         c.decay = float(self.decay)
         c.variance_norm = float(self.variance_norm)
-        for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction"):
+        for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction",
+                  "restir_spatial_radius"):
             setattr(c, f, float(getattr(self, f)))
         return c
 

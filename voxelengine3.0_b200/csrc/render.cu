@@ -28,6 +28,7 @@
 
 #include "../../include/ve.h"
 #include "builder.cuh"
+#include "emissive.cuh"
 #include "nrc.cuh"
 #include "raycast.cuh"
 #include "ve_device.cuh"
@@ -56,6 +57,12 @@ struct DevScene {
     uint32_t probes;
     uint32_t top_level;   // T0: levels 0..T0-1 resolved by the top table (0: none)
     const uint32_t* top;  // top table, (2^(T0-1))^3 words
+    // emissive lights (VE_FRAME_EMISSIVE; null until the scene's first such frame)
+    EmLight* em_list;     // the registry, kEmCapacity records
+    uint32_t* em_claim;   // claim table of registered (or dropped) light vids
+    uint32_t* em_state;   // {registered lights, lights staged this frame}
+    EmLight* em_stage;    // lights found this frame, appended at its end
+    ResEntry* res;        // per-voxel ReSTIR reservoirs, 2^kResLog2 entries
 };
 
 struct DevMaterial {
@@ -78,12 +85,17 @@ struct DevView {
     // importance-aware scheduling (rank.comp knobs)
     float w_pix, w_var, pix_norm, top_frac, mid_frac;
     uint32_t min_samples, budget, pad1;
+    // emissive NEE / ReSTIR DI (core.hpp:138-144 knobs)
+    uint32_t restir, restir_m, restir_nbrs, restir_max_m;
+    float restir_radius;
+    uint32_t pad2, pad3, pad4;
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
 constexpr uint32_t kDefaultRefill = 24;  // trace refill threshold (idle lanes of 32)
 enum : uint32_t {
-    CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_TOTAL = 64
+    CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_RES = 63,
+    CNT_TOTAL = 64
 };
 enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
@@ -101,7 +113,10 @@ enum : uint32_t {
     ST_NRC_SAMPLES,  // training samples recorded
     ST_SCHED_VOXELS, // scheduled frames: distinct visible voxels
     ST_SCHED_PATHS,  // scheduled frames: shade-list entries
-    ST_TOTAL = 16
+    ST_EM_LIGHTS,    // emissive frames: registered lights after the frame
+    ST_EM_NEE,       // emissive frames: NEE shadow rays toward lights
+    ST_RES_WRITES,   // emissive frames: reservoirs committed
+    ST_TOTAL = 19
 };
 enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u };
 // a cached voxel average ends a path (VE_FRAME_TERMINATE_HASH, and the
@@ -123,7 +138,10 @@ struct FrameArgs {
     float4* p_tp;        // throughput
     float4* p_direct;    // direct radiance (sun at bounce 0, bounce-0 emission)
     float4* p_indirect;  // indirect radiance
-    float4* p_pend;      // pending sun contribution; w = 0, set to 1 by the shadow trace when the sun is visible
+    float4* p_pend;      // pending NEE contribution; w: the shadow trace's result code (~0 escaped, hit vid, 0)
+    float4* p_sdir;      // emissive batches: NEE shadow direction, w = the light's vid (~0 for the sun)
+    PathRes* p_res;      // emissive batches: a path's bounce-0 reservoir until the commit
+    uint32_t* res_list;  // paths holding a reservoir (counter CNT_RES)
     uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
     uint32_t* live[2];
@@ -152,7 +170,7 @@ struct FrameArgs {
     uint32_t nrc_ready;     // cells without validation samples use the network
     uint32_t* p_aux;        // per path: training sample slot
     // importance-aware scheduling (VE_FRAME_SCHEDULED, single view)
-    uint4* hitinfo;         // per pixel: {leaf slot, x | y << 16, z | material << 16, 0} of the primary hit
+    uint4* hitinfo;         // per pixel: {leaf word, x | y << 16, z | material << 16, 0} of the primary hit
     uint32_t* claim_key;    // per-frame voxel claim table (vid, 0 = free)
     uint32_t* claim_pix;    // canonical (smallest) pixel of the voxel
     uint32_t* claim_cnt;    // pixels that see the voxel
@@ -306,7 +324,8 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
 // the next queue entry (one warp-aggregated atomicAdd on a per-pass cursor
 // serves all idle lanes of the warp, once `refill` of them are idle or none is
 // busy), so warps stay full although ray lengths differ by 100x.
-template <bool COUNT>
+// EM: the batch has VE_FRAME_EMISSIVE views (shadow rays toward lights).
+template <bool COUNT, bool EM = false>
 __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = a.counters[CNT_RAY + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
@@ -346,7 +365,8 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                     top = S.top;
                     T0 = S.top_level;
                     const f3 o = ld3(a.p_ray_o[p]);
-                    const f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
+                    f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
+                    if (EM && (e >> 31) && (v.flags & VE_FRAME_EMISSIVE)) d = ld3(a.p_sdir[p]);
                     finished = dda_init(s, o, d, v.cc_bounce, D, h);
                     active = !finished;
                 } else {
@@ -361,7 +381,11 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
         if (finished) {
             const uint32_t p = e & 0x7FFFFFFFu;
             if (e >> 31) {
-                if (h.status == kEscaped) reinterpret_cast<float*>(a.p_pend + p)[3] = 1.0f;
+                // the shadow ray's result code: ~0 left the volume, a hit
+                // voxel's vid (emissive batches: the light must be the hit),
+                // else 0 (the record's initial value)
+                if (h.status == kEscaped) reinterpret_cast<uint32_t*>(a.p_pend + p)[3] = 0xFFFFFFFFu;
+                else if (EM && h.status == kHit) reinterpret_cast<uint32_t*>(a.p_pend + p)[3] = voxel_key(h.x, h.y, h.z) + 1u;
             } else {
                 // h.id holds the hit leaf's word: the shade pass needs no
                 // dependent load from the node array
@@ -455,16 +479,174 @@ struct ShadeOut {
     // learned cache: a query (its record parked in the path's ray slots until
     // the warp's append), a recorded training sample, a hash-cache ending
     bool want_q = false, sampled = false, hash_term = false;
+    bool app_res = false, em_nee = false;  // a reservoir to commit; an emissive NEE shadow ray
     float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
     uint32_t dvid = 0, dscene = 0, dview = 0;
 };
 
+__device__ __forceinline__ f3 clamp_contrib(f3 c) {
+    return mk(gmin(c.x, kMaxContrib), gmin(c.y, kMaxContrib), gmin(c.z, kMaxContrib));
+}
+
+// A NEE sample waiting for its shadow ray: the contribution (already times
+// the throughput) and the ray toward the light voxel `target`.
+__device__ __forceinline__ void nee_pending(const FrameArgs& a, uint32_t p, f3 contrib, f3 ld, uint32_t target,
+                                            uint32_t& nf, ShadeOut& o) {
+    a.p_pend[p] = st3(contrib, 0.0f);
+    a.p_sdir[p] = make_float4(ld.x, ld.y, ld.z, __uint_as_float(target));
+    nf |= F_PENDING;
+    o.app_sh = true;
+    o.em_nee = true;
+}
+
+// Next-event estimation toward the registered emissive voxels at a
+// non-emissive hit of bounce b < 2 (shade.comp:615-836): ReSTIR DI at
+// bounce 0 when enabled (initial RIS over restir_m uniform candidates,
+// temporal reuse of the voxel's reservoir, spatial reuse of neighbours',
+// one shadow ray on the chosen sample), else the single-pick RIS estimator
+// (4 power-weighted candidates, a uniform point on a uniform face).
+// `rng` continues the path's sequence; the bounce sampling draws after it.
+__device__ __forceinline__ void emissive_nee(const FrameArgs& a, const DevView& v, const DevScene& S, uint32_t p,
+                                             uint32_t primary_vid, uint32_t b, uint32_t hx, uint32_t hy, uint32_t hz,
+                                             f3 N, f3 sp, f3 dir, f3 tp, f3 albedo, float roughness, float metallic,
+                                             float spec, uint32_t& rng, uint32_t& nf, ShadeOut& o) {
+    const uint32_t n_lights = min(S.em_state[0], kEmCapacity);
+    if (n_lights == 0u) return;  // frame-0 pre-discovery
+    const EmLight* lights = S.em_list;
+    if ((v.restir & VE_RESTIR_ENABLE) && b == 0u) {
+        Reservoir res{0u, 0u, 0u, 0.0f, 0u, 0.0f};
+        // (1) initial RIS, source pdf 1 / (lights x 6 faces)
+        const uint32_t n_m = max(v.restir_m, 1u);
+        const float inv_src = float(n_lights) * 6.0f;
+        for (uint32_t k = 0; k < n_m; k++) {
+            uint32_t pick = uint32_t(rand01(rng) * float(n_lights));
+            if (pick >= n_lights) pick = n_lights - 1u;
+            const EmLight cand = lights[pick];
+            uint32_t face = uint32_t(rand01(rng) * 6.0f);
+            if (face >= 6u) face = 5u;
+            const float uu = rand01(rng);
+            const float vv = rand01(rng);
+            const uint32_t seed = pack_face_seed(face, uu, vv);
+            const float target = target_pdf(cand, seed, sp, N);
+            r_update(res, pick, cand.vid, seed, target, target * inv_src, rng);
+        }
+        // (2) temporal reuse: the voxel's committed reservoir
+        if (v.restir & VE_RESTIR_TEMPORAL) {
+            Reservoir t;
+            if (res_load(S.res, primary_vid, lights, n_lights, t)) {
+                r_cap(t, v.restir_max_m);
+                r_combine(res, t, t.target, rng);
+            }
+        }
+        // (3) spatial reuse: neighbour voxels in the surface's tangent plane
+        if ((v.restir & VE_RESTIR_SPATIAL) && v.restir_nbrs > 0u) {
+            const f3 up = fabsf(N.z) < 0.999f ? mk(0.0f, 0.0f, 1.0f) : mk(1.0f, 0.0f, 0.0f);
+            const f3 T = normalize(cross(up, N));
+            const f3 B = cross(N, T);
+            const uint32_t K = min(v.restir_nbrs, 6u);
+            for (uint32_t k = 0; k < K; k++) {
+                const float ua = rand01(rng);
+                const float rr = v.restir_radius * sqrtf(rand01(rng));
+                float sn, cs;
+                sincos_turn(ua, &sn, &cs);
+                const f3 off = muls(add(muls(T, cs), muls(B, sn)), rr);
+                const int ox = int(roundf(off.x)), oy = int(roundf(off.y)), oz = int(roundf(off.z));
+                if (ox == 0 && oy == 0 && oz == 0) continue;
+                const uint32_t nvid = neighbour_vid(hx, hy, hz, 1u, ox, oy, oz);
+                if (nvid == 0u || nvid == primary_vid) continue;
+                Reservoir nb;
+                if (!res_load(S.res, nvid, lights, n_lights, nb)) continue;
+                const float tu = target_pdf(lights[nb.light_idx], nb.seed, sp, N);
+                if (tu <= 0.0f) continue;
+                r_cap(nb, v.restir_max_m);
+                r_combine(res, nb, tu, rng);
+            }
+        }
+        // (4) one shadow ray on the chosen sample; contribution f W with the
+        // size^2 Jacobian of the (face, u, v) parameterisation
+        if (res.m > 0u && res.target > 0.0f) {
+            const EmLight L = lights[res.light_idx];
+            if (L.vid == res.light_vid) {
+                f3 P, LN;
+                light_sample_point(res.seed, L, P, LN);
+                const f3 to = sub(P, sp);
+                const float d2 = dot(to, to);
+                const float dist = sqrtf(gmax(d2, 1e-12f));
+                if (dist > 1e-3f) {
+                    const f3 ld = divs(to, dist);
+                    const float cx = gmax(dot(N, ld), 0.0f);
+                    const float cy = gmax(dot(mk(-ld.x, -ld.y, -ld.z), LN), 0.0f);
+                    if (cx > 0.0f && cy > 0.0f) {
+                        const f3 brdf = evaluate_brdf(dir, ld, N, albedo, roughness, metallic, spec);
+                        const float W = res.wsum / (float(res.m) * res.target);
+                        const float sz2 = float(L.size * L.size);
+                        const float geom = cy / gmax(d2, 1e-6f);
+                        const f3 c = clamp_contrib(muls(muls(muls(mul(mk(L.er, L.eg, L.eb), brdf), geom), sz2), W));
+                        nee_pending(a, p, mul(tp, c), ld, L.vid, nf, o);
+                    }
+                }
+            }
+        }
+        // (5) the reservoir competes for the voxel's slot (committed at frame end)
+        if (res.m > 0u) {
+            const int e = res_claim(S.res, primary_vid);
+            if (e >= 0) {
+                atomicMax(&S.res[e].winner, p + 1u);
+                a.p_res[p] = PathRes{uint32_t(e), res, v.scene};
+                o.app_res = true;
+            }
+        }
+        return;
+    }
+    // single-pick RIS NEE
+    float wsum = 0.0f, chosen_t = 0.0f;
+    uint32_t chosen = 0u;
+    for (int k = 0; k < 4; k++) {
+        uint32_t pick = uint32_t(rand01(rng) * float(n_lights));
+        if (pick >= n_lights) pick = n_lights - 1u;
+        const EmLight cand = lights[pick];
+        const float lum = gmax(luminance(cand.er, cand.eg, cand.eb), 1e-6f);
+        const float target = lum * float(cand.size * cand.size);
+        wsum += target;
+        if (rand01(rng) * wsum < target) {
+            chosen = pick;
+            chosen_t = target;
+        }
+    }
+    const float avg_t = wsum / 4.0f;
+    const EmLight L = lights[chosen];
+    uint32_t face = uint32_t(rand01(rng) * 6.0f);
+    if (face >= 6u) face = 5u;
+    f3 fn, ft, fb;
+    face_frame(face, fn, ft, fb);
+    const float u1 = rand01(rng);
+    const float u2 = rand01(rng);
+    const f3 lp = face_point(L, fn, ft, fb, u1, u2);
+    f3 ld = sub(lp, sp);
+    const float d2 = dot(ld, ld);
+    const float dist = sqrtf(d2);
+    if (dist > 1e-3f && chosen_t > 0.0f) {
+        ld = divs(ld, dist);
+        const float cx = gmax(dot(N, ld), 0.0f);
+        const float cy = gmax(dot(mk(-ld.x, -ld.y, -ld.z), fn), 0.0f);
+        if (cx > 0.0f && cy > 0.0f) {
+            const f3 brdf = evaluate_brdf(dir, ld, N, albedo, roughness, metallic, spec);
+            const float area = 6.0f * float(L.size) * float(L.size);
+            const float ris = float(n_lights) * avg_t / gmax(chosen_t, 1e-6f);
+            const float geom = cy / gmax(d2, 1e-6f);
+            const f3 c = clamp_contrib(muls(muls(muls(mul(mk(L.er, L.eg, L.eb), brdf), geom), area), ris));
+            nee_pending(a, p, mul(tp, c), ld, L.vid, nf, o);
+        }
+    }
+}
+
 // One step of the bounce/shade loop (shade.comp:543-575, 838-908) for path
-// p, with the sun next-event estimate in the place of the dormant emissive
-// NEE: `hit` is the result of the ray along `dir` (ignored for a path marked
+// p, with the sun next-event estimate in the place of the emissive NEE
+// (VE_FRAME_EMISSIVE: emissive_nee instead): `hit` is the result of the ray along `dir` (ignored for a path marked
 // F_TERM), tp/direct/indirect the path state after any pending sun term was
 // resolved.  Writes the continuing path's state; the queue appends and the
 // AccumPass deposit are left to shade_emit.
+template <bool EM>
 __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4 meta, f3 tp, f3 direct,
                                            f3 indirect, f3 dir, uint4 hit, ShadeOut& o) {
     const uint32_t vi = meta.z & 0xFFFFu;
@@ -492,6 +674,17 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                 f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
                 em = mk(gmin(em.x, 20.0f), gmin(em.y, 20.0f), gmin(em.z, 20.0f));
                 if (b == 0u) direct = add(direct, em); else indirect = add(indirect, em);
+                // a light seen by a primary ray joins the registry at the end
+                // of the frame (shade.comp:585-613)
+                if (EM && (v.flags & VE_FRAME_EMISSIVE) && b == 0u) {
+                    const uint32_t hx = hit.z & 0xFFFFu, hy = hit.z >> 16, hz = hit.w & 0xFFFFu;
+                    const uint32_t lvid = voxel_key(hx, hy, hz) + 1u;
+                    if (em_claim(S.em_claim, lvid)) {
+                        const uint32_t k2 = atomicAdd(&S.em_state[1], 1u);
+                        if (k2 < (1u << kEmClaimLog2))
+                            S.em_stage[k2] = EmLight{albedo.x * k, albedo.y * k, albedo.z * k, lvid, hx, hy, hz, 1u};
+                    }
+                }
             }
             const f3 hp = mk(float(hit.z & 0xFFFFu), float(hit.z >> 16), float(hit.w & 0xFFFFu));
             const f3 sp = add(add(hp, mk(0.5f, 0.5f, 0.5f)), N);
@@ -568,16 +761,21 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                     }
                 }
             }
-            if (!ended && !emissive && b < 2u && dot(N, sun) > 0.0f) {
+            uint32_t rng = meta.y;
+            if (EM && (v.flags & VE_FRAME_EMISSIVE)) {
+                if (!ended && !emissive && b < 2u)
+                    emissive_nee(a, v, S, p, meta.x, b, hit.z & 0xFFFFu, hit.z >> 16, hit.w & 0xFFFFu, N, sp, dir, tp,
+                                 albedo, roughness, metallic, spec, rng, nf, o);
+            } else if (!ended && !emissive && b < 2u && dot(N, sun) > 0.0f) {
                 const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
                 f3 c = muls(brdf, v.sun_intensity);
                 c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
                 a.p_pend[p] = st3(mul(tp, c), 0.0f);
+                if (EM) a.p_sdir[p] = make_float4(sun.x, sun.y, sun.z, __uint_as_float(0xFFFFFFFFu));
                 nf |= F_PENDING;
                 o.app_sh = true;
             }
             bool term = false;
-            uint32_t rng = meta.y;
             if (ended) {
                 // ended by a cache: deposited now (hash) or after inference (network)
             } else if (b + 1u >= v.bounces + 1u) {
@@ -656,6 +854,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
 // The warp-collective part of a shading step: queue appends (live paths,
 // extension and shadow rays, learned-cache queries and samples) and the
 // warp-aggregated deposit.  Called by all 32 lanes.
+template <bool EM>
 __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const ShadeOut& o, uint32_t* live_out,
                                            uint32_t* live_cnt, uint32_t* ray_cnt, DepSlot* dep, uint32_t& n_ext,
                                            uint32_t& n_sh) {
@@ -682,6 +881,11 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
         warp_add_stat(&a.stats[ST_NRC_SAMPLES], o.sampled ? 1u : 0u);
     }
     warp_add_stat(&a.stats[ST_NRC_HASH], o.hash_term ? 1u : 0u);
+    if (EM) {
+        const uint32_t kr = warp_append(o.app_res, &a.counters[CNT_RES]);
+        if (o.app_res) a.res_list[kr] = p;
+        warp_add_stat(&a.stats[ST_EM_NEE], o.em_nee ? 1u : 0u);
+    }
     warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, a.stats);
     if (a.remaining) {  // serving: count finished paths per view slot
         const unsigned dm = __ballot_sync(0xffffffffu, o.do_dep);
@@ -697,7 +901,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
 // hit in registers (the same shade_step the shade pass runs), appending its
 // rays and live entry for trace pass 0 / shade pass 1 — the frame's largest
 // shade pass never round-trips the path state through memory.
-template <bool COUNT, bool FUSED>
+template <bool COUNT, bool FUSED, bool EM = false>
 __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     __shared__ DepSlot dep[FUSED ? 256 : 1];
     const uint32_t tile = blockIdx.x;
@@ -761,11 +965,11 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
                 // emit.comp:171-174
                 const uint32_t sample_idx = v.frame_index + spix * 2654435761u + list_idx * 1442695040u;
                 const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
-                shade_step(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
+                shade_step<EM>(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
                            mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o);
             }
-            shade_emit(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
-                       dep + (threadIdx.x & ~31u), n_ext, n_sh);
+            shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
+                           dep + (threadIdx.x & ~31u), n_ext, n_sh);
         }
         warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
         warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
@@ -801,6 +1005,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     }
 }
 
+template <bool EM = false>
 __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
@@ -817,10 +1022,11 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
         if (valid) {
             const uint4 meta = a.p_meta[p];
             const float4 pe = a.p_pend[p];  // read with the rest: no load waits on the flags
+            const uint32_t want = EM ? __float_as_uint(a.p_sdir[p].w) : 0xFFFFFFFFu;
             const uint32_t flags = meta.z >> 24;
             f3 direct = ld3(a.p_direct[p]);
             f3 indirect = ld3(a.p_indirect[p]);
-            if ((flags & F_PENDING) && pe.w != 0.0f) {
+            if ((flags & F_PENDING) && __float_as_uint(pe.w) == want) {
                 // the sun term belongs to the bounce that cast the shadow ray:
                 // the stored one when the path ended there, else the one before
                 const uint32_t b = (meta.z >> 16) & 0xFFu;
@@ -828,9 +1034,9 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
                 else indirect = add(indirect, ld3(pe));
             }
             const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
-            shade_step(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
+            shade_step<EM>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
         }
-        shade_emit(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), n_ext, n_sh);
+        shade_emit<EM>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), n_ext, n_sh);
     }
     warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
@@ -973,6 +1179,7 @@ __global__ void k_sched_threshold(float* rank, const DevView* views) {
 // emit.comp: one path per shade-list entry, from the representative pixel's
 // primary hit, list index i seeding the RNG; its first shading step runs
 // here as in the fused primary pass.
+template <bool EM = false>
 __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
     __shared__ DepSlot dep[256];
     const DevView& v = a.views[0];
@@ -995,17 +1202,73 @@ __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
             // emit.comp:171-174 with listIdx = the shade-list index
             const uint32_t sample_idx = v.frame_index + pix * 2654435761u + i * 1442695040u;
             const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
-            shade_step(a, p, make_uint4(e.x, rng, 0u + a.view_offset, pix), mk(1.0f, 1.0f, 1.0f), mk(0.0f, 0.0f, 0.0f),
+            shade_step<EM>(a, p, make_uint4(e.x, rng, 0u + a.view_offset, pix), mk(1.0f, 1.0f, 1.0f), mk(0.0f, 0.0f, 0.0f),
                        mk(0.0f, 0.0f, 0.0f), dir, make_uint4(kHit, hi.x, hi.y, hi.z), o);
             n_paths++;
         }
-        shade_emit(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
+        shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
                    n_ext, n_sh);
     }
     warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
     warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
     warp_add_stat(&a.stats[ST_PATHS], n_paths);
     warp_add_stat(&a.stats[ST_SCHED_PATHS], n_paths);
+}
+
+// ---------------------------------------------------------------------------
+// End-of-frame commits of emissive frames.
+// ---------------------------------------------------------------------------
+// Registry: sort keys = the staged lights' vids (unused slots ~0), values =
+// staging indices.
+__global__ void __launch_bounds__(256) k_em_keys(const DevScene* scenes, uint32_t sc, uint32_t* keys, uint32_t* vals) {
+    const DevScene S = scenes[sc];
+    constexpr uint32_t cap = 1u << kEmClaimLog2;
+    const uint32_t n = min(S.em_state[1], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+        keys[i] = i < n ? S.em_stage[i].vid : 0xFFFFFFFFu;
+        vals[i] = i;
+    }
+}
+// ... the staged lights in vid order fill the registry's free records (one
+// block: every thread reads the counts before thread 0 updates them).
+__global__ void __launch_bounds__(1024) k_em_append(const DevScene* scenes, uint32_t sc, const uint32_t* order,
+                                                    unsigned long long* stats) {
+    const DevScene S = scenes[sc];
+    const uint32_t count = min(S.em_state[0], kEmCapacity);
+    const uint32_t n = min(S.em_state[1], 1u << kEmClaimLog2);
+    const uint32_t add = min(n, kEmCapacity - count);
+    for (uint32_t i = threadIdx.x; i < add; i += blockDim.x) S.em_list[count + i] = S.em_stage[order[i]];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        S.em_state[0] = count + add;
+        S.em_state[1] = 0u;
+        atomicAdd(&stats[ST_EM_LIGHTS], (unsigned long long)(count + add));
+    }
+}
+// Reservoirs: each voxel keeps the reservoir of its winning path (the
+// largest slot among the frame's bounce-0 paths on it).
+__global__ void __launch_bounds__(256) k_res_commit(FrameArgs a) {
+    const uint32_t n = a.counters[CNT_RES];
+    uint32_t w = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < n) {
+            const uint32_t p = a.res_list[i];
+            const PathRes pr = a.p_res[p];
+            ResEntry* t = a.scenes[pr.scene].res + pr.entry;
+            if (t->winner == p + 1u) {
+                t->light_idx = pr.r.light_idx;
+                t->light_vid = pr.r.light_vid;
+                t->seed = pr.r.seed;
+                t->wsum = pr.r.wsum;
+                t->m = pr.r.m;
+                t->target = pr.r.target;
+                t->winner = 0u;
+                w++;
+            }
+        }
+    }
+    warp_add_stat(&a.stats[ST_RES_WRITES], w);
 }
 
 // Staging of a learned-cache query in a frame (runs in the encode kernel, at
@@ -1315,6 +1578,12 @@ struct SceneSlot {
     bool live = false;
     ve_nrc* nrc = nullptr;  // learned radiance cache attached to the scene
     float* rank = nullptr;  // scheduling state: {t_high, t_mid, histogram[256]}
+    // emissive lights and ReSTIR reservoirs (allocated by the first emissive frame)
+    ve::EmLight* em_list = nullptr;
+    uint32_t* em_claim = nullptr;
+    uint32_t* em_state = nullptr;
+    ve::EmLight* em_stage = nullptr;
+    ve::ResEntry* res = nullptr;
 };
 
 template <typename T>
@@ -1382,6 +1651,11 @@ struct ve_ctx {
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
+    ve::DevBuf<float4> p_sdir;          // emissive batches: NEE shadow directions + light vid
+    ve::DevBuf<ve::PathRes> p_res;      // emissive batches: bounce-0 reservoirs until the commit
+    ve::DevBuf<uint32_t> res_list;      // ... and the paths that hold one
+    ve::DevBuf<uint32_t> em_sort;       // registry commit: vid keys / staging indices, 2 x 2 x 2^17
+    ve::DevBuf<uint8_t> em_sort_tmp;    // ... CUB radix-sort scratch
     ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
@@ -1438,7 +1712,9 @@ static int sync_scenes(ve_ctx* c) {
     std::vector<DevScene> h(std::max<size_t>(c->scenes.size(), 1));
     for (size_t i = 0; i < c->scenes.size(); i++) {
         const SceneSlot& s = c->scenes[i];
-        h[i] = DevScene{s.nodes, s.n_words, s.cache, s.depth, c->cfg.hash_log2, c->cfg.hash_probes, s.top_level, s.top};
+        h[i] = DevScene{s.nodes,     s.n_words,   s.cache,    s.depth,    c->cfg.hash_log2, c->cfg.hash_probes,
+                        s.top_level, s.top,       s.em_list, s.em_claim, s.em_state,       s.em_stage,
+                        s.res};
     }
     const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
@@ -1603,6 +1879,44 @@ static int compute_normals(ve_ctx* c, SceneSlot& s) {
 
 // Scheduling thresholds {t_high = +inf, t_mid = -inf} and an empty histogram:
 // every voxel of the next scheduled frame falls in the middle tier.
+static void free_emissive(SceneSlot& s) {
+    if (s.em_list) cudaFree(s.em_list);
+    if (s.em_claim) cudaFree(s.em_claim);
+    if (s.em_state) cudaFree(s.em_state);
+    if (s.em_stage) cudaFree(s.em_stage);
+    if (s.res) cudaFree(s.res);
+    s.em_list = nullptr;
+    s.em_claim = nullptr;
+    s.em_state = nullptr;
+    s.em_stage = nullptr;
+    s.res = nullptr;
+}
+
+// No lights registered or staged, no reservoirs.
+static int reset_emissive(ve_ctx* c, SceneSlot& s) {
+    if (!s.em_claim) return VE_OK;
+    VE_CUDA(cudaMemsetAsync(s.em_claim, 0, sizeof(uint32_t) << kEmClaimLog2, c->stream));
+    VE_CUDA(cudaMemsetAsync(s.em_state, 0, 2 * sizeof(uint32_t), c->stream));
+    VE_CUDA(cudaMemsetAsync(s.res, 0, sizeof(ResEntry) << kResLog2, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+// The scene's light registry and reservoir table (first emissive frame).
+static int ensure_emissive(ve_ctx* c, SceneSlot& s) {
+    if (s.em_claim) return VE_OK;
+    if (cudaMalloc(&s.em_list, sizeof(EmLight) * kEmCapacity) != cudaSuccess ||
+        cudaMalloc(&s.em_claim, sizeof(uint32_t) << kEmClaimLog2) != cudaSuccess ||
+        cudaMalloc(&s.em_state, 2 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&s.em_stage, sizeof(EmLight) << kEmClaimLog2) != cudaSuccess ||
+        cudaMalloc(&s.res, sizeof(ResEntry) << kResLog2) != cudaSuccess) {
+        free_emissive(s);
+        return fail(VE_ERR_NOMEM, "render: emissive-light state allocation failed");
+    }
+    c->scenes_dirty = true;
+    return reset_emissive(c, s);
+}
+
 static int reset_rank(ve_ctx* c, float* rank) {
     std::vector<uint32_t> init(2 + kRankBins, 0u);
     init[0] = 0x7f800000u;
@@ -1741,6 +2055,11 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         return fail(VE_ERR_INVALID, "render: VE_FRAME_SCHEDULED renders one view per call");
     if ((flags & VE_FRAME_SCHEDULED) && (flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN)))
         return fail(VE_ERR_INVALID, "render: VE_FRAME_SCHEDULED does not combine with the learned cache");
+    if ((flags & VE_FRAME_EMISSIVE) && (flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN | VE_FRAME_TERMINATE_HASH)))
+        return fail(VE_ERR_INVALID, "render: VE_FRAME_EMISSIVE does not combine with cache-terminated paths");
+    for (uint32_t i = 0; i < nv; i++)
+        if ((views[i].frame.flags & VE_FRAME_EMISSIVE) && views[i].frame.restir_m > 64)
+            return fail(VE_ERR_INVALID, "render: restir_m must be <= 64");
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
     // learned radiance cache: one per batch, attached to the views' scenes
     ve_nrc* nrc = nullptr;
@@ -1790,6 +2109,28 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if ((rc = c->path_rgb.ensure(paths * 3))) return rc;
         if (old != c->path_rgb.p) c->gen++;
     }
+    // emissive lights: the scenes' registries and reservoir tables, the
+    // per-path NEE records and the registry commit's sort buffers
+    std::vector<int> em_scenes;
+    size_t em_sort_bytes = 0;
+    if (flags & VE_FRAME_EMISSIVE) {
+        for (uint32_t i = 0; i < nv; i++) {
+            if (!(views[i].frame.flags & VE_FRAME_EMISSIVE)) continue;
+            const int sc = views[i].scene_id;
+            if (std::find(em_scenes.begin(), em_scenes.end(), sc) == em_scenes.end()) em_scenes.push_back(sc);
+            if ((rc = ensure_emissive(c, c->scenes[sc]))) return rc;
+        }
+        constexpr int cap = 1 << kEmClaimLog2;
+        cub::DeviceRadixSort::SortPairs(nullptr, em_sort_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (const uint32_t*)nullptr, (uint32_t*)nullptr, cap, 0, 32, c->stream);
+        const void* before[] = {c->p_sdir.p, c->p_res.p, c->res_list.p, c->em_sort.p, c->em_sort_tmp.p};
+        if ((rc = c->p_sdir.ensure(paths)) || (rc = c->p_res.ensure(paths)) || (rc = c->res_list.ensure(paths)) ||
+            (rc = c->em_sort.ensure(4ull * cap)) || (rc = c->em_sort_tmp.ensure(em_sort_bytes)))
+            return rc;
+        const void* after[] = {c->p_sdir.p, c->p_res.p, c->res_list.p, c->em_sort.p, c->em_sort_tmp.p};
+        for (int i = 0; i < 5; i++)
+            if (before[i] != after[i]) c->gen++;
+    }
     if ((rc = sync_scenes(c))) return rc;
     // view table, written into a staging slot whose previous copy has run
     const int slot = c->staging_next;
@@ -1821,6 +2162,11 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         d.mid_frac = f.mid_fraction;
         d.min_samples = std::min<uint32_t>(f.min_samples, 2u);
         d.budget = f.shading_budget;
+        d.restir = f.restir;
+        d.restir_m = f.restir_m;
+        d.restir_nbrs = f.restir_spatial_neighbors;
+        d.restir_max_m = f.restir_max_m;
+        d.restir_radius = f.restir_spatial_radius;
         d.pix_base = uint32_t(pix_base);
         d.tile_base = tile_base;
         d.path_base = path_base;
@@ -1905,6 +2251,12 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         a.shade_cap = uint32_t(paths);
         a.rank = c->scenes[views[0].scene_id].rank;
     }
+    if (flags & VE_FRAME_EMISSIVE) {
+        a.p_sdir = c->p_sdir.p;
+        a.p_res = c->p_res.p;
+        a.res_list = c->res_list.p;
+    }
+    const bool em = (flags & VE_FRAME_EMISSIVE) != 0;
     // the frame's kernel sequence (no host synchronisation inside)
     auto enqueue = [&]() {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
@@ -1921,8 +2273,13 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
         }
         rec();
-        if (count) k_primary<true, true><<<tiles, 256, 0, st>>>(a);
-        else k_primary<false, true><<<tiles, 256, 0, st>>>(a);
+        if (em) {
+            if (count) k_primary<true, true, true><<<tiles, 256, 0, st>>>(a);
+            else k_primary<false, true, true><<<tiles, 256, 0, st>>>(a);
+        } else {
+            if (count) k_primary<true, true><<<tiles, 256, 0, st>>>(a);
+            else k_primary<false, true><<<tiles, 256, 0, st>>>(a);
+        }
         launches++;
         if (sched) {  // schedule -> rank -> shade list -> thresholds -> emit
             cudaMemsetAsync(a.claim_key, 0, 4ull * claim_size, st);
@@ -1936,19 +2293,26 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, b, a.sched_n, a.sched_off, int(pixels), st);
             k_sched_list<<<g, 256, 0, st>>>(a);
             k_sched_threshold<<<1, 1, 0, st>>>(a.rank, a.views);
-            k_sched_emit<<<c->grid_shade, 256, 0, st>>>(a);
+            if (em) k_sched_emit<true><<<c->grid_shade, 256, 0, st>>>(a);
+            else k_sched_emit<<<c->grid_shade, 256, 0, st>>>(a);
             launches += 6;
         }
         rec();
         for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
             if (pass > 0) {  // pass 0 runs inside the fused primary
-                k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
+                if (em) k_shade<true><<<c->grid_shade, 256, 0, st>>>(a, pass);
+                else k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
                 launches++;
             }
             rec();
             if (pass <= max_b) {
-                if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
-                else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
+                if (em) {
+                    if (count) k_trace<true, true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
+                    else k_trace<false, true><<<c->grid_trace, 256, 0, st>>>(a, pass);
+                } else {
+                    if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
+                    else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
+                }
                 launches++;
                 trace_launches++;
             }
@@ -1971,6 +2335,22 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         k_resolve<<<tiles, 256, 0, st>>>(a);
         launches++;
+        if (flags & VE_FRAME_EMISSIVE) {  // this frame's lights and reservoirs, for the next frame
+            constexpr int cap = 1 << kEmClaimLog2;
+            uint32_t* kin = c->em_sort.p;
+            uint32_t* kout = kin + cap;
+            uint32_t* vin = kin + 2 * cap;
+            uint32_t* vout = kin + 3 * cap;
+            for (int sc : em_scenes) {
+                k_em_keys<<<c->num_sms * 4, 256, 0, st>>>(a.scenes, uint32_t(sc), kin, vin);
+                size_t b = em_sort_bytes;
+                cub::DeviceRadixSort::SortPairs(c->em_sort_tmp.p, b, kin, kout, vin, vout, cap, 0, 32, st);
+                k_em_append<<<1, 1024, 0, st>>>(a.scenes, uint32_t(sc), vout, c->stats.p);
+                launches += 3;
+            }
+            k_res_commit<<<c->num_sms * 4, 256, 0, st>>>(a);
+            launches++;
+        }
         rec();
         k_accum_stats<<<1, 32, 0, st>>>(c->stats.p, c->totals.p);
         launches++;
@@ -1981,7 +2361,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     } else {
         std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
                                      flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
-                                              VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED),
+                                              VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED |
+                                              VE_FRAME_EMISSIVE),
                                      paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
                                      uint64_t(c->launch.refill_threshold), uint64_t(uintptr_t(nrc)),
                                      uint64_t(a.nrc_ready)};
@@ -1990,6 +2371,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             std::memcpy(&bits, &d.second, 4);
             key.push_back((uint64_t(uint32_t(d.first)) << 32) | bits);
         }
+        for (int sc : em_scenes) key.push_back((1ull << 62) | uint64_t(uint32_t(sc)));
         ve_ctx::GraphEntry* ge = nullptr;
         for (auto& g : c->graphs)
             if (g.key == key) ge = &g;
@@ -2176,7 +2558,7 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
     int bt = 0, btc = 0, bs = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade<false>, 256, 0);
     x->occ_trace = std::max(bt, 1);
     x->occ_trace_count = std::max(btc, 1);
     x->occ_shade = std::max(bs, 1);
@@ -2211,6 +2593,7 @@ int ve_ctx_destroy(ve_ctx* c) {
         if (s.cache) cudaFree(s.cache);
         if (s.top) cudaFree(s.top);
         if (s.rank) cudaFree(s.rank);
+        free_emissive(s);
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
     c->p_ray_o.release(); c->p_ray_d.release(); c->p_tp.release(); c->p_direct.release();
@@ -2220,6 +2603,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->hitinfo.release(); c->claim.release(); c->sched_n.release(); c->shade_list.release(); c->scan_tmp.release();
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
     c->out_mapped.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
+    c->p_sdir.release(); c->p_res.release(); c->res_list.release(); c->em_sort.release(); c->em_sort_tmp.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
         if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
         if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
@@ -2532,6 +2916,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     cudaFree(s.cache);
     if (s.top) cudaFree(s.top);
     if (s.rank) cudaFree(s.rank);
+    free_emissive(s);
     s = SceneSlot();
     c->scenes_dirty = true;
     c->gen++;
@@ -2661,6 +3046,8 @@ int ve_cache_reset(ve_ctx* c, int32_t id) {
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "cache_reset: unknown scene");
     VE_CUDA(cudaMemsetAsync(c->scenes[id].cache, 0, sizeof(CacheEntry) << c->cfg.hash_log2, c->stream));
+    // the emissive lights and reservoirs go with it
+    if (int rc = reset_emissive(c, c->scenes[id])) return rc;
     // the scheduling thresholds derive from the cache: forget them too
     if (c->scenes[id].rank) {
         const int rc = reset_rank(c, c->scenes[id].rank);
@@ -2792,6 +3179,9 @@ static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
     r.nrc_samples = h[ST_NRC_SAMPLES];
     r.scheduled_voxels = h[ST_SCHED_VOXELS];
     r.scheduled_paths = h[ST_SCHED_PATHS];
+    r.emissive_lights = h[ST_EM_LIGHTS];
+    r.nee_emissive = h[ST_EM_NEE];
+    r.restir_commits = h[ST_RES_WRITES];
 }
 
 int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {

@@ -165,6 +165,45 @@ __device__ __forceinline__ f3 cosine_direction(f3 n, uint32_t& rng) {
     return divs(v, sqrtf(d2));
 }
 
+// x^e for x in (0, 1] and e > 0 (the specular lobe's pow(NdotH, exponent)),
+// project-written so the host and the device agree bit for bit:
+// exp2(e * log2 x) with ln of the mantissa m in [sqrt(1/2), sqrt(2)) from
+// the series ln m = 2 atanh(s) = 2 (s + s^3/3 + ... + s^13/13),
+// s = (m - 1) / (m + 1), and 2^f, f in [-1/2, 1/2], from the Taylor series
+// of e^(f ln 2) to degree 8 (explicit fma throughout).  Results below 2^-125
+// read as 0.
+__device__ __forceinline__ float pow_unit(float x, float e) {
+    if (x != x) return x;  // NaN stays NaN
+    const uint32_t bits = __float_as_uint(x);
+    int ex = int(bits >> 23) - 127;
+    float m = __uint_as_float((bits & 0x007FFFFFu) | 0x3F800000u);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        ex += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = __fmaf_rn(s2, 0.0769230769f, 0.0909090909f);
+    p = __fmaf_rn(s2, p, 0.111111111f);
+    p = __fmaf_rn(s2, p, 0.142857143f);
+    p = __fmaf_rn(s2, p, 0.2f);
+    p = __fmaf_rn(s2, p, 0.333333333f);
+    const float lnm = 2.0f * __fmaf_rn(s * s2, p, s);
+    const float y = e * (float(ex) + lnm * 1.44269504f);
+    if (!(y > -125.0f)) return 0.0f;
+    const float n = floorf(y + 0.5f);
+    const float t = (y - n) * 0.693147181f;
+    float q = __fmaf_rn(t, 2.48015873e-5f, 1.98412698e-4f);
+    q = __fmaf_rn(t, q, 1.38888889e-3f);
+    q = __fmaf_rn(t, q, 8.33333333e-3f);
+    q = __fmaf_rn(t, q, 4.16666667e-2f);
+    q = __fmaf_rn(t, q, 0.166666667f);
+    q = __fmaf_rn(t, q, 0.5f);
+    q = __fmaf_rn(t, q, 1.0f);
+    q = __fmaf_rn(t, q, 1.0f);
+    return __uint_as_float(__float_as_uint(q) + (uint32_t(int(n)) << 23));
+}
+
 // EvaluateBRDF (internal.glsl:120-149)
 __device__ __forceinline__ f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float roughness, float metallic,
                                             float specular_intensity) {
@@ -180,7 +219,7 @@ __device__ __forceinline__ f3 evaluate_brdf(f3 V, f3 L, f3 N, f3 albedo, float r
         const f3 H = normalize(sub(L, V));
         const float NdotH = gmax(dot(N, H), 0.001f);
         const float spec_norm = (spec_exp + 2.0f) * 0.15915494f;
-        sp = (spec_norm * powf(NdotH, spec_exp)) * kS;
+        sp = (spec_norm * pow_unit(NdotH, spec_exp)) * kS;
     } else {
         // The lobe is multiplied by kS = 0: the product is +0 whenever the
         // half vector is finite, i.e. whenever |L - V|^2 > 0 (N, L, V are

@@ -115,3 +115,58 @@ def camera_sequence(w: Workload) -> List[Tuple[np.ndarray, np.ndarray]]:
     if w.name == "small":
         return [small_camera()] * w.frames
     return [orbit_camera(f, w.frames, w.seed) for f in range(w.frames)]
+
+
+# ---------------------------------------------------------------------------
+# The reference's default emissive scene: the Cornell box of
+# src/voxelengine.cpp:82-142 (depth 8, camera of :41-46), for VE_FRAME_EMISSIVE.
+# ---------------------------------------------------------------------------
+CORNELL = Workload("cornell", depth=8, variant=0, seed=0, width=512, height=512, spp=1, bounces=3, frames=16,
+                   fov=90.0, hash_log2=22, primary_controlchecks=70, bounce_controlchecks=120)
+# material indices in MaterialPool::addMaterial order (index 0 is reserved)
+CORNELL_EMISSIVE, CORNELL_RED, CORNELL_GREEN, CORNELL_WHITE, CORNELL_METALLIC, CORNELL_BLUE = 1, 2, 3, 4, 5, 6
+
+
+def cornell_materials() -> np.ndarray:
+    """128 std140 Material entries (64 B: color, specularColor, roughness,
+    specular, metallic, emissive (int), emissiveIntensity) as (128, 16) f32."""
+    out = np.zeros((128, 16), np.float32)
+    mats = {  # color, specularColor, roughness, specular, metallic, emissive, intensity
+        CORNELL_EMISSIVE: ((1, 1, 1, 0), (1, 1, 1, 1), 0.4, 0.03, 0.2, 1, 10.0),
+        CORNELL_RED: ((1, 0, 0, 0), (0.8, 0.1, 0.1, 1), 0.1, 0.9, 0.2, 0, 0.0),
+        CORNELL_GREEN: ((0, 1, 0, 0), (1, 1, 1, 1), 0.8, 0.1, 0.0, 0, 0.0),
+        CORNELL_WHITE: ((1, 1, 1, 0), (1, 1, 1, 1), 0.6, 0.2, 0.0, 0, 0.0),
+        CORNELL_METALLIC: ((0.8, 0.8, 0.8, 0), (1, 1, 1, 1), 0.15, 1.0, 0.7, 0, 0.0),
+        CORNELL_BLUE: ((0, 0, 1, 0), (1, 1, 1, 1), 0.8, 0.1, 0.0, 0, 0.0),
+    }
+    for i, (col, spc, rough, spec, metal, emissive, intensity) in mats.items():
+        out[i, 0:4] = col
+        out[i, 4:8] = spc
+        out[i, 8] = rough
+        out[i, 9] = spec
+        out[i, 10] = metal
+        out[i, 11] = np.array([emissive], np.int32).view(np.float32)[0]
+        out[i, 12] = intensity
+    return out
+
+
+def cornell_build(cpu, depth: int = 8) -> None:
+    """The scene's insertSphere / insertBox calls, in their order, on an
+    OctreeCPU-like object (ours or the reference's own)."""
+    L = 1 << depth
+    f = np.float32
+    cpu.insert_sphere((f(L) / f(3), f(L) / f(3) - f(5), f(L) / f(2)), f(L) / f(4), CORNELL_METALLIC)
+    cpu.insert_sphere((f(L) * f(3) / f(4) - f(5), f(L) * f(3) / f(4) - f(15), f(L) * f(3) / f(4) - f(5)), f(L) / f(4),
+                      CORNELL_WHITE)
+    cpu.insert_box((0, 0, 0), (L, 4, L), CORNELL_WHITE)            # floor
+    cpu.insert_box((0, 0, 0), (4, L, L), CORNELL_GREEN)            # left wall
+    cpu.insert_box((L - 4, 0, 0), (L, L, L), CORNELL_RED)          # right wall
+    cpu.insert_box((0, 0, L - 4), (L, L, L), CORNELL_METALLIC)     # back wall (mirror)
+    cpu.insert_box((0, L - 4, 0), (L, L, L), CORNELL_WHITE)        # ceiling
+    cpu.insert_box((L // 4, L - 8, L // 4), (L * 3 // 4, L - 4, L * 3 // 4), CORNELL_EMISSIVE)  # light panel
+
+
+def cornell_camera(depth: int = 8) -> Tuple[np.ndarray, np.ndarray]:
+    """Camera::Config of src/voxelengine.cpp:41-46: (L/2, L/2, -L/2) looking +z."""
+    h = float(1 << (depth - 1))
+    return np.array([h, h, -h], np.float32), np.array([0.0, 0.0, 1.0], np.float32)
