@@ -95,7 +95,8 @@ enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
 constexpr uint32_t kDefaultRefill = 24;  // trace refill threshold (idle lanes of 32)
 enum : uint32_t {
     CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_RES = 63,
-    CNT_TOTAL = 64
+    CNT_RAYSH = 64,  // shadow rays per pass (extension rays: CNT_RAY)
+    CNT_TOTAL = 96
 };
 enum : uint32_t {
     ST_RAYS_PRIMARY = 0,
@@ -145,7 +146,8 @@ struct FrameArgs {
     uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
     uint32_t* live[2];
-    uint32_t* rayq;
+    uint32_t* rayq;     // per pass: extension rays (path slot)
+    uint32_t* rayq_sh;  // ... and shadow rays (path slot | 1 << 31), a separate region
     uint32_t* counters;
     unsigned long long* stats;
     uint4* gbuf;
@@ -327,7 +329,10 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
 // EM: the batch has VE_FRAME_EMISSIVE views (shadow rays toward lights).
 template <bool COUNT, bool EM = false>
 __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
-    const uint32_t n = a.counters[CNT_RAY + pass];
+    // the pass's extension rays, then its shadow rays: warps stay mostly of
+    // one kind, and the shorter shadow rays form the tail of the pass
+    const uint32_t n_ext = a.counters[CNT_RAY + pass];
+    const uint32_t n = n_ext + a.counters[CNT_RAYSH + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
     bool active = false, exhausted = false;
@@ -354,7 +359,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
             if (!active && !exhausted) {
                 const uint32_t idx = first_idx + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (idx < n) {
-                    e = a.rayq[idx];
+                    e = idx < n_ext ? a.rayq[idx] : a.rayq_sh[idx - n_ext];
                     const uint32_t p = e & 0x7FFFFFFFu;
                     const uint4 meta = a.p_meta[p];
                     const DevView& v = a.views[meta.z & 0xFFFFu];
@@ -862,8 +867,8 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
     if (o.app_live) live_out[sl] = p;
     const uint32_t se = warp_append(o.app_ext, ray_cnt);
     if (o.app_ext) a.rayq[se] = p;
-    const uint32_t ss = warp_append(o.app_sh, ray_cnt);
-    if (o.app_sh) a.rayq[ss] = p | 0x80000000u;
+    const uint32_t ss = warp_append(o.app_sh, ray_cnt + (CNT_RAYSH - CNT_RAY));
+    if (o.app_sh) a.rayq_sh[ss] = p | 0x80000000u;
     n_ext += o.app_ext ? 1u : 0u;
     n_sh += o.app_sh ? 1u : 0u;
     if (a.nq || a.ns) {
@@ -2212,7 +2217,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.p_ray_o = c->p_ray_o.p; a.p_ray_d = c->p_ray_d.p; a.p_tp = c->p_tp.p;
     a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
     a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p;
-    a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p;
+    a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p; a.rayq_sh = c->rayq.p + paths;
     a.counters = c->counters.p; a.stats = c->stats.p;
     a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
     a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;

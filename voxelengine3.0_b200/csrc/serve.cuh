@@ -141,6 +141,7 @@ static FrameArgs serve_args(ve_server* s) {
     a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
     a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p;
     a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p;
+    a.rayq_sh = c->rayq.p + s->cfg.path_capacity;
     a.counters = c->counters.p; a.stats = c->stats.p;
     a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
     a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
@@ -193,6 +194,7 @@ static void serve_loop(ve_server* s) {
         // primaries) and is kept.  Shade writes its survivor count at ps + 1.
         cudaMemsetAsync(c->counters.p + CNT_LIVE + ps + 1, 0, 4, st);
         cudaMemsetAsync(c->counters.p + CNT_RAY + ps, 0, 4, st);
+        cudaMemsetAsync(c->counters.p + CNT_RAYSH + ps, 0, 4, st);
         cudaMemsetAsync(c->counters.p + CNT_CURSOR + ps, 0, 4, st);
         FrameArgs a = serve_args(s);
         for (ServeRequest* r : admit) {
