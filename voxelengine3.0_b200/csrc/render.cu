@@ -249,9 +249,12 @@ struct DepSlot {
 // AccumPass deposit, warp-aggregated: lanes depositing into the same
 // (scene, vid) are merged in shared memory and one leader lane issues the
 // atomics (count, luma^2, and one vector add of {r, g, b, weight}).
+// `n_dep` / `n_drop`: this thread's share of the deposits made / dropped
+// (a group's leader counts the group), added to the frame's counters once
+// per kernel instead of by one atomic per group on a single address.
 __device__ __forceinline__ void warp_deposit(bool active, uint32_t scene, uint32_t vid, float r, float g, float b,
-                                             float l2, DepSlot* sh, const DevScene* scenes,
-                                             unsigned long long* stats) {
+                                             float l2, DepSlot* sh, const DevScene* scenes, uint32_t& n_dep,
+                                             uint32_t& n_drop) {
     const unsigned am = __ballot_sync(0xffffffffu, active);
     if (am == 0u) return;
     const uint32_t lane = lane_id();
@@ -277,13 +280,64 @@ __device__ __forceinline__ void warp_deposit(bool active, uint32_t scene, uint32
                 atomicAdd(&e->count, n);
                 atomicAdd(&e->l2, sl);
                 atomicAdd(&e->rgbw, make_float4(sr, sg, sb, float(n)));
-                atomicAdd(&stats[ST_DEPOSITS], (unsigned long long)n);
+                n_dep += n;
             } else {
-                atomicAdd(&stats[ST_DROPPED], (unsigned long long)n);
+                n_drop += n;
             }
         }
     }
     __syncwarp();
+}
+
+// Per-thread tallies of a shading kernel, added to the frame's counters once
+// at its end.
+struct EmitCounts {
+    uint32_t ext = 0, sh = 0, dep = 0, drop = 0;
+};
+__device__ __forceinline__ void flush_counts(const EmitCounts& c, unsigned long long* stats) {
+    warp_add_stat(&stats[ST_RAYS_BOUNCE], c.ext);
+    warp_add_stat(&stats[ST_RAYS_SHADOW], c.sh);
+    warp_add_stat(&stats[ST_DEPOSITS], c.dep);
+    warp_add_stat(&stats[ST_DROPPED], c.drop);
+}
+
+// Block-aggregated appends to a shading step's three queues (live paths,
+// extension rays, shadow rays): one atomicAdd per queue and block instead of
+// per warp — each queue counter is a single address every block contends
+// on.  Called by all threads of a block of <= 256; successive calls
+// alternate between two buffers, so one barrier pair per call suffices.
+struct BlockQ {
+    uint32_t cnt[3][8];
+    uint32_t base[3];
+};
+__device__ __forceinline__ uint3 block_append3(bool p0, bool p1, bool p2, uint32_t* c0, uint32_t* c1, uint32_t* c2,
+                                               BlockQ& q) {
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const unsigned m0 = __ballot_sync(0xffffffffu, p0);
+    const unsigned m1 = __ballot_sync(0xffffffffu, p1);
+    const unsigned m2 = __ballot_sync(0xffffffffu, p2);
+    if (lane == 0u) {
+        q.cnt[0][w] = uint32_t(__popc(m0));
+        q.cnt[1][w] = uint32_t(__popc(m1));
+        q.cnt[2][w] = uint32_t(__popc(m2));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3u) {
+        const uint32_t k = threadIdx.x;
+        uint32_t acc = 0;
+        for (uint32_t i = 0; i < (blockDim.x >> 5); i++) {
+            const uint32_t c = q.cnt[k][i];
+            q.cnt[k][i] = acc;
+            acc += c;
+        }
+        uint32_t* ctr = k == 0u ? c0 : (k == 1u ? c1 : c2);
+        q.base[k] = acc ? atomicAdd(ctr, acc) : 0u;
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    return make_uint3(q.base[0] + q.cnt[0][w] + uint32_t(__popc(m0 & lt)),
+                      q.base[1] + q.cnt[1][w] + uint32_t(__popc(m1 & lt)),
+                      q.base[2] + q.cnt[2][w] + uint32_t(__popc(m2 & lt)));
 }
 
 __device__ __forceinline__ uint32_t find_view(const DevView* views, uint32_t n, uint32_t tile) {
@@ -861,16 +915,15 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
 // warp-aggregated deposit.  Called by all 32 lanes.
 template <bool EM>
 __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const ShadeOut& o, uint32_t* live_out,
-                                           uint32_t* live_cnt, uint32_t* ray_cnt, DepSlot* dep, uint32_t& n_ext,
-                                           uint32_t& n_sh) {
-    const uint32_t sl = warp_append(o.app_live, live_cnt);
-    if (o.app_live) live_out[sl] = p;
-    const uint32_t se = warp_append(o.app_ext, ray_cnt);
-    if (o.app_ext) a.rayq[se] = p;
-    const uint32_t ss = warp_append(o.app_sh, ray_cnt + (CNT_RAYSH - CNT_RAY));
-    if (o.app_sh) a.rayq_sh[ss] = p | 0x80000000u;
-    n_ext += o.app_ext ? 1u : 0u;
-    n_sh += o.app_sh ? 1u : 0u;
+                                           uint32_t* live_cnt, uint32_t* ray_cnt, DepSlot* dep, BlockQ& q,
+                                           EmitCounts& cnt) {
+    const uint3 s = block_append3(o.app_live, o.app_ext, o.app_sh, live_cnt, ray_cnt,
+                                  ray_cnt + (CNT_RAYSH - CNT_RAY), q);
+    if (o.app_live) live_out[s.x] = p;
+    if (o.app_ext) a.rayq[s.y] = p;
+    if (o.app_sh) a.rayq_sh[s.z] = p | 0x80000000u;
+    cnt.ext += o.app_ext ? 1u : 0u;
+    cnt.sh += o.app_sh ? 1u : 0u;
     if (a.nq || a.ns) {
         // learned cache: query records move from the path's ray slots into
         // the query queue (capacity = paths, never full)
@@ -891,7 +944,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
         if (o.app_res) a.res_list[kr] = p;
         warp_add_stat(&a.stats[ST_EM_NEE], o.em_nee ? 1u : 0u);
     }
-    warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, a.stats);
+    warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, cnt.dep, cnt.drop);
     if (a.remaining) {  // serving: count finished paths per view slot
         const unsigned dm = __ballot_sync(0xffffffffu, o.do_dep);
         if (o.do_dep) {
@@ -947,7 +1000,8 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
         // lanes of one chunk hold consecutive path slots (a row of the warp's
         // 8 x 4 pixel block), so path-state stores and queue entries stay
         // coalesced.  Lane i traced pixel i of the block.
-        uint32_t n_ext = 0, n_sh = 0;
+        __shared__ BlockQ bq[2];
+        EmitCounts cnt;
         const uint32_t lane = lane_id();
         const uint32_t spp = v.spp;  // one view per block: uniform
         const uint32_t pix = py * v.W + px;
@@ -974,10 +1028,9 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
                            mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o);
             }
             shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
-                           dep + (threadIdx.x & ~31u), n_ext, n_sh);
+                           dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
         }
-        warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
-        warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+        flush_counts(cnt, a.stats);
     }
     const uint32_t q = FUSED ? 0u : warp_append(spawn, &a.counters[CNT_LIVE + 0], v.spp);
     if (!FUSED && spawn) {
@@ -1018,8 +1071,10 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
     uint32_t* live_out = a.live[(pass + 1u) & 1u];
     uint32_t* live_cnt = &a.counters[CNT_LIVE + pass + 1u];
     uint32_t* ray_cnt = &a.counters[CNT_RAY + pass];
-    uint32_t n_ext = 0, n_sh = 0;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    __shared__ BlockQ bq[2];
+    EmitCounts cnt;
+    uint32_t it = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x, it++) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < n;
         const uint32_t p = valid ? live_in[i] : 0u;
@@ -1041,10 +1096,9 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
             const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
             shade_step<EM>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
         }
-        shade_emit<EM>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), n_ext, n_sh);
+        shade_emit<EM>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
     }
-    warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
-    warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+    flush_counts(cnt, a.stats);
 }
 
 // ---------------------------------------------------------------------------
@@ -1192,8 +1246,10 @@ __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
     const f3 plane = mk(v.cam[4], v.cam[5], v.cam[6]);
     const f3 right = mk(v.cam[8], v.cam[9], v.cam[10]);
     const f3 up = mk(v.cam[12], v.cam[13], v.cam[14]);
-    uint32_t n_ext = 0, n_sh = 0, n_paths = 0;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    __shared__ BlockQ bq[2];
+    EmitCounts cnt;
+    uint32_t n_paths = 0, it = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x, it++) {
         const uint32_t i = base + threadIdx.x;
         const uint32_t p = uint32_t(v.path_base) + i;
         ShadeOut o;
@@ -1212,10 +1268,9 @@ __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
             n_paths++;
         }
         shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
-                   n_ext, n_sh);
+                       bq[it & 1u], cnt);
     }
-    warp_add_stat(&a.stats[ST_RAYS_BOUNCE], n_ext);
-    warp_add_stat(&a.stats[ST_RAYS_SHADOW], n_sh);
+    flush_counts(cnt, a.stats);
     warp_add_stat(&a.stats[ST_PATHS], n_paths);
     warp_add_stat(&a.stats[ST_SCHED_PATHS], n_paths);
 }
@@ -1320,7 +1375,10 @@ struct ApplyDeposit {
             }
         }
         DepSlot* dep = reinterpret_cast<DepSlot*>(scratch) + (threadIdx.x & 96u);
-        warp_deposit(valid, dscene, dvid, dr, dg, db, dl2, dep, a.scenes, a.stats);
+        uint32_t n_dep = 0, n_drop = 0;
+        warp_deposit(valid, dscene, dvid, dr, dg, db, dl2, dep, a.scenes, n_dep, n_drop);
+        warp_add_stat(&a.stats[ST_DEPOSITS], n_dep);
+        warp_add_stat(&a.stats[ST_DROPPED], n_drop);
     }
 };
 
