@@ -48,6 +48,8 @@ extern "C" {
 #define VE_FRAME_TRAIN 32u        /* record training samples and train the scene's learned cache */
 #define VE_FRAME_EMISSIVE 128u    /* NEE toward the scene's emissive voxels instead of the sun: light
                                      registry, single-pick RIS and ReSTIR DI (shade.comp:576-836) */
+#define VE_FRAME_LBUFFER 256u    /* the reference's dual-channel lBuffer AccumPass (shade.comp:96-257)
+                                     in place of the FP32 per-voxel cache; one view per call */
 #define VE_FRAME_SCHEDULED 64u    /* importance-aware voxel scheduling (schedule/rank/threshold.comp)
                                      in place of spp paths per pixel; single-view calls */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
@@ -94,6 +96,14 @@ typedef struct ve_frame_config {
     uint32_t restir_spatial_neighbors;/* 1 (at most 6 are used) */
     uint32_t restir_max_m;            /* 24: history cap on reuse */
     float restir_spatial_radius;      /* 2.75: neighbour offset in voxels */
+    /* dual-channel lBuffer (VE_FRAME_LBUFFER), core.hpp:93-104, 150-157 */
+    uint32_t time;                    /* the caller's clock for the stale reset (the reference: 1/100 s) */
+    uint32_t update_time;             /* a slot older than this is reset on its next deposit */
+    uint32_t disable_stale_reset;
+    uint32_t sample_cap_direct;       /* 16: the direct channel halves at this count */
+    uint32_t sample_cap_indirect;     /* 64 */
+    float firefly_k;                  /* 1: a sample above k x the running mean is scaled down */
+    float firefly_floor;              /* 255: lower bound of that threshold (quantised units) */
 } ve_frame_config;
 
 #define VE_RESTIR_ENABLE 1u   /* ReSTIR DI at bounce 0 (else single-pick RIS there too) */
@@ -269,6 +279,12 @@ int ve_set_materials(ve_ctx* ctx, const void* entries, uint32_t n);
 int ve_cache_reset(ve_ctx* ctx, int32_t scene_id);
 int ve_cache_dump(ve_ctx* ctx, int32_t scene_id, uint32_t* vids, uint32_t* counts, float* values, uint64_t cap,
                   uint64_t* n);
+/* The scene's dual-channel lBuffer (VE_FRAME_LBUFFER frames): every occupied
+ * slot as 14 u32 {row, slot, vid, dir count, dir r, g, b, dir L^2, ind count,
+ * ind r, g, b, ind L^2, last time} in (row, slot) order; `n` = the occupied
+ * slots (records written: min(n, cap)).  Nothing before the first lBuffer
+ * frame. */
+int ve_lbuffer_dump(ve_ctx* ctx, int32_t scene_id, uint32_t* out, uint64_t cap, uint64_t* n);
 
 /* Renderer::run (src/renderer/renderer.hpp:13, renderer.cpp:282-712): one
  * frame of one view.  Returns after the host outputs are written; with all

@@ -35,7 +35,10 @@ class FrameParams(ctypes.Structure):
                 ("pixels_norm", ctypes.c_float), ("top_fraction", ctypes.c_float), ("mid_fraction", ctypes.c_float),
                 ("min_samples", _U32), ("shading_budget", _U32),
                 ("restir", _U32), ("restir_m", _U32), ("restir_spatial_neighbors", _U32), ("restir_max_m", _U32),
-                ("restir_spatial_radius", ctypes.c_float)]
+                ("restir_spatial_radius", ctypes.c_float),
+                ("time", _U32), ("update_time", _U32), ("disable_stale_reset", _U32),
+                ("sample_cap_direct", _U32), ("sample_cap_indirect", _U32),
+                ("firefly_k", ctypes.c_float), ("firefly_floor", ctypes.c_float)]
 
 
 class Stats(ctypes.Structure):
@@ -88,6 +91,9 @@ class Oracle:
         L.oracle_shading_normal.argtypes = [_U32, _np(np.float32), _np(np.float32)]
         L.oracle_renderer_new.restype = _P
         L.oracle_renderer_free.argtypes = [_P]
+        L.oracle_lb_apply.argtypes = [_np(np.uint32), _U64, ctypes.POINTER(FrameParams), _np(np.uint32)]
+        L.oracle_lbuffer_dump.restype = _U64
+        L.oracle_lbuffer_dump.argtypes = [_P, _P, _U64]
         L.oracle_cache_dump.restype = _U64
         L.oracle_cache_dump.argtypes = [_P, _P, _P, _P, _U64]
         L.oracle_render_frame.restype = ctypes.c_int
@@ -138,6 +144,14 @@ class Oracle:
         self.lib.oracle_raycast_batch(w, w.size, depth, o.reshape(-1), d.reshape(-1), o.shape[0], controlchecks,
                                       threads, out.reshape(-1))
         return out
+
+    LB_WIDTH, LB_SLOTS, LB_STRIDE = 32768, 32, 12
+
+    def lb_apply(self, records: np.ndarray, params, table: np.ndarray) -> None:
+        """depositSampleDual of (n, 8) u32 records {vid, 0, d.rgb f32, e.rgb f32}
+        in order, on `table` ((32768 * 32 * 12,) u32, modified in place)."""
+        r = np.ascontiguousarray(records, np.uint32)
+        self.lib.oracle_lb_apply(r.reshape(-1), r.shape[0], ctypes.byref(params), table)
 
     def pow_unit(self, x, e) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float32)
@@ -200,6 +214,13 @@ class OracleRenderer:
         assert rc == 0
         stats = {k: getattr(st, k) for k, _ in Stats._fields_}
         return {"gbuffer": gbuf, "rgb": rgb, "mapped": mapped, "path_rgb": path_rgb, "stats": stats}
+
+    def lbuffer(self) -> np.ndarray:
+        """Occupied lBuffer slots, (n, 14) u32 rows {row, slot, 12 slot words}."""
+        n = self.o.lib.oracle_lbuffer_dump(self.h, None, 0)
+        out = np.zeros((n, 14), np.uint32)
+        self.o.lib.oracle_lbuffer_dump(self.h, out.ctypes.data, n)
+        return out
 
     def cache(self):
         n = self.o.lib.oracle_cache_dump(self.h, None, None, None, 0)
@@ -310,9 +331,11 @@ def frame_params(fc) -> FrameParams:
     p.variance_norm = float(fc.variance_norm)
     for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction"):
         setattr(p, f, float(getattr(fc, f, FrameParams_defaults[f])))
-    for f in ("min_samples", "shading_budget", "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m"):
+    for f in ("min_samples", "shading_budget", "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m",
+              "time", "update_time", "disable_stale_reset", "sample_cap_direct", "sample_cap_indirect"):
         setattr(p, f, int(getattr(fc, f, FrameParams_defaults[f])))
-    p.restir_spatial_radius = float(getattr(fc, "restir_spatial_radius", FrameParams_defaults["restir_spatial_radius"]))
+    for f in ("restir_spatial_radius", "firefly_k", "firefly_floor"):
+        setattr(p, f, float(getattr(fc, f, FrameParams_defaults[f])))
     return p
 
 
@@ -321,4 +344,7 @@ FrameParams_defaults = {"weight_pixels": 0.1, "weight_variance": 0.9, "pixels_no
                         "mid_fraction": 0.40, "min_samples": 1, "shading_budget": 131072,
                         # core.hpp:138-144 ReSTIR defaults (enable | temporal | spatial)
                         "restir": 7, "restir_m": 4, "restir_spatial_neighbors": 1, "restir_max_m": 24,
-                        "restir_spatial_radius": 2.75}
+                        "restir_spatial_radius": 2.75,
+                        # core.hpp:93-104, 150-157 lBuffer defaults
+                        "time": 0, "update_time": 0, "disable_stale_reset": 0, "sample_cap_direct": 16,
+                        "sample_cap_indirect": 64, "firefly_k": 1.0, "firefly_floor": 255.0}

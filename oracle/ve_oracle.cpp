@@ -563,6 +563,8 @@ void run_parallel(uint32_t n, uint32_t threads, F&& fn) {
 struct Deposit {
     uint32_t vid;
     float rgb[3];
+    uint32_t slot;      // the path's slot (lBuffer frames apply deposits in slot order)
+    float d[3], e[3];   // clamped direct and indirect radiance (lBuffer frames)
 };
 
 struct PathOut {
@@ -961,6 +963,88 @@ inline void deposit_value(const PathOut& p, float out[3]) {
     }
 }
 
+// The two channels of a deposit apart (packRgbL2 of each, shade.comp:162-167).
+inline void deposit_dual(const PathOut& p, float d[3], float e[3]) {
+    const float dv[3] = {p.direct.x, p.direct.y, p.direct.z};
+    const float iv[3] = {p.indirect.x, p.indirect.y, p.indirect.z};
+    for (int c = 0; c < 3; c++) {
+        float a = dv[c], b = iv[c];
+        if (!(a == a)) a = 0.0f;
+        if (!(b == b)) b = 0.0f;
+        d[c] = gclamp(a, 0.0f, 1024.0f) + 0.0f;
+        e[c] = 0.0f + gclamp(b, 0.0f, 1024.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The reference's dual-channel lBuffer (shade.comp:96-257 depositSampleDual,
+// resolve.comp:109-148 lookupVoxelAvg, rank.comp:66-87), rows of 32 slots x
+// 12 words, applied sequentially in (row, path slot) order per frame.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kFrameLbuffer = 256;  // VE_FRAME_LBUFFER
+constexpr uint32_t kLbWidth = 32768, kLbSlots = 32, kLbStride = 12, kLbRowWords = kLbSlots * kLbStride;
+inline uint32_t lb_row(uint32_t vid) { return vid % (kLbWidth - 1u) + 1u; }
+inline void lb_pack(const float c[3], uint32_t out[4]) {  // packRgbL2 (shade.comp:154-160)
+    for (int k = 0; k < 3; k++) out[k] = uint32_t(gclamp(c[k], 0.0f, 1024.0f) * 255.0f);
+    const uint32_t L = (out[0] + out[1] + out[2]) / 3u;
+    out[3] = L * L;
+}
+inline void lb_reset(uint32_t* s, uint32_t vid, const uint32_t d[4], const uint32_t e[4], uint32_t time) {
+    s[0] = vid;
+    s[1] = 1u; s[2] = d[0]; s[3] = d[1]; s[4] = d[2]; s[5] = d[3];
+    s[6] = 1u; s[7] = e[0]; s[8] = e[1]; s[9] = e[2]; s[10] = e[3];
+    s[11] = time;
+}
+inline void lb_firefly(const uint32_t* s, uint32_t c[4], const ov_frame_params& P) {  // s: the channel's count
+    const uint32_t n = s[0];
+    if (n > 4u) {
+        const float meanL = float(s[1] + s[2] + s[3]) / float(3u * n);
+        const float sampleL = float(c[0] + c[1] + c[2]) / 3.0f;
+        const float thresh = gmax(meanL * P.firefly_k, P.firefly_floor);
+        if (sampleL > thresh) {
+            const float scale = thresh / sampleL;
+            c[0] = uint32_t(float(c[0]) * scale);
+            c[1] = uint32_t(float(c[1]) * scale);
+            c[2] = uint32_t(float(c[2]) * scale);
+            const uint32_t L = (c[0] + c[1] + c[2]) / 3u;
+            c[3] = L * L;
+        }
+    }
+}
+void lb_deposit(uint32_t* row, uint32_t vid, const float dir[3], const float ind[3], const ov_frame_params& P) {
+    uint32_t d[4], e[4];
+    lb_pack(dir, d);
+    lb_pack(ind, e);
+    uint32_t cand_t = 0xFFFFFFFFu, cand_i = 0u;
+    for (uint32_t i = 0; i < kLbSlots; i++) {
+        uint32_t* s = row + i * kLbStride;
+        if (s[0] == 0u) s[0] = vid;
+        const uint32_t id = s[0], t = s[11];
+        if (id != vid) {
+            if (t < cand_t) {
+                cand_t = t;
+                cand_i = i;
+            }
+            continue;
+        }
+        if (!P.disable_stale_reset && t != 0u && t + P.update_time < P.time) {
+            lb_reset(s, vid, d, e, P.time);
+            return;
+        }
+        if (s[1] >= P.sample_cap_direct)
+            for (int k = 1; k <= 5; k++) s[k] >>= 1;
+        if (s[6] >= P.sample_cap_indirect)
+            for (int k = 6; k <= 10; k++) s[k] >>= 1;
+        lb_firefly(s + 1, d, P);
+        lb_firefly(s + 6, e, P);
+        s[1] += 1u; s[2] += d[0]; s[3] += d[1]; s[4] += d[2]; s[5] += d[3];
+        s[6] += 1u; s[7] += e[0]; s[8] += e[1]; s[9] += e[2]; s[10] += e[3];
+        s[11] = P.time;
+        return;
+    }
+    if (cand_t != 0xFFFFFFFFu) lb_reset(row + cand_i * kLbStride, vid, d, e, P.time);
+}
+
 // lookupVoxelAvg (resolve.comp:109-148) over the FP64 cache.
 struct Avg {
     double rgb[3];
@@ -982,6 +1066,55 @@ Avg lookup_avg(const Cache& c, uint32_t vid) {
     return a;
 }
 
+// lookupVoxelAvg (resolve.comp:109-148) over the lBuffer, in the device's
+// float operations.
+Avg lb_lookup(const std::vector<uint32_t>& lb, uint32_t vid) {
+    Avg a{{0, 0, 0}, 0, 0};
+    if (vid == 0 || lb.empty()) return a;
+    const uint32_t* row = lb.data() + size_t(lb_row(vid)) * kLbRowWords;
+    for (uint32_t i = 0; i < kLbSlots; i++) {
+        const uint32_t* s = row + i * kLbStride;
+        if (s[0] != vid) continue;
+        const uint32_t dc = s[1], ic = s[6];
+        a.count = uint64_t(dc) + ic;
+        if (dc + ic == 0u) return a;
+        float da[3] = {0, 0, 0}, ia[3] = {0, 0, 0};
+        float var = 0.0f;
+        if (dc > 0u) {
+            const float inv = 1.0f / float(dc);
+            for (int k = 0; k < 3; k++) da[k] = float(s[2 + k]) * inv / 255.0f;
+        }
+        if (ic > 0u) {
+            const float inv = 1.0f / float(ic);
+            for (int k = 0; k < 3; k++) ia[k] = float(s[7 + k]) * inv / 255.0f;
+            const float meanL = float(s[7] + s[8] + s[9]) * inv / 3.0f;
+            var = gmax(float(s[10]) * inv - meanL * meanL, 0.0f) / (255.0f * 255.0f);
+        }
+        for (int k = 0; k < 3; k++) a.rgb[k] = double(da[k] + ia[k]);
+        a.count = uint32_t(dc + ic);
+        a.var = double(var);
+        return a;
+    }
+    return a;
+}
+// lookupIndirectVariance (rank.comp:66-87), raw quantised units.
+float lb_indirect_variance(const std::vector<uint32_t>& lb, uint32_t vid) {
+    if (lb.empty()) return 0.0f;
+    const uint32_t* row = lb.data() + size_t(lb_row(vid)) * kLbRowWords;
+    for (uint32_t i = 0; i < kLbSlots; i++) {
+        const uint32_t* s = row + i * kLbStride;
+        if (s[0] == 0u) return 0.0f;
+        if (s[0] != vid) continue;
+        const uint32_t c = s[6];
+        if (c < 2u) return 0.0f;
+        const float fc = float(c);
+        const float meanL = float(s[7] + s[8] + s[9]) / (3.0f * fc);
+        const float meanL2 = float(s[10]) / fc;
+        return gmax(meanL2 - meanL * meanL, 0.0f);
+    }
+    return 0.0f;
+}
+
 inline double aces(double x) {  // final.frag:11-18
     double v = (x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14);
     return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
@@ -999,6 +1132,8 @@ struct Renderer {
     std::vector<EmLight> lights;
     std::unordered_set<uint32_t> em_claimed;
     std::unordered_map<uint32_t, Reservoir> res;
+    std::vector<uint32_t> lb;  // lBuffer frames: kLbWidth rows x 32 slots x 12 words
+    Avg lookup(bool lbm, uint32_t vid) const { return lbm ? lb_lookup(lb, vid) : lookup_avg(cache, vid); }
 };
 
 // End of an emissive frame: new lights in vid order fill the registry up to
@@ -1084,10 +1219,15 @@ void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t 
         const Claim& cl = claims[vid];
         if (cl.pix != pix) continue;
         nvox++;
-        const Avg a = lookup_avg(R->cache, vid);
-        const float var = a.count >= 2u ? float(a.var) : 0.0f;
         const float pn = gclamp(float(cl.count) / gmax(P->pixels_norm, 1.0f), 0.0f, 1.0f);
-        const float vn = gclamp(var * (255.0f * 255.0f) / gmax(P->variance_norm, 1.0f), 0.0f, 1.0f);
+        float vn;
+        if (P->flags & kFrameLbuffer) {  // rank.comp:107 on the lBuffer's own scale
+            vn = gclamp(lb_indirect_variance(R->lb, vid) / gmax(P->variance_norm, 1.0f), 0.0f, 1.0f);
+        } else {
+            const Avg a = lookup_avg(R->cache, vid);
+            const float var = a.count >= 2u ? float(a.var) : 0.0f;
+            vn = gclamp(var * (255.0f * 255.0f) / gmax(P->variance_norm, 1.0f), 0.0f, 1.0f);
+        }
         const float imp = P->weight_pixels * pn + P->weight_variance * vn;
         const uint32_t n = imp >= R->t_high ? 2u : (imp >= R->t_mid ? 1u : P->min_samples);
         uint32_t bin = uint32_t(imp * float(kRankBins));
@@ -1131,6 +1271,8 @@ void schedule_frame(Renderer* R, const Scene& s, const Material* mats, uint32_t 
             Deposit dp;
             dp.vid = vid;
             deposit_value(po, dp.rgb);
+            dp.slot = uint32_t(i);
+            deposit_dual(po, dp.d, dp.e);
             if (path_rgb) {
                 float* o = path_rgb + 3 * uint64_t(i);
                 o[0] = dp.rgb[0]; o[1] = dp.rgb[1]; o[2] = dp.rgb[2];
@@ -1328,6 +1470,40 @@ void oracle_shading_normal(uint32_t leaf_word, const float dir[3], float out[3])
 }
 
 void* oracle_renderer_new() { return new Renderer(); }
+
+// depositSampleDual over a caller's table (kLbWidth rows x 32 x 12 words):
+// records of 8 words {vid, unused, d.rgb (f32), e.rgb (f32)} applied in the
+// given order (pinned in tests against a transcription of the shader).
+void oracle_lb_apply(const uint32_t* rec, uint64_t n, const ov_frame_params* P, uint32_t* table) {
+    for (uint64_t i = 0; i < n; i++) {
+        const uint32_t* r = rec + 8 * i;
+        float d[3], e[3];
+        std::memcpy(d, r + 2, 12);
+        std::memcpy(e, r + 5, 12);
+        lb_deposit(table + size_t(lb_row(r[0])) * kLbRowWords, r[0], d, e, *P);
+    }
+}
+
+// The lBuffer's occupied slots as {row, slot, 12 words} records in (row,
+// slot) order (the layout of the product's ve_lbuffer_dump); returns the
+// number of occupied slots.
+uint64_t oracle_lbuffer_dump(void* rp, uint32_t* out, uint64_t cap) {
+    const Renderer* R = static_cast<Renderer*>(rp);
+    uint64_t k = 0;
+    if (R->lb.empty()) return 0;
+    for (uint32_t r = 0; r < kLbWidth; r++)
+        for (uint32_t i = 0; i < kLbSlots; i++) {
+            const uint32_t* w = R->lb.data() + size_t(r) * kLbRowWords + i * kLbStride;
+            if (w[0] == 0u) continue;
+            if (out && k < cap) {
+                out[14 * k] = r;
+                out[14 * k + 1] = i;
+                std::memcpy(out + 14 * k + 2, w, kLbStride * 4);
+            }
+            k++;
+        }
+    return k;
+}
 void oracle_renderer_free(void* r) { delete static_cast<Renderer*>(r); }
 
 // Number of cache entries and a dump: vids[i], counts[i], and
@@ -1384,8 +1560,10 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     std::vector<Hit> hits(sched ? size_t(W) * H : 0);
     std::vector<uint32_t> vids(sched ? size_t(W) * H : 0, 0u);
 
-    // temporal decay of the cache before this frame's deposits
-    run_parallel(kShards, threads, [&](uint32_t sh) {
+    const bool lbm = (P->flags & kFrameLbuffer) != 0;
+    // temporal decay of the cache before this frame's deposits (the lBuffer
+    // has none: its channels halve at their sample caps)
+    if (!lbm) run_parallel(kShards, threads, [&](uint32_t sh) {
         for (auto& kv : R->cache.map[sh]) {
             CacheEntry& e = kv.second;
             const double k = P->decay;
@@ -1445,6 +1623,8 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                     Deposit dp;
                     dp.vid = vid;
                     deposit_value(po, dp.rgb);
+                    dp.slot = pix * P->spp + smp;
+                    deposit_dual(po, dp.d, dp.e);
                     if (path_rgb) {
                         float* o = path_rgb + 3 * (uint64_t(pix) * P->spp + smp);
                         o[0] = dp.rgb[0]; o[1] = dp.rgb[1]; o[2] = dp.rgb[2];
@@ -1476,7 +1656,18 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         for (uint32_t sh = 0; sh < kShards; sh++) total.deposits += deps[t][sh].size();
     }
     if (!ems.empty()) commit_emissive(R, ems, &total);
-    run_parallel(kShards, threads, [&](uint32_t sh) {
+    if (lbm) {  // AccumPass into the lBuffer: every deposit, in (row, path slot) order
+        if (R->lb.empty()) R->lb.assign(size_t(kLbWidth) * kLbRowWords, 0u);
+        std::vector<const Deposit*> all;
+        for (uint32_t t = 0; t < threads; t++)
+            for (uint32_t sh = 0; sh < kShards; sh++)
+                for (const Deposit& d : deps[t][sh]) all.push_back(&d);
+        std::sort(all.begin(), all.end(), [](const Deposit* x, const Deposit* y) {
+            const uint32_t rx = lb_row(x->vid), ry = lb_row(y->vid);
+            return rx != ry ? rx < ry : x->slot < y->slot;
+        });
+        for (const Deposit* d : all) lb_deposit(R->lb.data() + size_t(lb_row(d->vid)) * kLbRowWords, d->vid, d->d, d->e, *P);
+    } else run_parallel(kShards, threads, [&](uint32_t sh) {
         auto& m = R->cache.map[sh];
         for (uint32_t t = 0; t < threads; t++)
             for (const Deposit& d : deps[t][sh]) {
@@ -1514,7 +1705,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                             if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
                             const uint32_t nv = gb(qx, qy, 3), nc = gb(qx, qy, 0);
                             if (nv == 0 || nc >= P->primary_controlchecks) continue;
-                            Avg a = lookup_avg(R->cache, nv);
+                            Avg a = R->lookup(lbm, nv);
                             if (a.count == 0) continue;
                             const double dist = double(dx * dx + dy * dy);
                             const double w = double(std::min<uint64_t>(a.count, 32)) / (1.0 + dist * 0.15);
@@ -1560,7 +1751,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                     case 5:  // VARIANCE
                         if (vid == 0) miss();
                         else {
-                            Avg a = lookup_avg(R->cache, vid);
+                            Avg a = R->lookup(lbm, vid);
                             double v = a.count >= 2 ? a.var : 0.0;
                             double sc = v * (255.0 * 255.0) / std::max<double>(P->variance_norm, 1.0);
                             sc = sc < 0 ? 0 : (sc > 1 ? 1 : sc);
@@ -1569,7 +1760,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                         break;
                     default: {  // DEFAULT
                         if (vid == 0) { miss(); break; }
-                        Avg a = lookup_avg(R->cache, vid);
+                        Avg a = R->lookup(lbm, vid);
                         if (a.count >= 128 && a.var < 0.02) {
                             for (int c = 0; c < 3; c++) col[c] = a.rgb[c];
                             break;
@@ -1581,7 +1772,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                             if (qx < 0 || qy < 0 || qx >= W || qy >= H) continue;
                             const uint32_t nv = gb(qx, qy, 3);
                             if (nv == 0 || nv == vid) continue;
-                            Avg na = lookup_avg(R->cache, nv);
+                            Avg na = R->lookup(lbm, nv);
                             if (na.count == 0) continue;
                             const double d0 = na.rgb[0] - a.rgb[0], d1 = na.rgb[1] - a.rgb[1],
                                          d2 = na.rgb[2] - a.rgb[2];

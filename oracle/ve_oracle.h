@@ -37,6 +37,9 @@ struct ov_frame_params {
     /* emissive NEE (flags & 128), core.hpp:138-144 */
     uint32_t restir, restir_m, restir_spatial_neighbors, restir_max_m;
     float restir_spatial_radius;
+    /* dual-channel lBuffer (flags & 256), core.hpp:93-104, 150-157 */
+    uint32_t time, update_time, disable_stale_reset, sample_cap_direct, sample_cap_indirect;
+    float firefly_k, firefly_floor;
 };
 
 struct ov_stats {

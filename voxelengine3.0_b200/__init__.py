@@ -48,6 +48,7 @@ FRAME_TERMINATE_HASH = 16
 FRAME_TRAIN = 32
 FRAME_SCHEDULED = 64
 FRAME_EMISSIVE = 128
+FRAME_LBUFFER = 256
 RESTIR_ENABLE = 1
 RESTIR_TEMPORAL = 2
 RESTIR_SPATIAL = 4
@@ -81,7 +82,11 @@ class FrameConfigC(ctypes.Structure):
                 ("min_samples", ctypes.c_uint32), ("shading_budget", ctypes.c_uint32),
                 ("restir", ctypes.c_uint32), ("restir_m", ctypes.c_uint32),
                 ("restir_spatial_neighbors", ctypes.c_uint32), ("restir_max_m", ctypes.c_uint32),
-                ("restir_spatial_radius", ctypes.c_float)]
+                ("restir_spatial_radius", ctypes.c_float),
+                ("time", ctypes.c_uint32), ("update_time", ctypes.c_uint32),
+                ("disable_stale_reset", ctypes.c_uint32), ("sample_cap_direct", ctypes.c_uint32),
+                ("sample_cap_indirect", ctypes.c_uint32), ("firefly_k", ctypes.c_float),
+                ("firefly_floor", ctypes.c_float)]
 
 
 class ViewC(ctypes.Structure):
@@ -181,6 +186,7 @@ _SIGNATURES = {
     "ve_scene_download": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
     "ve_scene_footprint": ([_P, _I32, _PTR(_U64)], ctypes.c_int),
     "ve_raycast_batch": ([_P, _I32, _P, _P, _U64, _U32, _U32, _P], ctypes.c_int),
+    "ve_lbuffer_dump": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
     "ve_set_materials": ([_P, _P, _U32], ctypes.c_int),
     "ve_cache_reset": ([_P, _I32], ctypes.c_int),
     "ve_cache_dump": ([_P, _I32, _P, _P, _P, _U64, _PTR(_U64)], ctypes.c_int),
@@ -449,12 +455,21 @@ class FrameConfig:
     restir_spatial_neighbors: int = 1
     restir_max_m: int = 24
     restir_spatial_radius: float = 2.75
+    # dual-channel lBuffer (FRAME_LBUFFER), core.hpp:93-104, 150-157 defaults
+    time: int = 0
+    update_time: int = 0
+    disable_stale_reset: int = 0
+    sample_cap_direct: int = 16
+    sample_cap_indirect: int = 64
+    firefly_k: float = 1.0
+    firefly_floor: float = 255.0
 
     def to_c(self) -> FrameConfigC:
         c = FrameConfigC()
         for f in ("width", "height", "spp", "bounces", "primary_controlchecks", "bounce_controlchecks",
                   "reconstruction_radius", "render_type", "frame_index", "flags", "min_samples", "shading_budget",
-                  "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m"):
+                  "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m", "time", "update_time",
+                  "disable_stale_reset", "sample_cap_direct", "sample_cap_indirect"):
             setattr(c, f, int(getattr(self, f)))
         for i in range(3):
             c.sun_dir[i] = float(self.sun_dir[i])
@@ -463,7 +478,7 @@ class FrameConfig:
         c.decay = float(self.decay)
         c.variance_norm = float(self.variance_norm)
         for f in ("weight_pixels", "weight_variance", "pixels_norm", "top_fraction", "mid_fraction",
-                  "restir_spatial_radius"):
+                  "restir_spatial_radius", "firefly_k", "firefly_floor"):
             setattr(c, f, float(getattr(self, f)))
         return c
 
@@ -563,6 +578,14 @@ class Renderer:
         p = np.ascontiguousarray(np.asarray(positions, np.uint32).reshape(-1, 3))
         _check(self._lib.ve_scene_refresh(self._h, scene_id, _ptr(p) if p.size else None, p.shape[0],
                                           1 if keep_cache else 0))
+
+    def lbuffer_dump(self, scene_id: int) -> np.ndarray:
+        """Occupied lBuffer slots, (n, 14) u32 rows {row, slot, 12 slot words}."""
+        n = _U64()
+        _check(self._lib.ve_lbuffer_dump(self._h, scene_id, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 14), np.uint32)
+        _check(self._lib.ve_lbuffer_dump(self._h, scene_id, _ptr(out), n.value, ctypes.byref(n)))
+        return out
 
     def raycast_batch(self, scene_id: int, origins: np.ndarray, dirs: np.ndarray, controlchecks: int = 300,
                       full_walk: bool = False) -> np.ndarray:

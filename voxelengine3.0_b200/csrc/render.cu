@@ -29,6 +29,7 @@
 #include "../../include/ve.h"
 #include "builder.cuh"
 #include "emissive.cuh"
+#include "lbuffer.cuh"
 #include "nrc.cuh"
 #include "raycast.cuh"
 #include "ve_device.cuh"
@@ -63,6 +64,7 @@ struct DevScene {
     uint32_t* em_state;   // {registered lights, lights staged this frame}
     EmLight* em_stage;    // lights found this frame, appended at its end
     ResEntry* res;        // per-voxel ReSTIR reservoirs, 2^kResLog2 entries
+    uint32_t* lbuf;       // the dual-channel lBuffer (VE_FRAME_LBUFFER; null until first used)
 };
 
 struct DevMaterial {
@@ -89,6 +91,9 @@ struct DevView {
     uint32_t restir, restir_m, restir_nbrs, restir_max_m;
     float restir_radius;
     uint32_t pad2, pad3, pad4;
+    // dual-channel lBuffer (core.hpp:93-104, 150-157 knobs)
+    LbParams lb;
+    uint32_t pad5;
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
@@ -96,6 +101,7 @@ constexpr uint32_t kDefaultRefill = 24;  // trace refill threshold (idle lanes o
 enum : uint32_t {
     CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_RES = 63,
     CNT_RAYSH = 64,  // shadow rays per pass (extension rays: CNT_RAY)
+    CNT_LB = 84,     // lBuffer deposit records of the frame
     CNT_TOTAL = 96
 };
 enum : uint32_t {
@@ -120,6 +126,10 @@ enum : uint32_t {
     ST_TOTAL = 19
 };
 enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u };
+// Shading-kernel instances: emissive NEE (VE_FRAME_EMISSIVE) and the
+// dual-channel lBuffer AccumPass (VE_FRAME_LBUFFER) compile into their own
+// instances so the plain kernels keep their registers.
+constexpr int kModeEm = 1, kModeLb = 2;
 // a cached voxel average ends a path (VE_FRAME_TERMINATE_HASH, and the
 // learned cache's fallback) only when at least this many deposits made it
 constexpr uint32_t kHashTermMinCount = 8;
@@ -143,6 +153,7 @@ struct FrameArgs {
     float4* p_sdir;      // emissive batches: NEE shadow direction, w = the light's vid (~0 for the sun)
     PathRes* p_res;      // emissive batches: a path's bounce-0 reservoir until the commit
     uint32_t* res_list;  // paths holding a reservoir (counter CNT_RES)
+    LbRec* lb_rec;       // lBuffer frames: the frame's deposits (counter CNT_LB)
     uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
     uint32_t* live[2];
@@ -487,6 +498,17 @@ __device__ __forceinline__ Avg lookup_avg(const DevScene& S, uint32_t vid) {
     return r;
 }
 
+// The view's radiance cache: the dual-channel lBuffer (VE_FRAME_LBUFFER) or
+// the FP32 per-voxel cache.
+__device__ __forceinline__ Avg lookup_view(const DevView& v, const DevScene& S, uint32_t vid) {
+    if ((v.flags & VE_FRAME_LBUFFER) && S.lbuf) {
+        Avg r;
+        lb_lookup(S.lbuf, vid, r.rgb, r.count, r.var);
+        return r;
+    }
+    return lookup_avg(S, vid);
+}
+
 // Octahedral map of a unit vector to [-1, 1]^2 (Cigolle et al. 2014): the
 // learned cache's normal and direction inputs.
 __device__ __forceinline__ float2 oct_encode(f3 v) {
@@ -540,6 +562,7 @@ struct ShadeOut {
     bool want_q = false, sampled = false, hash_term = false;
     bool app_res = false, em_nee = false;  // a reservoir to commit; an emissive NEE shadow ray
     float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
+    float ir = 0.0f, ig = 0.0f, ib = 0.0f;  // lBuffer frames: dr..db direct, ir..ib indirect
     uint32_t dvid = 0, dscene = 0, dview = 0;
 };
 
@@ -705,9 +728,11 @@ __device__ __forceinline__ void emissive_nee(const FrameArgs& a, const DevView& 
 // F_TERM), tp/direct/indirect the path state after any pending sun term was
 // resolved.  Writes the continuing path's state; the queue appends and the
 // AccumPass deposit are left to shade_emit.
-template <bool EM>
+template <int MODE>
 __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4 meta, f3 tp, f3 direct,
                                            f3 indirect, f3 dir, uint4 hit, ShadeOut& o) {
+    constexpr bool EM = (MODE & kModeEm) != 0;
+    constexpr bool LB = (MODE & kModeLb) != 0;
     const uint32_t vi = meta.z & 0xFFFFu;
     uint32_t b = (meta.z >> 16) & 0xFFu;
     const uint32_t flags = meta.z >> 24;
@@ -892,6 +917,12 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
     }
     if (o.do_dep) {
         deposit_value(direct, indirect, o.dr, o.dg, o.db, o.dl2);
+        const float pr = o.dr, pg = o.dg, pb = o.db;  // the path's value (debug output)
+        if (LB) {  // the two channels apart (packRgbL2 of each, shade.comp:162-167)
+            float z;
+            deposit_value(direct, mk(0.0f, 0.0f, 0.0f), o.dr, o.dg, o.db, z);
+            deposit_value(mk(0.0f, 0.0f, 0.0f), indirect, o.ir, o.ig, o.ib, z);
+        }
         if ((flags | nf) & F_TRAIN) {  // training path: its target
             const uint32_t k = (nf & F_TRAIN) && !(flags & F_TRAIN) ? train_slot : a.p_aux[p];
             if (k < a.ns_cap) {
@@ -903,9 +934,9 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
         o.dscene = v.scene;
         o.dview = vi;
         if (a.path_rgb && (v.flags & VE_FRAME_PATH_RGB)) {
-            a.path_rgb[3ull * p + 0] = o.dr;
-            a.path_rgb[3ull * p + 1] = o.dg;
-            a.path_rgb[3ull * p + 2] = o.db;
+            a.path_rgb[3ull * p + 0] = pr;
+            a.path_rgb[3ull * p + 1] = pg;
+            a.path_rgb[3ull * p + 2] = pb;
         }
     }
 }
@@ -913,10 +944,12 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
 // The warp-collective part of a shading step: queue appends (live paths,
 // extension and shadow rays, learned-cache queries and samples) and the
 // warp-aggregated deposit.  Called by all 32 lanes.
-template <bool EM>
+template <int MODE>
 __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const ShadeOut& o, uint32_t* live_out,
                                            uint32_t* live_cnt, uint32_t* ray_cnt, DepSlot* dep, BlockQ& q,
                                            EmitCounts& cnt) {
+    constexpr bool EM = (MODE & kModeEm) != 0;
+    constexpr bool LB = (MODE & kModeLb) != 0;
     const uint3 s = block_append3(o.app_live, o.app_ext, o.app_sh, live_cnt, ray_cnt,
                                   ray_cnt + (CNT_RAYSH - CNT_RAY), q);
     if (o.app_live) live_out[s.x] = p;
@@ -944,7 +977,20 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
         if (o.app_res) a.res_list[kr] = p;
         warp_add_stat(&a.stats[ST_EM_NEE], o.em_nee ? 1u : 0u);
     }
-    warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, cnt.dep, cnt.drop);
+    if (LB) {  // recorded; applied per lBuffer row at the end of the frame
+        const uint32_t k = warp_append(o.do_dep, &a.counters[CNT_LB]);
+        if (o.do_dep) {
+            LbRec r;
+            r.vid = o.dvid;
+            r.slot = p;
+            r.d[0] = o.dr; r.d[1] = o.dg; r.d[2] = o.db;
+            r.e[0] = o.ir; r.e[1] = o.ig; r.e[2] = o.ib;
+            a.lb_rec[k] = r;
+            cnt.dep++;
+        }
+    } else {
+        warp_deposit(o.do_dep, o.dscene, o.dvid, o.dr, o.dg, o.db, o.dl2, dep, a.scenes, cnt.dep, cnt.drop);
+    }
     if (a.remaining) {  // serving: count finished paths per view slot
         const unsigned dm = __ballot_sync(0xffffffffu, o.do_dep);
         if (o.do_dep) {
@@ -959,7 +1005,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
 // hit in registers (the same shade_step the shade pass runs), appending its
 // rays and live entry for trace pass 0 / shade pass 1 — the frame's largest
 // shade pass never round-trips the path state through memory.
-template <bool COUNT, bool FUSED, bool EM = false>
+template <bool COUNT, bool FUSED, int MODE = 0>
 __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     __shared__ DepSlot dep[FUSED ? 256 : 1];
     const uint32_t tile = blockIdx.x;
@@ -1024,10 +1070,10 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
                 // emit.comp:171-174
                 const uint32_t sample_idx = v.frame_index + spix * 2654435761u + list_idx * 1442695040u;
                 const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
-                shade_step<EM>(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
+                shade_step<MODE>(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
                            mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o);
             }
-            shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
+            shade_emit<MODE>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
                            dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
         }
         flush_counts(cnt, a.stats);
@@ -1063,8 +1109,9 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     }
 }
 
-template <bool EM = false>
+template <int MODE = 0>
 __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
+    constexpr bool EM = (MODE & kModeEm) != 0;
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
     const uint32_t* live_in = a.live[pass & 1u];
@@ -1094,9 +1141,9 @@ __global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
                 else indirect = add(indirect, ld3(pe));
             }
             const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
-            shade_step<EM>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
+            shade_step<MODE>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
         }
-        shade_emit<EM>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
+        shade_emit<MODE>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
     }
     flush_counts(cnt, a.stats);
 }
@@ -1174,10 +1221,15 @@ __global__ void __launch_bounds__(256) k_sched_rank(FrameArgs a) {
             const int c = vid ? claim_find(a, vid) : -1;
             if (c >= 0 && a.claim_pix[c] == pix) {
                 nvox++;
-                const Avg av = lookup_avg(S, vid);
-                const float var = av.count >= 2u ? av.var : 0.0f;
                 const float pn = gclamp(float(a.claim_cnt[c]) / gmax(v.pix_norm, 1.0f), 0.0f, 1.0f);
-                const float vn = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
+                float vn;
+                if ((v.flags & VE_FRAME_LBUFFER) && S.lbuf) {  // rank.comp:107 on the lBuffer's own scale
+                    vn = gclamp(lb_indirect_variance(S.lbuf, vid) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
+                } else {
+                    const Avg av = lookup_avg(S, vid);
+                    const float var = av.count >= 2u ? av.var : 0.0f;
+                    vn = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
+                }
                 const float imp = v.w_pix * pn + v.w_var * vn;
                 n = imp >= t_high ? 2u : (imp >= t_mid ? 1u : v.min_samples);
                 uint32_t bin = uint32_t(imp * float(kRankBins));
@@ -1238,7 +1290,7 @@ __global__ void k_sched_threshold(float* rank, const DevView* views) {
 // emit.comp: one path per shade-list entry, from the representative pixel's
 // primary hit, list index i seeding the RNG; its first shading step runs
 // here as in the fused primary pass.
-template <bool EM = false>
+template <int MODE = 0>
 __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
     __shared__ DepSlot dep[256];
     const DevView& v = a.views[0];
@@ -1263,11 +1315,11 @@ __global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
             // emit.comp:171-174 with listIdx = the shade-list index
             const uint32_t sample_idx = v.frame_index + pix * 2654435761u + i * 1442695040u;
             const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
-            shade_step<EM>(a, p, make_uint4(e.x, rng, 0u + a.view_offset, pix), mk(1.0f, 1.0f, 1.0f), mk(0.0f, 0.0f, 0.0f),
+            shade_step<MODE>(a, p, make_uint4(e.x, rng, 0u + a.view_offset, pix), mk(1.0f, 1.0f, 1.0f), mk(0.0f, 0.0f, 0.0f),
                        mk(0.0f, 0.0f, 0.0f), dir, make_uint4(kHit, hi.x, hi.y, hi.z), o);
             n_paths++;
         }
-        shade_emit<EM>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
+        shade_emit<MODE>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0], dep + (threadIdx.x & ~31u),
                        bq[it & 1u], cnt);
     }
     flush_counts(cnt, a.stats);
@@ -1329,6 +1381,69 @@ __global__ void __launch_bounds__(256) k_res_commit(FrameArgs a) {
         }
     }
     warp_add_stat(&a.stats[ST_RES_WRITES], w);
+}
+
+// ---------------------------------------------------------------------------
+// End-of-frame AccumPass of lBuffer frames: the deposits sorted by (row,
+// path slot), then one thread per row applies its run in that order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_lb_keys(const LbRec* rec, const uint32_t* counters, uint32_t cap,
+                                                 unsigned long long* keys, uint32_t* vals) {
+    const uint32_t n = min(counters[CNT_LB], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+        keys[i] = i < n ? (((unsigned long long)lb_row(rec[i].vid)) << 32) | rec[i].slot : ~0ull;
+        vals[i] = i;
+    }
+}
+__global__ void __launch_bounds__(256) k_lb_bounds(const unsigned long long* keys, const uint32_t* counters,
+                                                   uint32_t cap, uint32_t* start, uint32_t* end) {
+    const uint32_t n = min(counters[CNT_LB], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t row = uint32_t(keys[i] >> 32);
+        if (i == 0u || uint32_t(keys[i - 1] >> 32) != row) start[row] = i;
+        if (i + 1u == n || uint32_t(keys[i + 1] >> 32) != row) end[row] = i + 1u;
+    }
+}
+__global__ void __launch_bounds__(256) k_lb_apply(const DevScene* scenes, const DevView* views, const LbRec* rec,
+                                                  const uint32_t* order, const uint32_t* start,
+                                                  const uint32_t* end) {
+    const DevView& v = views[0];
+    uint32_t* lb = scenes[v.scene].lbuf;
+    const LbParams P = v.lb;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < kLbWidth; r += gridDim.x * blockDim.x) {
+        uint32_t* row = lb + size_t(r) * kLbRowWords;
+        for (uint32_t i = start[r]; i < end[r]; i++) {
+            const LbRec x = rec[order[i]];
+            lb_deposit(row, x.vid, x.d, x.e, P);
+        }
+    }
+}
+
+// Launches of the shading kernels' instances for a mode (kModeEm | kModeLb).
+template <bool COUNT>
+static void launch_primary(int mode, uint32_t grid, cudaStream_t st, const FrameArgs& a) {
+    switch (mode) {
+        case 0: k_primary<COUNT, true, 0><<<grid, 256, 0, st>>>(a); break;
+        case kModeEm: k_primary<COUNT, true, kModeEm><<<grid, 256, 0, st>>>(a); break;
+        case kModeLb: k_primary<COUNT, true, kModeLb><<<grid, 256, 0, st>>>(a); break;
+        default: k_primary<COUNT, true, kModeEm | kModeLb><<<grid, 256, 0, st>>>(a); break;
+    }
+}
+static void launch_shade(int mode, uint32_t grid, cudaStream_t st, const FrameArgs& a, uint32_t pass) {
+    switch (mode) {
+        case 0: k_shade<0><<<grid, 256, 0, st>>>(a, pass); break;
+        case kModeEm: k_shade<kModeEm><<<grid, 256, 0, st>>>(a, pass); break;
+        case kModeLb: k_shade<kModeLb><<<grid, 256, 0, st>>>(a, pass); break;
+        default: k_shade<kModeEm | kModeLb><<<grid, 256, 0, st>>>(a, pass); break;
+    }
+}
+static void launch_sched_emit(int mode, uint32_t grid, cudaStream_t st, const FrameArgs& a) {
+    switch (mode) {
+        case 0: k_sched_emit<0><<<grid, 256, 0, st>>>(a); break;
+        case kModeEm: k_sched_emit<kModeEm><<<grid, 256, 0, st>>>(a); break;
+        case kModeLb: k_sched_emit<kModeLb><<<grid, 256, 0, st>>>(a); break;
+        default: k_sched_emit<kModeEm | kModeLb><<<grid, 256, 0, st>>>(a); break;
+    }
 }
 
 // Staging of a learned-cache query in a frame (runs in the encode kernel, at
@@ -1414,7 +1529,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
                 const uint4 nd = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)];
                 if (nd.w == 0u || nd.x >= v.cc_primary) continue;
-                const Avg na = lookup_avg(S, nd.w);
+                const Avg na = lookup_view(v, S, nd.w);
                 if (na.count == 0u) continue;
                 const float dist = float(dx * dx + dy * dy);
                 const float w = float(na.count < 32u ? na.count : 32u) / (1.0f + dist * 0.15f);
@@ -1458,7 +1573,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
         case VE_RENDER_VARIANCE:
             if (vid == 0u) col = miss();
             else {
-                const Avg c = lookup_avg(S, vid);
+                const Avg c = lookup_view(v, S, vid);
                 const float var = c.count >= 2u ? c.var : 0.0f;
                 const float sc = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
                 col = mk(sc, sc, sc);
@@ -1469,7 +1584,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 col = miss();
                 break;
             }
-            const Avg c = lookup_avg(S, vid);
+            const Avg c = lookup_view(v, S, vid);
             if (c.count >= 128u && c.var < 0.02f) {
                 col = c.rgb;
                 break;
@@ -1482,7 +1597,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
                 const uint32_t nv = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)].w;
                 if (nv == 0u || nv == vid) continue;
-                const Avg na = lookup_avg(S, nv);
+                const Avg na = lookup_view(v, S, nv);
                 if (na.count == 0u) continue;
                 const f3 dd = sub(na.rgb, c.rgb);
                 const float dc = sqrtf(dot(dd, dd));
@@ -1647,6 +1762,7 @@ struct SceneSlot {
     uint32_t* em_state = nullptr;
     ve::EmLight* em_stage = nullptr;
     ve::ResEntry* res = nullptr;
+    uint32_t* lbuf = nullptr;  // dual-channel lBuffer (first VE_FRAME_LBUFFER frame)
 };
 
 template <typename T>
@@ -1719,6 +1835,10 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> res_list;      // ... and the paths that hold one
     ve::DevBuf<uint32_t> em_sort;       // registry commit: vid keys / staging indices, 2 x 2 x 2^17
     ve::DevBuf<uint8_t> em_sort_tmp;    // ... CUB radix-sort scratch
+    ve::DevBuf<ve::LbRec> lb_rec;        // lBuffer frames: deposits
+    ve::DevBuf<unsigned long long> lb_keys;  // ... their (row, slot) keys, 2 x paths
+    ve::DevBuf<uint32_t> lb_idx;         // ... sort values 2 x paths + row bounds 2 x rows
+    ve::DevBuf<uint8_t> lb_tmp;          // ... CUB radix-sort scratch
     ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
@@ -1777,7 +1897,7 @@ static int sync_scenes(ve_ctx* c) {
         const SceneSlot& s = c->scenes[i];
         h[i] = DevScene{s.nodes,     s.n_words,   s.cache,    s.depth,    c->cfg.hash_log2, c->cfg.hash_probes,
                         s.top_level, s.top,       s.em_list, s.em_claim, s.em_state,       s.em_stage,
-                        s.res};
+                        s.res,       s.lbuf};
     }
     const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
@@ -1942,6 +2062,20 @@ static int compute_normals(ve_ctx* c, SceneSlot& s) {
 
 // Scheduling thresholds {t_high = +inf, t_mid = -inf} and an empty histogram:
 // every voxel of the next scheduled frame falls in the middle tier.
+constexpr size_t kLbBytes = size_t(kLbWidth) * kLbRowWords * sizeof(uint32_t);
+
+static int ensure_lbuffer(ve_ctx* c, SceneSlot& s) {
+    if (s.lbuf) return VE_OK;
+    if (cudaMalloc(&s.lbuf, kLbBytes) != cudaSuccess) {
+        s.lbuf = nullptr;
+        return fail(VE_ERR_NOMEM, "render: lBuffer allocation failed");
+    }
+    VE_CUDA(cudaMemsetAsync(s.lbuf, 0, kLbBytes, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    c->scenes_dirty = true;
+    return VE_OK;
+}
+
 static void free_emissive(SceneSlot& s) {
     if (s.em_list) cudaFree(s.em_list);
     if (s.em_claim) cudaFree(s.em_claim);
@@ -2120,6 +2254,10 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         return fail(VE_ERR_INVALID, "render: VE_FRAME_SCHEDULED does not combine with the learned cache");
     if ((flags & VE_FRAME_EMISSIVE) && (flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN | VE_FRAME_TERMINATE_HASH)))
         return fail(VE_ERR_INVALID, "render: VE_FRAME_EMISSIVE does not combine with cache-terminated paths");
+    if ((flags & VE_FRAME_LBUFFER) && nv != 1)
+        return fail(VE_ERR_INVALID, "render: VE_FRAME_LBUFFER renders one view per call");
+    if ((flags & VE_FRAME_LBUFFER) && (flags & (VE_FRAME_LEARNED | VE_FRAME_TRAIN | VE_FRAME_TERMINATE_HASH)))
+        return fail(VE_ERR_INVALID, "render: VE_FRAME_LBUFFER does not combine with cache-terminated paths");
     for (uint32_t i = 0; i < nv; i++)
         if ((views[i].frame.flags & VE_FRAME_EMISSIVE) && views[i].frame.restir_m > 64)
             return fail(VE_ERR_INVALID, "render: restir_m must be <= 64");
@@ -2194,6 +2332,20 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         for (int i = 0; i < 5; i++)
             if (before[i] != after[i]) c->gen++;
     }
+    size_t lb_sort_bytes = 0;
+    if (flags & VE_FRAME_LBUFFER) {
+        if ((rc = ensure_lbuffer(c, c->scenes[views[0].scene_id]))) return rc;
+        cub::DeviceRadixSort::SortPairs(nullptr, lb_sort_bytes, (const unsigned long long*)nullptr,
+                                        (unsigned long long*)nullptr, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        int(paths), 0, 47, c->stream);
+        const void* before[] = {c->lb_rec.p, c->lb_keys.p, c->lb_idx.p, c->lb_tmp.p};
+        if ((rc = c->lb_rec.ensure(paths)) || (rc = c->lb_keys.ensure(2 * paths)) ||
+            (rc = c->lb_idx.ensure(2 * paths + 2ull * kLbWidth)) || (rc = c->lb_tmp.ensure(lb_sort_bytes)))
+            return rc;
+        const void* after[] = {c->lb_rec.p, c->lb_keys.p, c->lb_idx.p, c->lb_tmp.p};
+        for (int i = 0; i < 4; i++)
+            if (before[i] != after[i]) c->gen++;
+    }
     if ((rc = sync_scenes(c))) return rc;
     // view table, written into a staging slot whose previous copy has run
     const int slot = c->staging_next;
@@ -2230,6 +2382,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         d.restir_nbrs = f.restir_spatial_neighbors;
         d.restir_max_m = f.restir_max_m;
         d.restir_radius = f.restir_spatial_radius;
+        d.lb = LbParams{f.time, f.update_time, f.disable_stale_reset, f.sample_cap_direct, f.sample_cap_indirect,
+                        f.firefly_k, f.firefly_floor};
         d.pix_base = uint32_t(pix_base);
         d.tile_base = tile_base;
         d.path_base = path_base;
@@ -2264,7 +2418,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         const int sc = views[i].scene_id;
         bool seen = false;
         for (auto& d : decays) seen |= d.first == sc;
-        if (!seen) decays.emplace_back(sc, views[i].frame.decay);
+        // the lBuffer has no decay (its channels halve at their sample caps)
+        if (!seen && !(views[i].frame.flags & VE_FRAME_LBUFFER)) decays.emplace_back(sc, views[i].frame.decay);
     }
     FrameArgs a{};
     a.views = c->d_views.p;
@@ -2314,12 +2469,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         a.shade_cap = uint32_t(paths);
         a.rank = c->scenes[views[0].scene_id].rank;
     }
+    if (flags & VE_FRAME_LBUFFER) a.lb_rec = c->lb_rec.p;
     if (flags & VE_FRAME_EMISSIVE) {
         a.p_sdir = c->p_sdir.p;
         a.p_res = c->p_res.p;
         a.res_list = c->res_list.p;
     }
     const bool em = (flags & VE_FRAME_EMISSIVE) != 0;
+    const bool lbm = (flags & VE_FRAME_LBUFFER) != 0;
+    const int mode = (em ? kModeEm : 0) | (lbm ? kModeLb : 0);
     // the frame's kernel sequence (no host synchronisation inside)
     auto enqueue = [&]() {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
@@ -2336,13 +2494,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
         }
         rec();
-        if (em) {
-            if (count) k_primary<true, true, true><<<tiles, 256, 0, st>>>(a);
-            else k_primary<false, true, true><<<tiles, 256, 0, st>>>(a);
-        } else {
-            if (count) k_primary<true, true><<<tiles, 256, 0, st>>>(a);
-            else k_primary<false, true><<<tiles, 256, 0, st>>>(a);
-        }
+        if (count) launch_primary<true>(mode, tiles, st, a);
+        else launch_primary<false>(mode, tiles, st, a);
         launches++;
         if (sched) {  // schedule -> rank -> shade list -> thresholds -> emit
             cudaMemsetAsync(a.claim_key, 0, 4ull * claim_size, st);
@@ -2356,15 +2509,13 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, b, a.sched_n, a.sched_off, int(pixels), st);
             k_sched_list<<<g, 256, 0, st>>>(a);
             k_sched_threshold<<<1, 1, 0, st>>>(a.rank, a.views);
-            if (em) k_sched_emit<true><<<c->grid_shade, 256, 0, st>>>(a);
-            else k_sched_emit<<<c->grid_shade, 256, 0, st>>>(a);
+            launch_sched_emit(mode, c->grid_shade, st, a);
             launches += 6;
         }
         rec();
         for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
             if (pass > 0) {  // pass 0 runs inside the fused primary
-                if (em) k_shade<true><<<c->grid_shade, 256, 0, st>>>(a, pass);
-                else k_shade<<<c->grid_shade, 256, 0, st>>>(a, pass);
+                launch_shade(mode, c->grid_shade, st, a, pass);
                 launches++;
             }
             rec();
@@ -2396,6 +2547,22 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
             rec();
         }
+        if (lbm) {  // AccumPass: the frame's deposits into the lBuffer, row by row
+            const uint32_t capn = uint32_t(paths);
+            unsigned long long* kin = c->lb_keys.p;
+            unsigned long long* kout = kin + capn;
+            uint32_t* vin = c->lb_idx.p;
+            uint32_t* vout = vin + capn;
+            uint32_t* rs = vout + capn;
+            uint32_t* re = rs + kLbWidth;
+            cudaMemsetAsync(rs, 0, 2ull * kLbWidth * sizeof(uint32_t), st);
+            k_lb_keys<<<c->num_sms * 8, 256, 0, st>>>(c->lb_rec.p, c->counters.p, capn, kin, vin);
+            size_t b = lb_sort_bytes;
+            cub::DeviceRadixSort::SortPairs(c->lb_tmp.p, b, kin, kout, vin, vout, int(capn), 0, 47, st);
+            k_lb_bounds<<<c->num_sms * 8, 256, 0, st>>>(kout, c->counters.p, capn, rs, re);
+            k_lb_apply<<<kLbWidth / 256, 256, 0, st>>>(a.scenes, a.views, c->lb_rec.p, vout, rs, re);
+            launches += 4;
+        }
         k_resolve<<<tiles, 256, 0, st>>>(a);
         launches++;
         if (flags & VE_FRAME_EMISSIVE) {  // this frame's lights and reservoirs, for the next frame
@@ -2425,7 +2592,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
                                      flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
                                               VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED |
-                                              VE_FRAME_EMISSIVE),
+                                              VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER),
                                      paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
                                      uint64_t(c->launch.refill_threshold), uint64_t(uintptr_t(nrc)),
                                      uint64_t(a.nrc_ready)};
@@ -2656,6 +2823,7 @@ int ve_ctx_destroy(ve_ctx* c) {
         if (s.cache) cudaFree(s.cache);
         if (s.top) cudaFree(s.top);
         if (s.rank) cudaFree(s.rank);
+        if (s.lbuf) cudaFree(s.lbuf);
         free_emissive(s);
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
@@ -2667,6 +2835,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
     c->out_mapped.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
     c->p_sdir.release(); c->p_res.release(); c->res_list.release(); c->em_sort.release(); c->em_sort_tmp.release();
+    c->lb_rec.release(); c->lb_keys.release(); c->lb_idx.release(); c->lb_tmp.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
         if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
         if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
@@ -2979,6 +3148,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     cudaFree(s.cache);
     if (s.top) cudaFree(s.top);
     if (s.rank) cudaFree(s.rank);
+    if (s.lbuf) cudaFree(s.lbuf);
     free_emissive(s);
     s = SceneSlot();
     c->scenes_dirty = true;
@@ -3109,14 +3279,44 @@ int ve_cache_reset(ve_ctx* c, int32_t id) {
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "cache_reset: unknown scene");
     VE_CUDA(cudaMemsetAsync(c->scenes[id].cache, 0, sizeof(CacheEntry) << c->cfg.hash_log2, c->stream));
-    // the emissive lights and reservoirs go with it
+    // the emissive lights and reservoirs go with it, and the lBuffer
     if (int rc = reset_emissive(c, c->scenes[id])) return rc;
+    if (c->scenes[id].lbuf) {
+        VE_CUDA(cudaMemsetAsync(c->scenes[id].lbuf, 0, kLbBytes, c->stream));
+        VE_CUDA(cudaStreamSynchronize(c->stream));
+    }
     // the scheduling thresholds derive from the cache: forget them too
     if (c->scenes[id].rank) {
         const int rc = reset_rank(c, c->scenes[id].rank);
         if (rc) return rc;
     }
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    return VE_OK;
+}
+
+int ve_lbuffer_dump(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t* n) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "lbuffer_dump: unknown scene");
+    const SceneSlot& s = c->scenes[id];
+    if (n) *n = 0;
+    if (!s.lbuf) return VE_OK;
+    std::vector<uint32_t> h(kLbBytes / sizeof(uint32_t));
+    VE_CUDA(cudaMemcpyAsync(h.data(), s.lbuf, kLbBytes, cudaMemcpyDeviceToHost, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    uint64_t k = 0;
+    for (uint32_t r = 0; r < kLbWidth; r++)
+        for (uint32_t i = 0; i < kLbSlots; i++) {
+            const uint32_t* w = h.data() + (size_t(r) * kLbSlots + i) * kLbStride;
+            if (w[0] == 0u) continue;
+            if (out && k < cap) {
+                uint32_t* o = out + 14 * k;
+                o[0] = r;
+                o[1] = i;
+                std::memcpy(o + 2, w, kLbStride * sizeof(uint32_t));
+            }
+            k++;
+        }
+    if (n) *n = k;
     return VE_OK;
 }
 

@@ -207,7 +207,7 @@ static void serve_loop(ve_server* s) {
             d.W = f.width; d.H = f.height; d.spp = f.spp;
             d.bounces = f.bounces; d.cc_primary = f.primary_controlchecks; d.cc_bounce = f.bounce_controlchecks;
             d.recon_radius = f.reconstruction_radius; d.render_type = f.render_type; d.frame_index = f.frame_index;
-            d.flags = f.flags & ~(VE_FRAME_PATH_RGB | VE_FRAME_SCHEDULED | VE_FRAME_EMISSIVE);
+            d.flags = f.flags & ~(VE_FRAME_PATH_RGB | VE_FRAME_SCHEDULED | VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER);
             d.tiles_x = (f.width + 15) / 16;
             for (int k = 0; k < 3; k++) { d.sun[k] = f.sun_dir[k]; d.sky[k] = f.sky[k]; }
             d.sun_intensity = f.sun_intensity;
@@ -228,10 +228,10 @@ static void serve_loop(ve_server* s) {
             // live[0] / CNT_LIVE + 0 of the arguments it is given)
             ap.counters = c->counters.p + ps;
             ap.live[0] = (ps & 1u) ? c->live1.p : c->live0.p;
-            k_primary<false, false><<<r->tiles, 256, 0, st>>>(ap);
+            k_primary<false, false, 0><<<r->tiles, 256, 0, st>>>(ap);
         }
         // 2. one shade + one trace pass over every live path
-        k_shade<<<c->grid_shade, 256, 0, st>>>(a, ps);
+        k_shade<0><<<c->grid_shade, 256, 0, st>>>(a, ps);
         k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, ps);
         if (ps == kRing - 1)  // wrap: the survivors' count moves to slot 0
             cudaMemcpyAsync(c->counters.p + CNT_LIVE, c->counters.p + CNT_LIVE + kRing, 4, cudaMemcpyDeviceToDevice,
