@@ -641,6 +641,39 @@ def run_scheduled(args, rank, world):
     return 0
 
 
+def run_lbuffer(args, rank, world):
+    """The reference's dual-channel lBuffer AccumPass (VE_FRAME_LBUFFER,
+    deterministic per-row application) against the FP32 per-voxel cache on
+    the depth-10 1080p workload: device time per frame and rMSE against the
+    64-spp plain render at equal device time."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=600.0, device=local)
+    torch.cuda.set_device(local)
+    H = _EqualTime(ve, wl, local)
+    plain = H.run(0, None, args.eq_frames)
+    lb = H.run(ve.FRAME_LBUFFER, plain["ms"], 64)
+    for res in (plain, lb):
+        res["ms_per_frame"] = res["ms"] / max(res["frames"], 1)
+    line = {"metric": "ms per frame, lBuffer AccumPass (depth-10 1080p, 4 spp x 3 bounces)",
+            "value": lb["ms_per_frame"], "unit": "ms", "n_gpus": world, "steps": lb["frames"], "warmup": 1,
+            "ms_per_step": lb["ms_per_frame"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 shading / u32 lBuffer", "data": "synthetic (seeded terrain, fixed orbit camera)",
+            "config": {"workload": "lbuffer: depth-10 terrain 1920x1080, 4 spp x 3 bounces, caps 16/64, "
+                                   "equal device time with the FP32-cache frames", "budget_ms": plain["ms"]},
+            "fp32_cache": plain, "lbuffer": lb}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    H.r.close()
+    vd.shutdown(dist)
+    return 0
+
+
 def run_emissive(args, rank, world):
     """The reference's Cornell box (depth 8, light panel of 65,536 emissive
     voxels, camera of its demo) at 1920x1080, 1 spp x 3 bounces, with
@@ -787,7 +820,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "emissive", "build"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "emissive", "lbuffer", "build"], default="large")
     ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
     ap.add_argument("--eq-frames", type=int, default=4, help="learned, scheduled: plain frames setting the time budget")
     ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
@@ -817,6 +850,8 @@ def main():
         return run_scheduled(args, rank, world)
     if args.workload == "emissive":
         return run_emissive(args, rank, world)
+    if args.workload == "lbuffer":
+        return run_lbuffer(args, rank, world)
     if args.workload == "build":
         return run_build(args, rank, world)
 

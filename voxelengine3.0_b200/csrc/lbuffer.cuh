@@ -12,9 +12,9 @@
 //
 // Determinism: the reference's deposits race on the slots' atomics, so the
 // result depends on the arrival order.  Here a frame's deposits are
-// collected, sorted by (row, path slot) and applied by one thread per row in
-// that order — the same operations the reference performs, in one fixed
-// order that the oracle repeats.
+// collected, ordered by (row, path slot) and applied row by row in that
+// order — the same operations the reference performs, in one fixed order
+// that the oracle repeats.
 #pragma once
 #include <cstdint>
 
@@ -72,7 +72,27 @@ __device__ __forceinline__ void lb_firefly(const uint32_t* s, uint32_t c[4], con
     }
 }
 
-// depositSampleDual (shade.comp:162-257) by the thread that owns the row.
+// A deposit into the slot that holds `vid` (shade.comp:184-254): the stale
+// reset, the per-channel halving at the caps, the firefly clamp, the sums.
+__device__ __forceinline__ void lb_update(uint32_t* s, uint32_t vid, uint32_t d[4], uint32_t e[4],
+                                          const LbParams& P) {
+    const uint32_t t = s[11];
+    if (!P.disable_stale && t != 0u && t + P.update_time < P.time) {
+        lb_reset(s, vid, d, e, P.time);
+        return;
+    }
+    if (s[1] >= P.cap_dir)
+        for (int k = 1; k <= 5; k++) s[k] >>= 1;
+    if (s[6] >= P.cap_ind)
+        for (int k = 6; k <= 10; k++) s[k] >>= 1;
+    lb_firefly(s + 1, d, P);
+    lb_firefly(s + 6, e, P);
+    s[1] += 1u; s[2] += d[0]; s[3] += d[1]; s[4] += d[2]; s[5] += d[3];
+    s[6] += 1u; s[7] += e[0]; s[8] += e[1]; s[9] += e[2]; s[10] += e[3];
+    s[11] = P.time;
+}
+
+// depositSampleDual (shade.comp:162-257) on a whole row, sequentially.
 __device__ __forceinline__ void lb_deposit(uint32_t* row, uint32_t vid, const float dir[3], const float ind[3],
                                            const LbParams& P) {
     uint32_t d[4], e[4];
@@ -82,27 +102,14 @@ __device__ __forceinline__ void lb_deposit(uint32_t* row, uint32_t vid, const fl
     for (uint32_t i = 0; i < kLbSlots; i++) {
         uint32_t* s = row + i * kLbStride;
         if (s[0] == 0u) s[0] = vid;  // claim an empty slot
-        const uint32_t id = s[0], t = s[11];
-        if (id != vid) {
-            if (t < cand_t) {
-                cand_t = t;
+        if (s[0] != vid) {
+            if (s[11] < cand_t) {
+                cand_t = s[11];
                 cand_i = i;
             }
             continue;
         }
-        if (!P.disable_stale && t != 0u && t + P.update_time < P.time) {
-            lb_reset(s, vid, d, e, P.time);
-            return;
-        }
-        if (s[1] >= P.cap_dir)
-            for (int k = 1; k <= 5; k++) s[k] >>= 1;
-        if (s[6] >= P.cap_ind)
-            for (int k = 6; k <= 10; k++) s[k] >>= 1;
-        lb_firefly(s + 1, d, P);
-        lb_firefly(s + 6, e, P);
-        s[1] += 1u; s[2] += d[0]; s[3] += d[1]; s[4] += d[2]; s[5] += d[3];
-        s[6] += 1u; s[7] += e[0]; s[8] += e[1]; s[9] += e[2]; s[10] += e[3];
-        s[11] = P.time;
+        lb_update(s, vid, d, e, P);
         return;
     }
     if (cand_t != 0xFFFFFFFFu) lb_reset(row + cand_i * kLbStride, vid, d, e, P.time);

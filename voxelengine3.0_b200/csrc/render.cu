@@ -101,7 +101,6 @@ constexpr uint32_t kDefaultRefill = 24;  // trace refill threshold (idle lanes o
 enum : uint32_t {
     CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_RES = 63,
     CNT_RAYSH = 64,  // shadow rays per pass (extension rays: CNT_RAY)
-    CNT_LB = 84,     // lBuffer deposit records of the frame
     CNT_TOTAL = 96
 };
 enum : uint32_t {
@@ -153,7 +152,8 @@ struct FrameArgs {
     float4* p_sdir;      // emissive batches: NEE shadow direction, w = the light's vid (~0 for the sun)
     PathRes* p_res;      // emissive batches: a path's bounce-0 reservoir until the commit
     uint32_t* res_list;  // paths holding a reservoir (counter CNT_RES)
-    LbRec* lb_rec;       // lBuffer frames: the frame's deposits (counter CNT_LB)
+    LbRec* lb_rec;       // lBuffer frames: each path's deposit, at its path slot
+    uint32_t* lb_key;    // ... and its lBuffer row (0: the path made no deposit)
     uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
     uint32_t* live[2];
@@ -977,15 +977,15 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
         if (o.app_res) a.res_list[kr] = p;
         warp_add_stat(&a.stats[ST_EM_NEE], o.em_nee ? 1u : 0u);
     }
-    if (LB) {  // recorded; applied per lBuffer row at the end of the frame
-        const uint32_t k = warp_append(o.do_dep, &a.counters[CNT_LB]);
+    if (LB) {  // recorded at the path's slot; applied per lBuffer row at the end of the frame
         if (o.do_dep) {
             LbRec r;
             r.vid = o.dvid;
             r.slot = p;
             r.d[0] = o.dr; r.d[1] = o.dg; r.d[2] = o.db;
             r.e[0] = o.ir; r.e[1] = o.ig; r.e[2] = o.ib;
-            a.lb_rec[k] = r;
+            a.lb_rec[p] = r;
+            a.lb_key[p] = lb_row(o.dvid);
             cnt.dep++;
         }
     } else {
@@ -1384,24 +1384,19 @@ __global__ void __launch_bounds__(256) k_res_commit(FrameArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// End-of-frame AccumPass of lBuffer frames: the deposits sorted by (row,
-// path slot), then one thread per row applies its run in that order.
+// End-of-frame AccumPass of lBuffer frames.  Deposits sit at their path
+// slots, so a stable radix sort of their rows (15 bits) orders them by
+// (row, path slot); each row's run is then applied by one warp, lane i
+// holding slot i of the row in registers: the reference's sequential slot
+// scan becomes one ballot per deposit.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_lb_keys(const LbRec* rec, const uint32_t* counters, uint32_t cap,
-                                                 unsigned long long* keys, uint32_t* vals) {
-    const uint32_t n = min(counters[CNT_LB], cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
-        keys[i] = i < n ? (((unsigned long long)lb_row(rec[i].vid)) << 32) | rec[i].slot : ~0ull;
-        vals[i] = i;
-    }
-}
-__global__ void __launch_bounds__(256) k_lb_bounds(const unsigned long long* keys, const uint32_t* counters,
-                                                   uint32_t cap, uint32_t* start, uint32_t* end) {
-    const uint32_t n = min(counters[CNT_LB], cap);
+__global__ void __launch_bounds__(256) k_lb_bounds(const uint32_t* keys, uint32_t n, uint32_t* start,
+                                                   uint32_t* end) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t row = uint32_t(keys[i] >> 32);
-        if (i == 0u || uint32_t(keys[i - 1] >> 32) != row) start[row] = i;
-        if (i + 1u == n || uint32_t(keys[i + 1] >> 32) != row) end[row] = i + 1u;
+        const uint32_t row = keys[i];
+        if (row == 0u) continue;  // paths without a deposit
+        if (i == 0u || keys[i - 1] != row) start[row] = i;
+        if (i + 1u == n || keys[i + 1] != row) end[row] = i + 1u;
     }
 }
 __global__ void __launch_bounds__(256) k_lb_apply(const DevScene* scenes, const DevView* views, const LbRec* rec,
@@ -1410,13 +1405,61 @@ __global__ void __launch_bounds__(256) k_lb_apply(const DevScene* scenes, const 
     const DevView& v = views[0];
     uint32_t* lb = scenes[v.scene].lbuf;
     const LbParams P = v.lb;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < kLbWidth; r += gridDim.x * blockDim.x) {
-        uint32_t* row = lb + size_t(r) * kLbRowWords;
-        for (uint32_t i = start[r]; i < end[r]; i++) {
-            const LbRec x = rec[order[i]];
-            lb_deposit(row, x.vid, x.d, x.e, P);
+    const uint32_t lane = lane_id();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < kLbWidth; r += warps) {
+        const uint32_t b = start[r], e = end[r];
+        if (b == e) continue;
+        uint32_t* gs = lb + size_t(r) * kLbRowWords + lane * kLbStride;
+        uint32_t s[kLbStride];
+#pragma unroll
+        for (int k = 0; k < int(kLbStride); k++) s[k] = gs[k];
+        for (uint32_t i0 = b; i0 < e; i0 += 32u) {
+            // the next 32 deposits fetched by the 32 lanes at once, then
+            // applied one by one from shuffles
+            LbRec mine{};
+            if (i0 + lane < e) mine = rec[order[i0 + lane]];
+            const uint32_t cnt = min(32u, e - i0);
+            for (uint32_t k = 0; k < cnt; k++) {
+                LbRec x;
+                x.vid = __shfl_sync(0xffffffffu, mine.vid, int(k));
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    x.d[q] = __shfl_sync(0xffffffffu, mine.d[q], int(k));
+                    x.e[q] = __shfl_sync(0xffffffffu, mine.e[q], int(k));
+                }
+                uint32_t d[4], c[4];
+                lb_pack(x.d, d);
+                lb_pack(x.e, c);
+                // the scan's stop: the vid's slot or the first empty one
+                // (empty slots only follow the used ones: none is ever cleared)
+                const unsigned m = __ballot_sync(0xffffffffu, s[0] == x.vid || s[0] == 0u);
+                if (m) {
+                    if (int(lane) == __ffs(m) - 1) {
+                        if (s[0] == 0u) s[0] = x.vid;
+                        lb_update(s, x.vid, d, c, P);
+                    }
+                } else {  // no slot: the least recently used one (first of equal times)
+                    uint32_t t = s[11], who = lane;
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const uint32_t t2 = __shfl_xor_sync(0xffffffffu, t, o);
+                        const uint32_t w2 = __shfl_xor_sync(0xffffffffu, who, o);
+                        if (t2 < t || (t2 == t && w2 < who)) {
+                            t = t2;
+                            who = w2;
+                        }
+                    }
+                    if (t != 0xFFFFFFFFu && lane == who) lb_reset(s, x.vid, d, c, P.time);
+                }
+            }
         }
+#pragma unroll
+        for (int k = 0; k < int(kLbStride); k++) gs[k] = s[k];
     }
+}
+
+__global__ void __launch_bounds__(256) k_iota(uint32_t* v, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
 // Launches of the shading kernels' instances for a mode (kModeEm | kModeLb).
@@ -1835,10 +1878,11 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> res_list;      // ... and the paths that hold one
     ve::DevBuf<uint32_t> em_sort;       // registry commit: vid keys / staging indices, 2 x 2 x 2^17
     ve::DevBuf<uint8_t> em_sort_tmp;    // ... CUB radix-sort scratch
-    ve::DevBuf<ve::LbRec> lb_rec;        // lBuffer frames: deposits
-    ve::DevBuf<unsigned long long> lb_keys;  // ... their (row, slot) keys, 2 x paths
-    ve::DevBuf<uint32_t> lb_idx;         // ... sort values 2 x paths + row bounds 2 x rows
+    ve::DevBuf<ve::LbRec> lb_rec;        // lBuffer frames: deposits at their path slots
+    ve::DevBuf<uint32_t> lb_keys;        // ... their rows (0: none), 2 x paths (sort in, out)
+    ve::DevBuf<uint32_t> lb_idx;         // ... path slots 0..n-1 (sort values in), order (out), row bounds
     ve::DevBuf<uint8_t> lb_tmp;          // ... CUB radix-sort scratch
+    uint64_t lb_iota = 0;                // lb_idx holds 0..lb_iota-1
     ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
@@ -2335,16 +2379,20 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     size_t lb_sort_bytes = 0;
     if (flags & VE_FRAME_LBUFFER) {
         if ((rc = ensure_lbuffer(c, c->scenes[views[0].scene_id]))) return rc;
-        cub::DeviceRadixSort::SortPairs(nullptr, lb_sort_bytes, (const unsigned long long*)nullptr,
-                                        (unsigned long long*)nullptr, (const uint32_t*)nullptr, (uint32_t*)nullptr,
-                                        int(paths), 0, 47, c->stream);
+        cub::DeviceRadixSort::SortPairs(nullptr, lb_sort_bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (const uint32_t*)nullptr, (uint32_t*)nullptr, int(paths), 0, 15, c->stream);
         const void* before[] = {c->lb_rec.p, c->lb_keys.p, c->lb_idx.p, c->lb_tmp.p};
+        const size_t idx_cap = c->lb_idx.cap;
         if ((rc = c->lb_rec.ensure(paths)) || (rc = c->lb_keys.ensure(2 * paths)) ||
             (rc = c->lb_idx.ensure(2 * paths + 2ull * kLbWidth)) || (rc = c->lb_tmp.ensure(lb_sort_bytes)))
             return rc;
         const void* after[] = {c->lb_rec.p, c->lb_keys.p, c->lb_idx.p, c->lb_tmp.p};
         for (int i = 0; i < 4; i++)
             if (before[i] != after[i]) c->gen++;
+        if (before[2] != after[2] || idx_cap != c->lb_idx.cap || c->lb_iota < paths) {  // sort values: 0, 1, 2, ...
+            k_iota<<<c->num_sms * 8, 256, 0, c->stream>>>(c->lb_idx.p, uint32_t(paths));
+            c->lb_iota = paths;
+        }
     }
     if ((rc = sync_scenes(c))) return rc;
     // view table, written into a staging slot whose previous copy has run
@@ -2469,7 +2517,10 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         a.shade_cap = uint32_t(paths);
         a.rank = c->scenes[views[0].scene_id].rank;
     }
-    if (flags & VE_FRAME_LBUFFER) a.lb_rec = c->lb_rec.p;
+    if (flags & VE_FRAME_LBUFFER) {
+        a.lb_rec = c->lb_rec.p;
+        a.lb_key = c->lb_keys.p;
+    }
     if (flags & VE_FRAME_EMISSIVE) {
         a.p_sdir = c->p_sdir.p;
         a.p_res = c->p_res.p;
@@ -2485,6 +2536,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         // paths of pixels without a primary hit are never spawned: their
         // debug slots read as zero
         if (flags & VE_FRAME_PATH_RGB) cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st);
+        // lBuffer frames: row 0 (no deposit) for paths that are never spawned
+        if (lbm) cudaMemsetAsync(c->lb_keys.p, 0, paths * sizeof(uint32_t), st);
         rec();
         for (auto& d : decays) {
             if (d.second != 1.0f) {
@@ -2549,19 +2602,18 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         if (lbm) {  // AccumPass: the frame's deposits into the lBuffer, row by row
             const uint32_t capn = uint32_t(paths);
-            unsigned long long* kin = c->lb_keys.p;
-            unsigned long long* kout = kin + capn;
+            uint32_t* kin = c->lb_keys.p;
+            uint32_t* kout = kin + capn;
             uint32_t* vin = c->lb_idx.p;
             uint32_t* vout = vin + capn;
             uint32_t* rs = vout + capn;
             uint32_t* re = rs + kLbWidth;
             cudaMemsetAsync(rs, 0, 2ull * kLbWidth * sizeof(uint32_t), st);
-            k_lb_keys<<<c->num_sms * 8, 256, 0, st>>>(c->lb_rec.p, c->counters.p, capn, kin, vin);
             size_t b = lb_sort_bytes;
-            cub::DeviceRadixSort::SortPairs(c->lb_tmp.p, b, kin, kout, vin, vout, int(capn), 0, 47, st);
-            k_lb_bounds<<<c->num_sms * 8, 256, 0, st>>>(kout, c->counters.p, capn, rs, re);
-            k_lb_apply<<<kLbWidth / 256, 256, 0, st>>>(a.scenes, a.views, c->lb_rec.p, vout, rs, re);
-            launches += 4;
+            cub::DeviceRadixSort::SortPairs(c->lb_tmp.p, b, kin, kout, vin, vout, int(capn), 0, 15, st);
+            k_lb_bounds<<<c->num_sms * 8, 256, 0, st>>>(kout, capn, rs, re);
+            k_lb_apply<<<kLbWidth / 8, 256, 0, st>>>(a.scenes, a.views, c->lb_rec.p, vout, rs, re);
+            launches += 3;
         }
         k_resolve<<<tiles, 256, 0, st>>>(a);
         launches++;
