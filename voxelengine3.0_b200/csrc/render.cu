@@ -500,8 +500,9 @@ __device__ __forceinline__ Avg lookup_avg(const DevScene& S, uint32_t vid) {
 
 // The view's radiance cache: the dual-channel lBuffer (VE_FRAME_LBUFFER) or
 // the FP32 per-voxel cache.
+template <bool LB>
 __device__ __forceinline__ Avg lookup_view(const DevView& v, const DevScene& S, uint32_t vid) {
-    if ((v.flags & VE_FRAME_LBUFFER) && S.lbuf) {
+    if (LB && (v.flags & VE_FRAME_LBUFFER) && S.lbuf) {
         Avg r;
         lb_lookup(S.lbuf, vid, r.rgb, r.count, r.var);
         return r;
@@ -1547,6 +1548,8 @@ __device__ __forceinline__ float aces(float x) {  // final.frag:11-18
 
 // AvgPass (resolve.comp:362-382 with resolveDefault :224-261,
 // reconstructTimeout :193-219 and the visualisation modes) + tonemap.
+// LB: the batch has VE_FRAME_LBUFFER views.
+template <bool LB = false>
 __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
     const uint32_t tile = blockIdx.x;
     const uint32_t vi = find_view(a.views, a.n_views, tile);
@@ -1572,7 +1575,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
                 const uint4 nd = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)];
                 if (nd.w == 0u || nd.x >= v.cc_primary) continue;
-                const Avg na = lookup_view(v, S, nd.w);
+                const Avg na = lookup_view<LB>(v, S, nd.w);
                 if (na.count == 0u) continue;
                 const float dist = float(dx * dx + dy * dy);
                 const float w = float(na.count < 32u ? na.count : 32u) / (1.0f + dist * 0.15f);
@@ -1616,7 +1619,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
         case VE_RENDER_VARIANCE:
             if (vid == 0u) col = miss();
             else {
-                const Avg c = lookup_view(v, S, vid);
+                const Avg c = lookup_view<LB>(v, S, vid);
                 const float var = c.count >= 2u ? c.var : 0.0f;
                 const float sc = gclamp(var * (255.0f * 255.0f) / gmax(v.variance_norm, 1.0f), 0.0f, 1.0f);
                 col = mk(sc, sc, sc);
@@ -1627,7 +1630,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 col = miss();
                 break;
             }
-            const Avg c = lookup_view(v, S, vid);
+            const Avg c = lookup_view<LB>(v, S, vid);
             if (c.count >= 128u && c.var < 0.02f) {
                 col = c.rgb;
                 break;
@@ -1640,7 +1643,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
                 if (qx < 0 || qy < 0 || qx >= int(W) || qy >= int(H)) continue;
                 const uint32_t nv = a.gbuf[v.pix_base + uint32_t(qy) * W + uint32_t(qx)].w;
                 if (nv == 0u || nv == vid) continue;
-                const Avg na = lookup_view(v, S, nv);
+                const Avg na = lookup_view<LB>(v, S, nv);
                 if (na.count == 0u) continue;
                 const f3 dd = sub(na.rgb, c.rgb);
                 const float dc = sqrtf(dot(dd, dd));
@@ -2615,7 +2618,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             k_lb_apply<<<kLbWidth / 8, 256, 0, st>>>(a.scenes, a.views, c->lb_rec.p, vout, rs, re);
             launches += 3;
         }
-        k_resolve<<<tiles, 256, 0, st>>>(a);
+        if (lbm) k_resolve<true><<<tiles, 256, 0, st>>>(a);
+        else k_resolve<<<tiles, 256, 0, st>>>(a);
         launches++;
         if (flags & VE_FRAME_EMISSIVE) {  // this frame's lights and reservoirs, for the next frame
             constexpr int cap = 1 << kEmClaimLog2;
