@@ -12,7 +12,9 @@ radius 600.  A ray is one DDA traversal (primary, bounce or sun shadow).
   events on the renderer's stream around K frames, max over ranks.
 * ``e2e``: the same frames through the public API with host outputs (voxel-id
   image + RGB into pinned host memory) and the per-frame view table uploaded;
-  events around all K steps, copies included.
+  each frame's images are copied on the renderer's copy stream while the next
+  frame renders (VE_FRAME_ASYNC_OUTPUTS, two alternating pinned sets); events
+  around all K steps and the last frame's copies.
 * ``roofline``: the trace kernel (bounce + shadow DDA): algorithmic bytes
   (4 B per distinct node word read + 48 B ray state per traversal) over its
   CUDA-event time inside the timed frames, against the measured HBM copy
@@ -812,6 +814,81 @@ def run_build(args, rank, world):
     return 0
 
 
+def run_split(args, rank, world):
+    """Split frames: each 1080p frame of the large workload rendered by every
+    rank on its band of rows, one all-gather of the frame's cache records
+    (NCCL), the rank-order merge and the band's AvgPass (strong scaling: the
+    frame is fixed as N grows).  At N=1 the band is the whole frame and the
+    line measures the split path's overhead over the plain frame."""
+    import torch
+
+    import ve_b200.dist as vd
+    import ve_b200.workloads as wl
+
+    ve = load_package()
+    rank, world, local = vd.env_rank()
+    dist = vd.init("nccl", timeout_s=300.0, device=local)
+    torch.cuda.set_device(local)
+    W = wl.LARGE
+    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
+    r = ve.Renderer(device=local, hash_log2=W.hash_log2)
+    r.set_materials(ve.terrain_materials(W.seed))
+    sid = r.upload_scene(words, W.depth)
+    stream = torch.cuda.ExternalStream(r.stream, device=local)
+    sf = vd.SplitFrame(r, sid, dist, device=f"cuda:{local}")
+    dev = f"cuda:{local}"
+
+    def cam(i):
+        eye, d = wl.orbit_camera(i % W.frames, W.frames, W.seed)
+        return ve.camera_ubo(eye, d, W.fov, W.width / W.height)
+
+    K, Wm = args.steps, args.warmup
+    for i in range(Wm):
+        sf.render(cam(i), frame_config(ve, W, i), outputs=(), gather=False)
+
+    def timed(outputs, gather):
+        r.reset_total_stats()
+        torch.cuda.synchronize(local)
+        vd.barrier(dist)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        records = 0
+        e0.record(stream)
+        for i in range(K):
+            sf.render(cam(Wm + i), frame_config(ve, W, Wm + i), outputs=outputs, gather=gather)
+            records += sum(sf.last["counts"])
+        e1.record(stream)
+        e1.synchronize()
+        ms = vd.max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        tot = r.total_stats()
+        rays = vd.sum_over_ranks(rays_of(tot), dist, dev)
+        return ms, rays, tot, records
+
+    with ClockSampler(local) as clk:
+        ms, rays, tot, records = timed((), False)
+    value = rays / (ms / 1e3) / 1e6
+    e_ms, e_rays, etot, _ = timed(("rgb",), True)
+    e2e_value = e_rays / (e_ms / 1e3) / 1e6
+    if rank == 0:
+        line = {"metric": METRIC + " (split frames)", "value": value, "unit": "Mrays/s", "n_gpus": world,
+                "steps": K, "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded value-noise terrain, seeded orbit camera)",
+                "config": {"workload": "split: large (depth-10, 1920x1080, 4 spp x 3 bounces) frames split into "
+                                       f"{world} bands of rows", "parallelism": f"row bands x{world}",
+                           "records_per_step": records / K,
+                           "exchange_bytes_per_step": 32.0 * records / K,
+                           "l2": "inputs larger than L2 (310 MB node array)"},
+                "e2e": {"value": e2e_value, "unit": "Mrays/s",
+                        "h2d_bytes_per_step": (etot["h2d_bytes"] + 0.0) / K,
+                        "d2h_bytes_per_step": 12.0 * W.width * W.height},
+                "gpu_launches": int(tot["kernel_launches"]) + (2 + world) * K,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    r.close()
+    vd.shutdown(dist)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -820,7 +897,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "emissive", "lbuffer", "build"], default="large")
+    ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "emissive", "lbuffer", "build",
+                                                  "split"], default="large")
     ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
     ap.add_argument("--eq-frames", type=int, default=4, help="learned, scheduled: plain frames setting the time budget")
     ap.add_argument("--requests", type=int, default=10000, help="serving: requests in the Poisson stream")
@@ -854,6 +932,8 @@ def main():
         return run_lbuffer(args, rank, world)
     if args.workload == "build":
         return run_build(args, rank, world)
+    if args.workload == "split":
+        return run_split(args, rank, world)
 
     import torch
 
@@ -929,24 +1009,32 @@ def main():
     peak, peak_kind = peaks()
 
     # ---- e2e: public API, host outputs, view upload each step --------------
-    hv = torch.empty((W.height, W.width), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-    hrgb = torch.empty((W.height, W.width, 3), dtype=torch.float32, pin_memory=True).numpy()
-    outs = ve.FrameOutputsC()
-    outs.voxel_id = hv.ctypes.data
-    outs.rgb = hrgb.ctypes.data
+    # outputs copied on the renderer's copy stream while the next frame
+    # renders (VE_FRAME_ASYNC_OUTPUTS), into two alternating pinned sets;
+    # every frame's images reach host memory inside the timed region
+    sets = []
+    for _ in range(2):
+        hv = torch.empty((W.height, W.width), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        hrgb = torch.empty((W.height, W.width, 3), dtype=torch.float32, pin_memory=True).numpy()
+        o = ve.FrameOutputsC()
+        o.voxel_id = hv.ctypes.data
+        o.rgb = hrgb.ctypes.data
+        sets.append((o, hv, hrgb))
     lib = ve.load_library()
     import ctypes
 
-    views = [ve.Renderer.make_view(sid, cam_list[i], frame_config(ve, W, frame(Wm + i))) for i in range(K)]
+    views = [ve.Renderer.make_view(sid, cam_list[i], frame_config(ve, W, frame(Wm + i), ve.FRAME_ASYNC_OUTPUTS))
+             for i in range(K)]
     r.reset_total_stats()
     barrier()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for i in range(K):
-        rc = lib.ve_render(r._h, ctypes.byref(views[i]), ctypes.byref(outs))
+        rc = lib.ve_render(r._h, ctypes.byref(views[i]), ctypes.byref(sets[i & 1][0]))
         if rc != 0:
             raise RuntimeError(lib.ve_last_error().decode())
+    r.synchronize()  # the last frame's copies
     f1.record(stream)
     f1.synchronize()
     e2e_ms = max_over_ranks(f0.elapsed_time(f1))

@@ -52,6 +52,15 @@ extern "C" {
                                      in place of the FP32 per-voxel cache; one view per call */
 #define VE_FRAME_SCHEDULED 64u    /* importance-aware voxel scheduling (schedule/rank/threshold.comp)
                                      in place of spp paths per pixel; single-view calls */
+#define VE_FRAME_SPLIT 512u       /* one band of rows of a frame split across ranks: paths start only
+                                     on rows [row_begin, row_end) and deposit into a per-frame table
+                                     that ve_split_export / ve_split_merge exchange; the AvgPass runs
+                                     in ve_split_resolve after the merge */
+#define VE_FRAME_ASYNC_OUTPUTS 1024u /* host outputs (voxel_id, hit_node, rgb, mapped only) are copied on the
+                                     context's copy stream while later frames render: the call returns
+                                     once the frame is enqueued, and the host buffers (pinned memory for
+                                     the copies to run asynchronously) hold the frame after
+                                     ve_ctx_synchronize */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
                                      replaying a CUDA graph of the frame's kernel sequence */
 
@@ -104,6 +113,8 @@ typedef struct ve_frame_config {
     uint32_t sample_cap_indirect;     /* 64 */
     float firefly_k;                  /* 1: a sample above k x the running mean is scaled down */
     float firefly_floor;              /* 255: lower bound of that threshold (quantised units) */
+    /* split frames (VE_FRAME_SPLIT): this rank's band of rows */
+    uint32_t row_begin, row_end;
 } ve_frame_config;
 
 #define VE_RESTIR_ENABLE 1u   /* ReSTIR DI at bounce 0 (else single-pick RIS there too) */
@@ -294,6 +305,41 @@ int ve_render(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
  * batch: one primary pass over all views, one trace and one shade pass per
  * bounce depth for all their paths, one resolve pass. `outs` may be NULL. */
 int ve_render_batch(ve_ctx* ctx, const ve_view* views, uint32_t n_views, ve_frame_outputs* outs);
+/* Split frames (one frame of one view over several GPUs, each rendering a
+ * band of rows; the multi-GPU form of Renderer::run for frames too large
+ * for one device).  A rank renders its band with VE_FRAME_SPLIT (ve_render:
+ * primary rays of the band and of max(reconstruction_radius, 1) rows on
+ * either side, paths of the band's pixels only; the scene's cache is
+ * decayed, the frame's deposits go to a per-frame table; no AvgPass, and
+ * rgb / mapped outputs must be NULL).  Then every rank:
+ *   ve_split_export  the per-frame table as records (device memory),
+ *   (all-gather of the records across ranks: NCCL over NVLink),
+ *   ve_split_merge   every rank's records, in rank order, into the cache,
+ *   ve_split_resolve the AvgPass of the band.
+ * All ranks merge the same records in the same order, so their caches stay
+ * identical; the merged cache holds the counts of the unsplit frame and its
+ * sums up to float rounding.  A record is 8 x 32-bit words {vid, count,
+ * luma^2, r, g, b, weight, 0} (32 B). */
+typedef struct ve_split_record {
+    uint32_t vid, count;
+    float l2, r, g, b, w;
+    uint32_t reserved;
+} ve_split_record;
+/* Records of the last VE_FRAME_SPLIT frame of `scene_id` into device memory
+ * `dev_out` (room for `cap`); `n` = records in the frame (written: min(n,
+ * cap)).  Synchronous. */
+int ve_split_export(ve_ctx* ctx, int32_t scene_id, void* dev_out, uint64_t cap, uint64_t* n);
+/* Adds `n_parts` record arrays (device memory; part k starts at record
+ * k * stride and holds counts[k] records) into the scene's cache, part 0
+ * first.  `dropped` (may be NULL): records whose voxel found no cache entry.
+ * Synchronous. */
+int ve_split_merge(ve_ctx* ctx, int32_t scene_id, const void* dev_parts, const uint64_t* counts, uint32_t n_parts,
+                   uint64_t stride, uint64_t* dropped);
+/* The AvgPass (resolve.comp) of the band of `view` (the view of the last
+ * VE_FRAME_SPLIT render) from the merged cache; the outputs' rows
+ * [row_begin, row_end) are written (host pointers to full-size images). */
+int ve_split_resolve(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
+
 /* Launch shape of the persistent bounce kernels: resident blocks per SM of
  * the trace and shade kernels (0 = occupancy maximum) and the number of idle
  * lanes at which a trace warp refills itself with new rays (0 = default, 24). */

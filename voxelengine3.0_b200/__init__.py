@@ -49,6 +49,9 @@ FRAME_TRAIN = 32
 FRAME_SCHEDULED = 64
 FRAME_EMISSIVE = 128
 FRAME_LBUFFER = 256
+FRAME_SPLIT = 512
+FRAME_ASYNC_OUTPUTS = 1024
+SPLIT_RECORD_BYTES = 32  # ve_split_record
 RESTIR_ENABLE = 1
 RESTIR_TEMPORAL = 2
 RESTIR_SPATIAL = 4
@@ -86,7 +89,7 @@ class FrameConfigC(ctypes.Structure):
                 ("time", ctypes.c_uint32), ("update_time", ctypes.c_uint32),
                 ("disable_stale_reset", ctypes.c_uint32), ("sample_cap_direct", ctypes.c_uint32),
                 ("sample_cap_indirect", ctypes.c_uint32), ("firefly_k", ctypes.c_float),
-                ("firefly_floor", ctypes.c_float)]
+                ("firefly_floor", ctypes.c_float), ("row_begin", ctypes.c_uint32), ("row_end", ctypes.c_uint32)]
 
 
 class ViewC(ctypes.Structure):
@@ -213,6 +216,9 @@ _SIGNATURES = {
     "ve_server_wait": ([_P, _U64, _U32, _PTR(RequestInfoC)], ctypes.c_int),
     "ve_server_get_stats": ([_P, _PTR(ServerStatsC)], ctypes.c_int),
     "ve_server_destroy": ([_P], ctypes.c_int),
+    "ve_split_export": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_split_merge": ([_P, _I32, _P, _P, _U32, _U64, _PTR(_U64)], ctypes.c_int),
+    "ve_split_resolve": ([_P, _PTR(ViewC), _PTR(FrameOutputsC)], ctypes.c_int),
     "ve_set_launch_config": ([_P, _PTR(LaunchConfigC)], ctypes.c_int),
     "ve_autotune": ([_P, _PTR(ViewC), _U32, _U32, _PTR(LaunchConfigC)], ctypes.c_int),
     "ve_reset_total_stats": ([_P], ctypes.c_int),
@@ -463,13 +469,16 @@ class FrameConfig:
     sample_cap_indirect: int = 64
     firefly_k: float = 1.0
     firefly_floor: float = 255.0
+    # split frames (FRAME_SPLIT): this rank's band of rows
+    row_begin: int = 0
+    row_end: int = 0
 
     def to_c(self) -> FrameConfigC:
         c = FrameConfigC()
         for f in ("width", "height", "spp", "bounces", "primary_controlchecks", "bounce_controlchecks",
                   "reconstruction_radius", "render_type", "frame_index", "flags", "min_samples", "shading_budget",
                   "restir", "restir_m", "restir_spatial_neighbors", "restir_max_m", "time", "update_time",
-                  "disable_stale_reset", "sample_cap_direct", "sample_cap_indirect"):
+                  "disable_stale_reset", "sample_cap_direct", "sample_cap_indirect", "row_begin", "row_end"):
             setattr(c, f, int(getattr(self, f)))
         for i in range(3):
             c.sun_dir[i] = float(self.sun_dir[i])
@@ -484,6 +493,15 @@ class FrameConfig:
 
 
 OUTPUT_KINDS = ("gbuffer", "voxel_id", "hit_node", "rgb", "mapped", "path_rgb")
+
+
+def _dev_ptr(buf) -> Optional[int]:
+    """Device address of a tensor-like object (data_ptr()) or an integer."""
+    if buf is None:
+        return None
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr())
+    return int(buf)
 
 
 def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
@@ -648,6 +666,23 @@ class Renderer:
         _check(self._lib.ve_render(self._h, ctypes.byref(view), ctypes.byref(o) if want else None))
         return arrays
 
+    def render_into(self, scene_id: int, camera: np.ndarray, fc: FrameConfig, arrays: Dict[str, np.ndarray]) -> None:
+        """One frame into caller-owned host arrays (name -> C-contiguous array
+        of the output's size).  With FRAME_ASYNC_OUTPUTS the call returns once
+        the frame is enqueued; the arrays (pinned memory for an asynchronous
+        copy) hold the frame after synchronize()."""
+        npx = fc.width * fc.height
+        size = {"gbuffer": 4 * npx, "voxel_id": npx, "hit_node": npx, "rgb": 3 * npx, "mapped": 3 * npx}
+        o = FrameOutputsC()
+        for k, a in arrays.items():
+            if k not in size:
+                raise ValueError(f"unknown output {k!r}")
+            if not a.flags.c_contiguous or a.size != size[k] or a.itemsize != 4:
+                raise ValueError(f"output {k!r}: {size[k]} contiguous 32-bit elements expected")
+            setattr(o, k, a.ctypes.data)
+        view = self.make_view(scene_id, camera, fc)
+        _check(self._lib.ve_render(self._h, ctypes.byref(view), ctypes.byref(o)))
+
     def render_batch(self, views: Sequence[tuple], outputs: Iterable[str] = ("voxel_id", "rgb")):
         """views: sequence of (scene_id, camera, FrameConfig)."""
         arr = (ViewC * len(views))()
@@ -661,6 +696,34 @@ class Renderer:
             results.append(arrays)
         _check(self._lib.ve_render_batch(self._h, arr, len(views), outs if want else None))
         return results
+
+    # split frames (one frame over several ranks; see dist.SplitFrame)
+    def split_export(self, scene_id: int, out, cap: int) -> int:
+        """Records of the last FRAME_SPLIT frame into device memory `out` (a
+        tensor or an address, room for `cap` records of 32 B); returns the
+        frame's record count."""
+        n = _U64()
+        _check(self._lib.ve_split_export(self._h, scene_id, _dev_ptr(out), cap, ctypes.byref(n)))
+        return n.value
+
+    def split_merge(self, scene_id: int, parts, counts: Sequence[int], stride: int) -> int:
+        """Adds the ranks' records (device memory; part k at record k * stride)
+        into the scene's cache in rank order; returns the records dropped."""
+        c = np.ascontiguousarray(np.asarray(counts, np.uint64))
+        d = _U64()
+        _check(self._lib.ve_split_merge(self._h, scene_id, _dev_ptr(parts), _ptr(c) if c.size else None, c.size,
+                                        stride, ctypes.byref(d)))
+        return d.value
+
+    def split_resolve(self, scene_id: int, camera: np.ndarray, fc: FrameConfig,
+                      outputs: Iterable[str] = ("rgb",)) -> Dict[str, np.ndarray]:
+        """AvgPass of the band of the last FRAME_SPLIT frame; full-size host
+        images with the band's rows written."""
+        view = self.make_view(scene_id, camera, fc)
+        want = list(outputs)
+        o, arrays = _alloc_outputs(fc, want)
+        _check(self._lib.ve_split_resolve(self._h, ctypes.byref(view), ctypes.byref(o) if want else None))
+        return arrays
 
     def launch_config(self) -> Dict[str, int]:
         c = LaunchConfigC()

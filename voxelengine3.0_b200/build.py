@@ -27,6 +27,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 CU_SOURCES = ["render.cu"]
 CXX_SOURCES = ["host/octree_cpu.cpp", "host/terrain.cpp", "host/host_api.cpp"]
 HEADERS = ["ve_device.cuh", "raycast.cuh", "serve.cuh", "tc.cuh", "nrc.cuh", "nrc_host.cuh", "builder.cuh",
+           "emissive.cuh", "lbuffer.cuh",
            "host/scene_host.h"]
 
 

@@ -16,6 +16,7 @@
 //   resolve    AvgPass + visualisation modes + ACES tonemap per pixel
 // All queue sizes live in device counters: kernels size their loops from
 // them, so a frame needs no host synchronisation.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -94,6 +95,9 @@ struct DevView {
     // dual-channel lBuffer (core.hpp:93-104, 150-157 knobs)
     LbParams lb;
     uint32_t pad5;
+    // rows whose paths start (split frames: the rank's band) and rows whose
+    // primary rays run (the band and the AvgPass's halo); [0, H) otherwise
+    uint32_t row_lo, row_hi, g_lo, g_hi;
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
@@ -1014,7 +1018,8 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     const DevView& v = a.views[vi];
     uint32_t px, py;
     tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
-    const bool inside = px < v.W && py < v.H;
+    const bool inside = px < v.W && py >= v.g_lo && py < v.g_hi;
+    const bool band = py >= v.row_lo && py < v.row_hi;
     const DevScene S = a.scenes[v.scene];
     Hit h;
     h.status = kEscaped;
@@ -1041,7 +1046,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
         if (v.flags & VE_FRAME_SCHEDULED)  // paths come from the shade list: keep the hit
             a.hitinfo[v.pix_base + pix] = make_uint4(word, h.x | (h.y << 16), h.z | (h.material << 16), 0u);
     }
-    const bool spawn = inside && vid != 0u && !(v.flags & VE_FRAME_SCHEDULED);
+    const bool spawn = inside && band && vid != 0u && !(v.flags & VE_FRAME_SCHEDULED);
     if (FUSED && !(v.flags & VE_FRAME_SCHEDULED)) {
         // the warp's (pixel, sample) pairs in chunks of 32, pixel-major: the
         // lanes of one chunk hold consecutive path slots (a row of the warp's
@@ -1083,7 +1088,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     if (!FUSED && spawn) {
         const uint32_t pix = py * v.W + px;
         for (uint32_t s = 0; s < v.spp; s++) {
-            const unsigned long long p = v.path_base + (unsigned long long)pix * v.spp + s;
+            const uint32_t p = uint32_t(v.path_base + (unsigned long long)pix * v.spp + s);
             const uint32_t list_idx = pix * v.spp + s;
             // emit.comp:171-174
             const uint32_t sample_idx = v.frame_index + pix * 2654435761u + list_idx * 1442695040u;
@@ -1097,7 +1102,7 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
             a.live[0][q + s] = uint32_t(p);
         }
     }
-    warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside ? 1u : 0u);
+    warp_add_stat(&a.stats[ST_RAYS_PRIMARY], inside && band ? 1u : 0u);
     warp_add_stat(&a.stats[ST_PATHS], spawn ? v.spp : 0u);
     if (a.remaining) {  // the whole block belongs to one view
         uint32_t sp = spawn ? v.spp : 0u;
@@ -1556,7 +1561,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
     const DevView& v = a.views[vi];
     uint32_t px, py;
     tile_pixel(tile - v.tile_base, v.tiles_x, &px, &py);
-    if (px >= v.W || py >= v.H) return;
+    if (px >= v.W || py < v.row_lo || py >= v.row_hi) return;
     const DevScene S = a.scenes[v.scene];
     const uint32_t W = v.W, H = v.H;
     const uint32_t gp = v.pix_base + py * W + px;
@@ -1876,6 +1881,14 @@ struct ve_ctx {
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
+    // VE_FRAME_ASYNC_OUTPUTS: a second set of device images (frames alternate
+    // between the sets), the stream their host copies run on, and events
+    // that order a set's next resolve after its last copy
+    ve::DevBuf<uint32_t> out_vid2, out_node2;
+    ve::DevBuf<float> out_rgb2, out_mapped2;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t frame_done = nullptr, copy_done[2] = {};
+    int out_parity = 0;
     ve::DevBuf<float4> p_sdir;          // emissive batches: NEE shadow directions + light vid
     ve::DevBuf<ve::PathRes> p_res;      // emissive batches: bounce-0 reservoirs until the commit
     ve::DevBuf<uint32_t> res_list;      // ... and the paths that hold one
@@ -1886,6 +1899,14 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> lb_idx;         // ... path slots 0..n-1 (sort values in), order (out), row bounds
     ve::DevBuf<uint8_t> lb_tmp;          // ... CUB radix-sort scratch
     uint64_t lb_iota = 0;                // lb_idx holds 0..lb_iota-1
+    // split frames: the per-frame deposit table, the scene table whose
+    // cache points at it, export / merge counters, the scene of the last
+    // split frame
+    ve::DevBuf<ve::CacheEntry> split_delta;
+    ve::DevBuf<ve::DevScene> d_scenes_split;
+    ve::DevBuf<uint32_t> split_cnt;
+    int split_scene = -1;
+    ve_frame_config split_frame{};  // the last split frame's config
     ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
@@ -2187,6 +2208,9 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
                 if (after[i] != before[i]) { c->gen++; break; }
         }
     } bump{c, before};
+    // a copy of an earlier frame's images may still read the buffers
+    if (c->copy_stream && (pixels > c->out_vid.cap || 3 * pixels > c->out_rgb.cap))
+        cudaStreamSynchronize(c->copy_stream);
     if ((rc = c->gbuf.ensure(pixels)) || (rc = c->out_vid.ensure(pixels)) || (rc = c->out_node.ensure(pixels)) ||
         (rc = c->out_rgb.ensure(pixels * 3)) || (rc = c->out_mapped.ensure(pixels * 3)))
         return rc;
@@ -2268,6 +2292,64 @@ static void apply_launch(ve_ctx* c) {
     if (c->launch.refill_threshold == 0 || c->launch.refill_threshold > 32) c->launch.refill_threshold = kDefaultRefill;
 }
 
+// Row ranges of a view: a split frame's band and, for its primary rays, the
+// band widened by the rows the AvgPass reads around a pixel (the
+// reconstruction radius, and 1 for the 4-neighbour filter).
+static void set_rows(DevView& d, const ve_frame_config& f, bool split) {
+    if (!split) {
+        d.row_lo = 0; d.row_hi = f.height; d.g_lo = 0; d.g_hi = f.height;
+        return;
+    }
+    const uint32_t halo = std::max<uint32_t>(f.reconstruction_radius, 1u);
+    d.row_lo = f.row_begin;
+    d.row_hi = f.row_end;
+    d.g_lo = f.row_begin > halo ? f.row_begin - halo : 0u;
+    d.g_hi = std::min<uint32_t>(f.row_end + halo, f.height);
+}
+
+// Path slots a view takes in a batch: spp per pixel (per pixel of the band
+// for split frames), or the shade list's bound for scheduled frames.
+static uint64_t view_paths(const ve_frame_config& f) {
+    if (f.flags & VE_FRAME_SCHEDULED) return std::min<uint64_t>(f.shading_budget, 2ull * f.width * f.height);
+    if (f.flags & VE_FRAME_SPLIT) {
+        const uint32_t hi = std::min(f.row_end, f.height), lo = std::min(f.row_begin, hi);
+        return uint64_t(hi - lo) * f.width * f.spp;
+    }
+    return uint64_t(f.width) * f.height * f.spp;
+}
+
+// The device view record of a view (everything but its offsets in the batch).
+static void fill_view(DevView& d, const ve_view& v) {
+    const ve_frame_config& f = v.frame;
+    std::memset(&d, 0, sizeof(d));
+    std::memcpy(d.cam, v.camera, sizeof(d.cam));
+    d.scene = uint32_t(v.scene_id);
+    d.W = f.width; d.H = f.height; d.spp = f.spp;
+    d.bounces = f.bounces; d.cc_primary = f.primary_controlchecks; d.cc_bounce = f.bounce_controlchecks;
+    d.recon_radius = f.reconstruction_radius; d.render_type = f.render_type; d.frame_index = f.frame_index;
+    d.flags = f.flags;
+    d.tiles_x = (f.width + 15) / 16;
+    for (int k = 0; k < 3; k++) { d.sun[k] = f.sun_dir[k]; d.sky[k] = f.sky[k]; }
+    d.sun_intensity = f.sun_intensity;
+    d.decay = f.decay;
+    d.variance_norm = f.variance_norm;
+    d.w_pix = f.weight_pixels;
+    d.w_var = f.weight_variance;
+    d.pix_norm = f.pixels_norm;
+    d.top_frac = f.top_fraction;
+    d.mid_frac = f.mid_fraction;
+    d.min_samples = std::min<uint32_t>(f.min_samples, 2u);
+    d.budget = f.shading_budget;
+    d.restir = f.restir;
+    d.restir_m = f.restir_m;
+    d.restir_nbrs = f.restir_spatial_neighbors;
+    d.restir_max_m = f.restir_max_m;
+    d.restir_radius = f.restir_spatial_radius;
+    d.lb = LbParams{f.time, f.update_time, f.disable_stale_reset, f.sample_cap_direct, f.sample_cap_indirect,
+                    f.firefly_k, f.firefly_floor};
+    set_rows(d, f, (f.flags & VE_FRAME_SPLIT) != 0);
+}
+
 static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_outputs* outs) {
     if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "render: no views");
     if (nv > 65535u) return fail(VE_ERR_INVALID, "render: at most 65535 views per batch");
@@ -2290,8 +2372,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         const uint32_t tx = (f.width + 15) / 16, ty = (f.height + 15) / 16;
         tiles += tx * ty;
         pixels += uint64_t(f.width) * f.height;
-        paths += (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2ull * f.width * f.height)
-                                                : uint64_t(f.width) * f.height * f.spp;
+        paths += view_paths(f);
         max_b = std::max(max_b, f.bounces);
         flags |= f.flags;
     }
@@ -2308,6 +2389,26 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     for (uint32_t i = 0; i < nv; i++)
         if ((views[i].frame.flags & VE_FRAME_EMISSIVE) && views[i].frame.restir_m > 64)
             return fail(VE_ERR_INVALID, "render: restir_m must be <= 64");
+    const bool split = (flags & VE_FRAME_SPLIT) != 0;
+    if (!split) c->split_scene = -1;  // the GBuffer of a split frame is about to be overwritten
+    if (split) {
+        const ve_frame_config& f = views[0].frame;
+        if (nv != 1) return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT renders one view per call");
+        if (flags & (VE_FRAME_SCHEDULED | VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER | VE_FRAME_LEARNED | VE_FRAME_TRAIN |
+                     VE_FRAME_TERMINATE_HASH))
+            return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT renders plain path-traced frames only");
+        if (f.row_begin >= f.row_end || f.row_end > f.height)
+            return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT needs row_begin < row_end <= height");
+        if (outs && (outs[0].rgb || outs[0].mapped || outs[0].voxel_id || outs[0].hit_node))
+            return fail(VE_ERR_INVALID, "render: a VE_FRAME_SPLIT frame's image comes from ve_split_resolve");
+    }
+    const bool async_out = (flags & VE_FRAME_ASYNC_OUTPUTS) != 0;
+    if (async_out) {
+        if (split) return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT frames have no images to copy");
+        for (uint32_t i = 0; outs && i < nv; i++)
+            if (outs[i].gbuffer || outs[i].path_rgb)
+                return fail(VE_ERR_INVALID, "render: VE_FRAME_ASYNC_OUTPUTS copies voxel_id, hit_node, rgb and mapped only");
+    }
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
     // learned radiance cache: one per batch, attached to the views' scenes
     ve_nrc* nrc = nullptr;
@@ -2320,6 +2421,25 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     }
     int rc = ensure_frame(c, pixels, paths, nv);
     if (rc) return rc;
+    int parity = 0;  // the device image set this frame's resolve writes
+    if (async_out) {
+        if (!c->copy_stream) {
+            if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->frame_done, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->copy_done[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->copy_done[1], cudaEventDisableTiming) != cudaSuccess)
+                return fail(VE_ERR_CUDA, "render: copy stream creation failed");
+        }
+        const void* before[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p};
+        if (pixels > c->out_vid2.cap || 3 * pixels > c->out_rgb2.cap) cudaStreamSynchronize(c->copy_stream);
+        if ((rc = c->out_vid2.ensure(pixels)) || (rc = c->out_node2.ensure(pixels)) ||
+            (rc = c->out_rgb2.ensure(3 * pixels)) || (rc = c->out_mapped2.ensure(3 * pixels)))
+            return rc;
+        const void* after[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p};
+        for (int i = 0; i < 4; i++)
+            if (before[i] != after[i]) c->gen++;
+        parity = c->out_parity;
+    }
     const bool sched = (flags & VE_FRAME_SCHEDULED) != 0;
     uint32_t claim_size = 0;
     size_t scan_bytes = 0;
@@ -2398,6 +2518,22 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
     }
     if ((rc = sync_scenes(c))) return rc;
+    if (split) {  // the frame's deposits go to the per-frame table
+        const int sid = views[0].scene_id;
+        const void* before[] = {c->split_delta.p, c->d_scenes_split.p};
+        if ((rc = c->split_delta.ensure(size_t(1) << c->cfg.hash_log2)) ||
+            (rc = c->d_scenes_split.ensure(c->d_scenes.cap)) || (rc = c->split_cnt.ensure(2)))
+            return rc;
+        if (before[0] != c->split_delta.p || before[1] != c->d_scenes_split.p) c->gen++;
+        CacheEntry* delta = c->split_delta.p;
+        VE_CUDA(cudaMemcpyAsync(c->d_scenes_split.p, c->d_scenes.p, c->scenes.size() * sizeof(DevScene),
+                                cudaMemcpyDeviceToDevice, c->stream));
+        VE_CUDA(cudaMemcpyAsync(&c->d_scenes_split.p[sid].cache, &delta, sizeof(delta), cudaMemcpyHostToDevice,
+                                c->stream));
+        VE_CUDA(cudaStreamSynchronize(c->stream));
+        c->split_scene = sid;
+        c->split_frame = views[0].frame;
+    }
     // view table, written into a staging slot whose previous copy has run
     const int slot = c->staging_next;
     c->staging_next = (slot + 1) % ve_ctx::kStaging;
@@ -2406,42 +2542,17 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     uint32_t tile_base = 0;
     uint64_t pix_base = 0, path_base = 0;
     for (uint32_t i = 0; i < nv; i++) {
-        const ve_view& v = views[i];
-        const ve_frame_config& f = v.frame;
+        const ve_frame_config& f = views[i].frame;
         DevView& d = hv[i];
-        std::memset(&d, 0, sizeof(d));
-        std::memcpy(d.cam, v.camera, sizeof(d.cam));
-        d.scene = uint32_t(v.scene_id);
-        d.W = f.width; d.H = f.height; d.spp = f.spp;
-        d.bounces = f.bounces; d.cc_primary = f.primary_controlchecks; d.cc_bounce = f.bounce_controlchecks;
-        d.recon_radius = f.reconstruction_radius; d.render_type = f.render_type; d.frame_index = f.frame_index;
-        d.flags = f.flags;
-        d.tiles_x = (f.width + 15) / 16;
-        for (int k = 0; k < 3; k++) { d.sun[k] = f.sun_dir[k]; d.sky[k] = f.sky[k]; }
-        d.sun_intensity = f.sun_intensity;
-        d.decay = f.decay;
-        d.variance_norm = f.variance_norm;
-        d.w_pix = f.weight_pixels;
-        d.w_var = f.weight_variance;
-        d.pix_norm = f.pixels_norm;
-        d.top_frac = f.top_fraction;
-        d.mid_frac = f.mid_fraction;
-        d.min_samples = std::min<uint32_t>(f.min_samples, 2u);
-        d.budget = f.shading_budget;
-        d.restir = f.restir;
-        d.restir_m = f.restir_m;
-        d.restir_nbrs = f.restir_spatial_neighbors;
-        d.restir_max_m = f.restir_max_m;
-        d.restir_radius = f.restir_spatial_radius;
-        d.lb = LbParams{f.time, f.update_time, f.disable_stale_reset, f.sample_cap_direct, f.sample_cap_indirect,
-                        f.firefly_k, f.firefly_floor};
+        fill_view(d, views[i]);
         d.pix_base = uint32_t(pix_base);
         d.tile_base = tile_base;
-        d.path_base = path_base;
+        // a split frame's paths are numbered from its band's first pixel: the
+        // base wraps so that base + pixel * spp + sample is the slot (mod 2^64)
+        d.path_base = (f.flags & VE_FRAME_SPLIT) ? path_base - uint64_t(f.row_begin) * f.width * f.spp : path_base;
         tile_base += d.tiles_x * ((f.height + 15) / 16);
         pix_base += uint64_t(f.width) * f.height;
-        path_base += (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2ull * f.width * f.height)
-                                                    : uint64_t(f.width) * f.height * f.spp;
+        path_base += view_paths(f);
     }
     cudaStream_t st = c->stream;
     const bool timing = (flags & VE_FRAME_TIMING) != 0;
@@ -2476,15 +2587,18 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.views = c->d_views.p;
     a.n_views = nv;
     a.total_tiles = tiles;
-    a.scenes = c->d_scenes.p;
+    a.scenes = split ? c->d_scenes_split.p : c->d_scenes.p;
     a.mats = c->d_mats.p;
     a.p_ray_o = c->p_ray_o.p; a.p_ray_d = c->p_ray_d.p; a.p_tp = c->p_tp.p;
     a.p_direct = c->p_direct.p; a.p_indirect = c->p_indirect.p; a.p_pend = c->p_pend.p;
     a.p_hit = c->p_hit.p; a.p_meta = c->p_meta.p;
     a.live[0] = c->live0.p; a.live[1] = c->live1.p; a.rayq = c->rayq.p; a.rayq_sh = c->rayq.p + paths;
     a.counters = c->counters.p; a.stats = c->stats.p;
-    a.gbuf = c->gbuf.p; a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
-    a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
+    a.gbuf = c->gbuf.p;
+    a.out_vid = parity ? c->out_vid2.p : c->out_vid.p;
+    a.out_node = parity ? c->out_node2.p : c->out_node.p;
+    a.out_rgb = parity ? c->out_rgb2.p : c->out_rgb.p;
+    a.out_mapped = parity ? c->out_mapped2.p : c->out_mapped.p;
     a.path_rgb = (flags & VE_FRAME_PATH_RGB) ? c->path_rgb.p : nullptr;
     a.refill = c->launch.refill_threshold;
     a.view_offset = 0;
@@ -2541,6 +2655,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (flags & VE_FRAME_PATH_RGB) cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st);
         // lBuffer frames: row 0 (no deposit) for paths that are never spawned
         if (lbm) cudaMemsetAsync(c->lb_keys.p, 0, paths * sizeof(uint32_t), st);
+        if (split) cudaMemsetAsync(c->split_delta.p, 0, (size_t(1) << c->cfg.hash_log2) * sizeof(CacheEntry), st);
         rec();
         for (auto& d : decays) {
             if (d.second != 1.0f) {
@@ -2618,9 +2733,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             k_lb_apply<<<kLbWidth / 8, 256, 0, st>>>(a.scenes, a.views, c->lb_rec.p, vout, rs, re);
             launches += 3;
         }
-        if (lbm) k_resolve<true><<<tiles, 256, 0, st>>>(a);
-        else k_resolve<<<tiles, 256, 0, st>>>(a);
-        launches++;
+        if (split) {
+            // the AvgPass follows the merge (ve_split_resolve)
+        } else if (lbm) {
+            k_resolve<true><<<tiles, 256, 0, st>>>(a);
+            launches++;
+        } else {
+            k_resolve<<<tiles, 256, 0, st>>>(a);
+            launches++;
+        }
         if (flags & VE_FRAME_EMISSIVE) {  // this frame's lights and reservoirs, for the next frame
             constexpr int cap = 1 << kEmClaimLog2;
             uint32_t* kin = c->em_sort.p;
@@ -2641,6 +2762,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         k_accum_stats<<<1, 32, 0, st>>>(c->stats.p, c->totals.p);
         launches++;
     };
+    // this frame's resolve overwrites an image set whose copy may be pending
+    if (c->copy_stream) VE_CUDA(cudaStreamWaitEvent(st, c->copy_done[parity], 0));
     const bool use_graph = !timing && !(c->cfg.flags & VE_CFG_NO_GRAPHS);
     if (!use_graph) {
         enqueue();
@@ -2648,7 +2771,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
                                      flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
                                               VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED |
-                                              VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER),
+                                              VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER | VE_FRAME_SPLIT),
                                      paths, uint64_t(c->grid_trace), uint64_t(c->grid_shade),
                                      uint64_t(c->launch.refill_threshold), uint64_t(uintptr_t(nrc)),
                                      uint64_t(a.nrc_ready)};
@@ -2658,6 +2781,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             key.push_back((uint64_t(uint32_t(d.first)) << 32) | bits);
         }
         for (int sc : em_scenes) key.push_back((1ull << 62) | uint64_t(uint32_t(sc)));
+        key.push_back((1ull << 61) | uint64_t(parity));
         ve_ctx::GraphEntry* ge = nullptr;
         for (auto& g : c->graphs)
             if (g.key == key) ge = &g;
@@ -2709,14 +2833,43 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     }
     VE_CUDA(cudaMemcpyAsync(c->h_stats, c->stats.p, ST_TOTAL * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     // host outputs
-    if (outs) {
+    if (outs && async_out) {  // on the copy stream, after the frame; the call does not wait
+        VE_CUDA(cudaEventRecord(c->frame_done, st));
+        VE_CUDA(cudaStreamWaitEvent(c->copy_stream, c->frame_done, 0));
+        cudaStream_t cs = c->copy_stream;
+        uint64_t pb = 0;
+        for (uint32_t i = 0; i < nv; i++) {
+            const ve_frame_config& f = views[i].frame;
+            const uint64_t np = uint64_t(f.width) * f.height;
+            const ve_frame_outputs& o = outs[i];
+            if (o.voxel_id) { VE_CUDA(cudaMemcpyAsync(o.voxel_id, a.out_vid + pb, np * 4, cudaMemcpyDeviceToHost, cs)); d2h += np * 4; }
+            if (o.hit_node) { VE_CUDA(cudaMemcpyAsync(o.hit_node, a.out_node + pb, np * 4, cudaMemcpyDeviceToHost, cs)); d2h += np * 4; }
+            if (o.rgb) { VE_CUDA(cudaMemcpyAsync(o.rgb, a.out_rgb + 3 * pb, np * 12, cudaMemcpyDeviceToHost, cs)); d2h += np * 12; }
+            if (o.mapped) { VE_CUDA(cudaMemcpyAsync(o.mapped, a.out_mapped + 3 * pb, np * 12, cudaMemcpyDeviceToHost, cs)); d2h += np * 12; }
+            pb += np;
+        }
+        VE_CUDA(cudaEventRecord(c->copy_done[parity], cs));
+        c->out_parity = parity ^ 1;
+    } else if (outs) {
         uint64_t pb = 0, qb = 0;
         for (uint32_t i = 0; i < nv; i++) {
             const ve_frame_config& f = views[i].frame;
             const uint64_t np = uint64_t(f.width) * f.height;
-            const uint64_t nq = (f.flags & VE_FRAME_SCHEDULED) ? std::min<uint64_t>(f.shading_budget, 2 * np)
-                                                               : np * f.spp;
+            const uint64_t nq = view_paths(f);
             ve_frame_outputs& o = outs[i];
+            if (split) {  // the band's rows
+                const uint64_t r0 = uint64_t(f.row_begin) * f.width, nr = uint64_t(f.row_end - f.row_begin) * f.width;
+                if (o.gbuffer) {
+                    VE_CUDA(cudaMemcpyAsync(o.gbuffer + 4 * r0, c->gbuf.p + pb + r0, nr * 16, cudaMemcpyDeviceToHost, st));
+                    d2h += nr * 16;
+                }
+                if (o.path_rgb && (f.flags & VE_FRAME_PATH_RGB)) {
+                    VE_CUDA(cudaMemcpyAsync(o.path_rgb + 3 * r0 * f.spp, c->path_rgb.p + 3 * qb, nr * f.spp * 12,
+                                            cudaMemcpyDeviceToHost, st));
+                    d2h += nr * f.spp * 12;
+                }
+                continue;
+            }
             if (o.gbuffer) { VE_CUDA(cudaMemcpyAsync(o.gbuffer, c->gbuf.p + pb, np * 16, cudaMemcpyDeviceToHost, st)); d2h += np * 16; }
             if (o.voxel_id) { VE_CUDA(cudaMemcpyAsync(o.voxel_id, c->out_vid.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
             if (o.hit_node) { VE_CUDA(cudaMemcpyAsync(o.hit_node, c->out_node.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
@@ -2760,6 +2913,48 @@ __global__ void __launch_bounds__(256) k_raycast_batch(DevScene S, const float* 
         w[3] = h.x; w[4] = h.y; w[5] = h.z;
         w[6] = h.size; w[7] = h.checks;
     }
+}
+
+// Split frames: the per-frame deposit table as records {vid, count, luma^2,
+// r, g, b, weight, 0}, compacted by a warp-aggregated counter.
+__global__ void __launch_bounds__(256) k_split_export(const CacheEntry* __restrict__ t, uint32_t n,
+                                                      uint4* __restrict__ out, uint32_t cap, uint32_t* cnt) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // uniform per warp
+        const uint32_t i = base + threadIdx.x;
+        CacheEntry e{};
+        if (i < n) e = t[i];
+        const bool live = i < n && e.key != 0u;
+        const uint32_t j = warp_append(live, cnt);
+        if (live && j < cap) {
+            out[2ull * j + 0] = make_uint4(e.key, e.count, __float_as_uint(e.l2), __float_as_uint(e.rgbw.x));
+            out[2ull * j + 1] = make_uint4(__float_as_uint(e.rgbw.y), __float_as_uint(e.rgbw.z),
+                                           __float_as_uint(e.rgbw.w), 0u);
+        }
+    }
+}
+
+// Adds one rank's records into the cache.  A part holds each voxel once
+// (it comes from one deposit table), so every entry sees one addition per
+// part and the parts' launch order fixes the order of its sums.
+__global__ void __launch_bounds__(256) k_split_merge(CacheEntry* cache, uint32_t log2n, uint32_t probes,
+                                                     const uint4* __restrict__ rec, uint32_t n, uint32_t* dropped) {
+    uint32_t drops = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 a = rec[2ull * i + 0], b = rec[2ull * i + 1];
+        if (a.x == 0u || a.y == 0u) continue;
+        const int s = cache_claim(cache, log2n, probes, a.x);
+        if (s < 0) {
+            drops++;
+            continue;
+        }
+        CacheEntry* e = cache + s;
+        atomicAdd(&e->count, a.y);
+        atomicAdd(&e->l2, __uint_as_float(a.z));
+        atomicAdd(&e->rgbw, make_float4(__uint_as_float(a.w), __uint_as_float(b.x), __uint_as_float(b.y),
+                                        __uint_as_float(b.z)));
+    }
+    if (drops) atomicAdd(dropped, drops);
 }
 
 }  // namespace ve
@@ -2892,6 +3087,15 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->out_mapped.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
     c->p_sdir.release(); c->p_res.release(); c->res_list.release(); c->em_sort.release(); c->em_sort_tmp.release();
     c->lb_rec.release(); c->lb_keys.release(); c->lb_idx.release(); c->lb_tmp.release();
+    c->split_delta.release(); c->d_scenes_split.release(); c->split_cnt.release();
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->frame_done) cudaEventDestroy(c->frame_done);
+    for (auto& e : c->copy_done)
+        if (e) cudaEventDestroy(e);
+    c->out_vid2.release(); c->out_node2.release(); c->out_rgb2.release(); c->out_mapped2.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
         if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
         if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
@@ -2917,6 +3121,7 @@ int ve_ctx_stream(ve_ctx* c, void** stream) {
 int ve_ctx_synchronize(ve_ctx* c) {
     if (!c) return fail(VE_ERR_INVALID, "ctx_synchronize: null context");
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->copy_stream) VE_CUDA(cudaStreamSynchronize(c->copy_stream));
     return VE_OK;
 }
 
@@ -3413,6 +3618,143 @@ int ve_render_batch(ve_ctx* c, const ve_view* views, uint32_t n, ve_frame_output
     if (!c) return fail(VE_ERR_INVALID, "render_batch: null context");
     cudaSetDevice(c->device);
     return render_batch(c, views, n, outs);
+}
+
+// A device range [p, p + bytes) inside one allocation of this context's
+// device (split-frame record buffers come from the caller).
+static int check_device_range(ve_ctx* c, const void* p, uint64_t bytes, const char* what) {
+    if (bytes == 0) return VE_OK;
+    if (!p) return fail(VE_ERR_INVALID, std::string(what) + ": null device pointer");
+    if (uintptr_t(p) % 16u) return fail(VE_ERR_INVALID, std::string(what) + ": records must be 16-byte aligned");
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || at.devicePointer == nullptr ||
+        (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != c->device) {
+        cudaGetLastError();
+        return fail(VE_ERR_INVALID, std::string(what) + ": not device memory of the context's GPU");
+    }
+    using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static RangeFn range = nullptr;
+    if (!range) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            range = reinterpret_cast<RangeFn>(fn);
+    }
+    if (!range) return fail(VE_ERR_CUDA, std::string(what) + ": cannot query allocation ranges");
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (range(&base, &size, CUdeviceptr(uintptr_t(p))) != CUDA_SUCCESS)
+        return fail(VE_ERR_INVALID, std::string(what) + ": not a device allocation");
+    if (uintptr_t(p) + bytes > uintptr_t(base) + size)
+        return fail(VE_ERR_INVALID, std::string(what) + ": the records run past the end of their allocation");
+    return VE_OK;
+}
+
+static int split_scene_ok(ve_ctx* c, int32_t id, const char* what) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, std::string(what) + ": unknown scene");
+    if (c->split_scene != id || !c->split_delta.p)
+        return fail(VE_ERR_STATE, std::string(what) + ": no VE_FRAME_SPLIT frame of this scene");
+    return VE_OK;
+}
+
+int ve_split_export(ve_ctx* c, int32_t id, void* dev_out, uint64_t cap, uint64_t* n) {
+    if (int rc = split_scene_ok(c, id, "split_export")) return rc;
+    if (!n) return fail(VE_ERR_INVALID, "split_export: null count");
+    cudaSetDevice(c->device);
+    const uint64_t N = uint64_t(1) << c->cfg.hash_log2;
+    cap = std::min(cap, N);
+    if (int rc = check_device_range(c, dev_out, cap * sizeof(ve_split_record), "split_export")) return rc;
+    uint32_t* cnt = c->split_cnt.p;
+    VE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t), c->stream));
+    k_split_export<<<c->num_sms * 8, 256, 0, c->stream>>>(c->split_delta.p, uint32_t(N),
+                                                          static_cast<uint4*>(dev_out), uint32_t(cap), cnt);
+    VE_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    VE_CUDA(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    *n = h;
+    return VE_OK;
+}
+
+int ve_split_merge(ve_ctx* c, int32_t id, const void* dev_parts, const uint64_t* counts, uint32_t n_parts,
+                   uint64_t stride, uint64_t* dropped) {
+    if (int rc = split_scene_ok(c, id, "split_merge")) return rc;
+    if (n_parts && !counts) return fail(VE_ERR_INVALID, "split_merge: null counts");
+    const uint64_t N = uint64_t(1) << c->cfg.hash_log2;
+    uint64_t end = 0;
+    for (uint32_t k = 0; k < n_parts; k++) {
+        if (counts[k] > stride) return fail(VE_ERR_INVALID, "split_merge: a part holds more records than its stride");
+        if (counts[k] > N) return fail(VE_ERR_INVALID, "split_merge: a part holds more records than a cache");
+        if (counts[k]) end = std::max(end, uint64_t(k) * stride + counts[k]);
+    }
+    cudaSetDevice(c->device);
+    if (int rc = check_device_range(c, dev_parts, end * sizeof(ve_split_record), "split_merge")) return rc;
+    uint32_t* drop = c->split_cnt.p + 1;
+    VE_CUDA(cudaMemsetAsync(drop, 0, sizeof(uint32_t), c->stream));
+    const ve_split_record* base = static_cast<const ve_split_record*>(dev_parts);
+    CacheEntry* cache = c->scenes[id].cache;
+    for (uint32_t k = 0; k < n_parts; k++) {
+        if (!counts[k]) continue;
+        const uint32_t blocks = uint32_t(std::min<uint64_t>((counts[k] + 255) / 256, uint64_t(c->num_sms) * 8));
+        k_split_merge<<<blocks, 256, 0, c->stream>>>(cache, c->cfg.hash_log2, c->cfg.hash_probes,
+                                                     reinterpret_cast<const uint4*>(base + uint64_t(k) * stride),
+                                                     uint32_t(counts[k]), drop);
+    }
+    VE_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    VE_CUDA(cudaMemcpyAsync(&h, drop, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    VE_CUDA(cudaStreamSynchronize(c->stream));
+    if (dropped) *dropped = h;
+    return VE_OK;
+}
+
+int ve_split_resolve(ve_ctx* c, const ve_view* view, ve_frame_outputs* out) {
+    if (!c || !view) return fail(VE_ERR_INVALID, "split_resolve: null argument");
+    if (int rc = split_scene_ok(c, view->scene_id, "split_resolve")) return rc;
+    const ve_frame_config& f = view->frame;
+    const ve_frame_config& g = c->split_frame;
+    if (!(f.flags & VE_FRAME_SPLIT) || f.width != g.width || f.height != g.height || f.row_begin != g.row_begin ||
+        f.row_end != g.row_end || f.reconstruction_radius != g.reconstruction_radius)
+        return fail(VE_ERR_STATE, "split_resolve: the view is not the one of the last VE_FRAME_SPLIT frame");
+    if (f.render_type > VE_RENDER_VARIANCE) return fail(VE_ERR_INVALID, "split_resolve: unknown render type");
+    cudaSetDevice(c->device);
+    const uint32_t tiles = ((f.width + 15) / 16) * ((f.height + 15) / 16);
+    const int slot = c->staging_next;
+    c->staging_next = (slot + 1) % ve_ctx::kStaging;
+    VE_CUDA(cudaEventSynchronize(c->staging_ev[slot]));
+    DevView* hv = c->h_views[slot];
+    fill_view(hv[0], *view);
+    cudaStream_t st = c->stream;
+    if (c->copy_stream) VE_CUDA(cudaStreamWaitEvent(st, c->copy_done[0], 0));  // an async copy of set 0
+    VE_CUDA(cudaMemcpyAsync(c->d_views.p, hv, sizeof(DevView), cudaMemcpyHostToDevice, st));
+    VE_CUDA(cudaEventRecord(c->staging_ev[slot], st));
+    FrameArgs a{};
+    a.views = c->d_views.p;
+    a.n_views = 1;
+    a.total_tiles = tiles;
+    a.scenes = c->d_scenes.p;
+    a.mats = c->d_mats.p;
+    a.gbuf = c->gbuf.p;
+    a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
+    a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
+    k_resolve<<<tiles, 256, 0, st>>>(a);
+    VE_CUDA(cudaGetLastError());
+    uint64_t d2h = 0;
+    if (out) {
+        const uint64_t r0 = uint64_t(f.row_begin) * f.width, nr = uint64_t(f.row_end - f.row_begin) * f.width;
+        if (out->gbuffer) { VE_CUDA(cudaMemcpyAsync(out->gbuffer + 4 * r0, c->gbuf.p + r0, nr * 16, cudaMemcpyDeviceToHost, st)); d2h += nr * 16; }
+        if (out->voxel_id) { VE_CUDA(cudaMemcpyAsync(out->voxel_id + r0, c->out_vid.p + r0, nr * 4, cudaMemcpyDeviceToHost, st)); d2h += nr * 4; }
+        if (out->hit_node) { VE_CUDA(cudaMemcpyAsync(out->hit_node + r0, c->out_node.p + r0, nr * 4, cudaMemcpyDeviceToHost, st)); d2h += nr * 4; }
+        if (out->rgb) { VE_CUDA(cudaMemcpyAsync(out->rgb + 3 * r0, c->out_rgb.p + 3 * r0, nr * 12, cudaMemcpyDeviceToHost, st)); d2h += nr * 12; }
+        if (out->mapped) { VE_CUDA(cudaMemcpyAsync(out->mapped + 3 * r0, c->out_mapped.p + 3 * r0, nr * 12, cudaMemcpyDeviceToHost, st)); d2h += nr * 12; }
+    }
+    VE_CUDA(cudaStreamSynchronize(st));
+    c->tot_h2d += sizeof(DevView);
+    c->tot_d2h += d2h;
+    return VE_OK;
 }
 
 int ve_get_launch_config(ve_ctx* c, ve_launch_config* cfg) {

@@ -1,16 +1,22 @@
-"""Multi-GPU plumbing for the replica mode: one process per GPU, no collective
-on the data path.
+"""Multi-GPU plumbing: one process per GPU.
 
-Frames, views and requests are independent; every rank holds its own copy of
-the octree and its own radiance cache and renders its share of the work.  The
-only communication is for measurement: a barrier around the timed region and
-the max (time) / sum (rays) over ranks.
+Replica mode (the default): frames, views and requests are independent;
+every rank holds its own copy of the octree and its own radiance cache and
+renders its share of the work.  The only communication is for measurement: a
+barrier around the timed region and the max (time) / sum (rays) over ranks.
+
+Split frames (SplitFrame): one frame of one view too large for one GPU.
+Each rank renders a band of rows; the frame's cache deposits are exchanged
+once (an all-gather of each rank's records, NCCL over NVLink) and merged by
+every rank in rank order, so all ranks' caches stay identical; each rank
+then runs the AvgPass of its band and the bands are gathered.
 """
 from __future__ import annotations
 
+import dataclasses
 import datetime
 import os
-from typing import List, Optional, Sequence
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple
 
 
 def env_rank() -> tuple:
@@ -80,3 +86,128 @@ def shutdown(dist=None) -> None:
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# split frames
+# ---------------------------------------------------------------------------
+def band_rows(height: int, rank: int, world: int) -> Tuple[int, int]:
+    """Rows [lo, hi) of one rank's band: contiguous, near-equal, in rank order."""
+    if height < world:
+        raise ValueError(f"a frame of {height} rows cannot be split across {world} ranks")
+    return height * rank // world, height * (rank + 1) // world
+
+
+_IMAGE_OUTPUTS = ("voxel_id", "hit_node", "rgb", "mapped")
+_RENDER_OUTPUTS = ("gbuffer", "path_rgb")
+_RECORD_WORDS = 8  # ve_split_record: 8 x 32-bit words
+
+
+class SplitFrame:
+    """Renders frames of one view across the ranks of a process group.
+
+    `renderer` is a ve_b200.Renderer (or an object with its render /
+    split_export / split_merge / split_resolve methods); `dist` the
+    torch.distributed module after init_process_group, or None for one rank.
+    Record exchange and row gathers run on `device` ("cuda" under NCCL).
+    """
+
+    def __init__(self, renderer, scene_id: int, dist=None, device=None):
+        import torch
+
+        self.r = renderer
+        self.scene_id = scene_id
+        self.dist = dist
+        self.rank = dist.get_rank() if dist is not None else 0
+        self.world = dist.get_world_size() if dist is not None else 1
+        if device is None:
+            device = "cuda" if dist is None or dist.get_backend() == "nccl" else "cpu"
+        self.device = torch.device(device)
+        self._buf = None
+        self.last: Dict[str, object] = {}
+
+    def _records(self, cap: int):
+        import torch
+
+        need = max(cap, 1) * _RECORD_WORDS
+        if self._buf is None or self._buf.numel() < need:
+            self._buf = torch.empty(need, dtype=torch.int32, device=self.device)
+        return self._buf
+
+    def _sync(self) -> None:
+        import torch
+
+        if self.device.type == "cuda":
+            torch.cuda.current_stream(self.device).synchronize()
+
+    def exchange(self, local, n: int):
+        """All-gathers every rank's first records of `local` (n of them here):
+        returns (parts, counts, stride) with part k at record k * stride."""
+        import torch
+
+        if self.dist is None:
+            return local, [int(n)], max(int(n), 1)
+        t = torch.tensor([int(n)], dtype=torch.int64, device=self.device)
+        counts_t = [torch.zeros_like(t) for _ in range(self.world)]
+        self.dist.all_gather(counts_t, t)
+        counts = [int(c.item()) for c in counts_t]
+        stride = max(max(counts), 1)
+        mine = local[: stride * _RECORD_WORDS]
+        if self.dist.get_backend() == "nccl":
+            parts = torch.empty(self.world * stride * _RECORD_WORDS, dtype=torch.int32, device=self.device)
+            self.dist.all_gather_into_tensor(parts, mine)
+        else:
+            lst = [torch.empty_like(mine) for _ in range(self.world)]
+            self.dist.all_gather(lst, mine)
+            parts = torch.cat(lst)
+        self._sync()  # the renderer's stream reads the parts next
+        return parts, counts, stride
+
+    def gather_rows(self, image, lo: int, hi: int, height: int):
+        """Full image from every rank's band [lo, hi) of a (height, ...) array."""
+        import numpy as np
+        import torch
+
+        if self.dist is None:
+            return image
+        rows = max(height * (k + 1) // self.world - height * k // self.world for k in range(self.world))
+        band = np.zeros((rows,) + image.shape[1:], image.dtype)
+        band[: hi - lo] = image[lo:hi]
+        if band.dtype.itemsize != 4:
+            raise ValueError("rows of 32-bit elements only")
+        t = torch.from_numpy(band.view(np.int32)).to(self.device)
+        lst = [torch.empty_like(t) for _ in range(self.world)]
+        self.dist.all_gather(lst, t)
+        out = np.empty_like(image)
+        for k, part in enumerate(lst):
+            a, b = band_rows(height, k, self.world)
+            out[a:b] = part.cpu().numpy().view(image.dtype)[: b - a]
+        return out
+
+    def render(self, camera, fc, outputs: Iterable[str] = ("rgb",), gather: bool = True) -> Dict[str, object]:
+        """One frame; returns full-size host images (only this rank's band
+        rows are filled when gather=False)."""
+        from . import FRAME_SPLIT
+
+        want = list(outputs)
+        lo, hi = band_rows(fc.height, self.rank, self.world)
+        f = dataclasses.replace(fc, flags=fc.flags | FRAME_SPLIT, row_begin=lo, row_end=hi)
+        out = dict(self.r.render(self.scene_id, camera, f, outputs=[k for k in want if k in _RENDER_OUTPUTS]))
+        # a band's deposits land on its pixels' primary voxels: at most one
+        # record per pixel of the largest band
+        cap = max(fc.height * (k + 1) // self.world - fc.height * k // self.world for k in range(self.world)) * fc.width
+        buf = self._records(cap)
+        n = self.r.split_export(self.scene_id, buf, cap)
+        parts, counts, stride = self.exchange(buf, n)
+        dropped = self.r.split_merge(self.scene_id, parts, counts, stride)
+        out.update(self.r.split_resolve(self.scene_id, camera, f, [k for k in want if k in _IMAGE_OUTPUTS]))
+        if gather:
+            for k in list(out):
+                a = out[k]
+                if k == "path_rgb":  # pixel-major: rows of width * spp paths
+                    a = a.reshape(fc.height, fc.width * fc.spp, 3)
+                    out[k] = self.gather_rows(a, lo, hi, fc.height).reshape(-1, 3)
+                else:
+                    out[k] = self.gather_rows(a, lo, hi, fc.height)
+        self.last = {"band": (lo, hi), "records": n, "counts": counts, "dropped": dropped}
+        return out
