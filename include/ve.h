@@ -327,7 +327,8 @@ typedef struct ve_split_record {
 } ve_split_record;
 /* Records of the last VE_FRAME_SPLIT frame of `scene_id` into device memory
  * `dev_out` (room for `cap`); `n` = records in the frame (written: min(n,
- * cap)).  Synchronous. */
+ * cap)).  A frame's records are exported once: the export empties the
+ * per-frame table.  Synchronous. */
 int ve_split_export(ve_ctx* ctx, int32_t scene_id, void* dev_out, uint64_t cap, uint64_t* n);
 /* Adds `n_parts` record arrays (device memory; part k starts at record
  * k * stride and holds counts[k] records) into the scene's cache, part 0

@@ -41,7 +41,7 @@ def pinned(shape, dtype):
 
 
 def test_async_frames_equal_sync_frames(ve, pair):
-    (ra, sa), (rb, sb) = pair
+    (ra, sa), (rb, sb) = pair[0]
     cam, fc = pair[1], pair[2]
     ra.cache_reset(sa)
     rb.cache_reset(sb)

@@ -725,6 +725,20 @@ class Renderer:
         _check(self._lib.ve_split_resolve(self._h, ctypes.byref(view), ctypes.byref(o) if want else None))
         return arrays
 
+    def split_resolve_into(self, scene_id: int, camera: np.ndarray, fc: FrameConfig,
+                           arrays: Dict[str, np.ndarray]) -> None:
+        """split_resolve into caller-owned full-size host arrays (the band's
+        rows are written)."""
+        npx = fc.width * fc.height
+        size = {"gbuffer": 4 * npx, "voxel_id": npx, "hit_node": npx, "rgb": 3 * npx, "mapped": 3 * npx}
+        o = FrameOutputsC()
+        for k, a in arrays.items():
+            if k not in size or not a.flags.c_contiguous or a.size != size[k] or a.itemsize != 4:
+                raise ValueError(f"output {k!r}: {size.get(k)} contiguous 32-bit elements expected")
+            setattr(o, k, a.ctypes.data)
+        view = self.make_view(scene_id, camera, fc)
+        _check(self._lib.ve_split_resolve(self._h, ctypes.byref(view), ctypes.byref(o)))
+
     def launch_config(self) -> Dict[str, int]:
         c = LaunchConfigC()
         _check(self._lib.ve_get_launch_config(self._h, ctypes.byref(c)))

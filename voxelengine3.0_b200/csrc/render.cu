@@ -1906,6 +1906,7 @@ struct ve_ctx {
     ve::DevBuf<ve::DevScene> d_scenes_split;
     ve::DevBuf<uint32_t> split_cnt;
     int split_scene = -1;
+    bool split_delta_clean = false;  // the per-frame table is all zeros (cleared by the last export)
     ve_frame_config split_frame{};  // the last split frame's config
     ve::DevBuf<float> ray_in;      // ve_raycast_batch: origins and directions
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
@@ -2524,7 +2525,14 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if ((rc = c->split_delta.ensure(size_t(1) << c->cfg.hash_log2)) ||
             (rc = c->d_scenes_split.ensure(c->d_scenes.cap)) || (rc = c->split_cnt.ensure(2)))
             return rc;
-        if (before[0] != c->split_delta.p || before[1] != c->d_scenes_split.p) c->gen++;
+        if (before[0] != c->split_delta.p || before[1] != c->d_scenes_split.p) {
+            c->gen++;
+            c->split_delta_clean = false;
+        }
+        if (!c->split_delta_clean)  // not exported since its last frame (or new): clear it
+            VE_CUDA(cudaMemsetAsync(c->split_delta.p, 0, (size_t(1) << c->cfg.hash_log2) * sizeof(CacheEntry),
+                                    c->stream));
+        c->split_delta_clean = false;
         CacheEntry* delta = c->split_delta.p;
         VE_CUDA(cudaMemcpyAsync(c->d_scenes_split.p, c->d_scenes.p, c->scenes.size() * sizeof(DevScene),
                                 cudaMemcpyDeviceToDevice, c->stream));
@@ -2655,7 +2663,6 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (flags & VE_FRAME_PATH_RGB) cudaMemsetAsync(c->path_rgb.p, 0, paths * 3 * sizeof(float), st);
         // lBuffer frames: row 0 (no deposit) for paths that are never spawned
         if (lbm) cudaMemsetAsync(c->lb_keys.p, 0, paths * sizeof(uint32_t), st);
-        if (split) cudaMemsetAsync(c->split_delta.p, 0, (size_t(1) << c->cfg.hash_log2) * sizeof(CacheEntry), st);
         rec();
         for (auto& d : decays) {
             if (d.second != 1.0f) {
@@ -2916,8 +2923,9 @@ __global__ void __launch_bounds__(256) k_raycast_batch(DevScene S, const float* 
 }
 
 // Split frames: the per-frame deposit table as records {vid, count, luma^2,
-// r, g, b, weight, 0}, compacted by a warp-aggregated counter.
-__global__ void __launch_bounds__(256) k_split_export(const CacheEntry* __restrict__ t, uint32_t n,
+// r, g, b, weight, 0}, compacted by a warp-aggregated counter; the entries
+// read are cleared, so the table is empty for the next split frame.
+__global__ void __launch_bounds__(256) k_split_export(CacheEntry* __restrict__ t, uint32_t n,
                                                       uint4* __restrict__ out, uint32_t cap, uint32_t* cnt) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // uniform per warp
@@ -2925,6 +2933,7 @@ __global__ void __launch_bounds__(256) k_split_export(const CacheEntry* __restri
         CacheEntry e{};
         if (i < n) e = t[i];
         const bool live = i < n && e.key != 0u;
+        if (live) t[i] = CacheEntry{};
         const uint32_t j = warp_append(live, cnt);
         if (live && j < cap) {
             out[2ull * j + 0] = make_uint4(e.key, e.count, __float_as_uint(e.l2), __float_as_uint(e.rgbw.x));
@@ -3672,6 +3681,7 @@ int ve_split_export(ve_ctx* c, int32_t id, void* dev_out, uint64_t cap, uint64_t
     k_split_export<<<c->num_sms * 8, 256, 0, c->stream>>>(c->split_delta.p, uint32_t(N),
                                                           static_cast<uint4*>(dev_out), uint32_t(cap), cnt);
     VE_CUDA(cudaGetLastError());
+    c->split_delta_clean = true;
     uint32_t h = 0;
     VE_CUDA(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));

@@ -124,7 +124,23 @@ class SplitFrame:
             device = "cuda" if dist is None or dist.get_backend() == "nccl" else "cpu"
         self.device = torch.device(device)
         self._buf = None
+        self._images: Dict[str, object] = {}  # pinned host images, reused frame to frame
         self.last: Dict[str, object] = {}
+
+    def _image(self, name: str, fc):
+        """A pinned full-size host image for output `name` (32-bit elements)."""
+        import numpy as np
+        import torch
+
+        shape = {"voxel_id": (fc.height, fc.width), "hit_node": (fc.height, fc.width),
+                 "rgb": (fc.height, fc.width, 3), "mapped": (fc.height, fc.width, 3)}[name]
+        dtype = np.uint32 if name in ("voxel_id", "hit_node") else np.float32
+        t = self._images.get(name)
+        if t is None or tuple(t.shape) != shape:
+            t = torch.empty(shape, dtype=torch.int32 if dtype == np.uint32 else torch.float32,
+                            pin_memory=torch.cuda.is_available())
+            self._images[name] = t
+        return t.numpy().view(dtype)
 
     def _records(self, cap: int):
         import torch
@@ -186,7 +202,8 @@ class SplitFrame:
 
     def render(self, camera, fc, outputs: Iterable[str] = ("rgb",), gather: bool = True) -> Dict[str, object]:
         """One frame; returns full-size host images (only this rank's band
-        rows are filled when gather=False)."""
+        rows are filled when gather=False).  Without a gather (or on one
+        rank) the images are pinned buffers that the next call reuses."""
         from . import FRAME_SPLIT
 
         want = list(outputs)
@@ -200,7 +217,12 @@ class SplitFrame:
         n = self.r.split_export(self.scene_id, buf, cap)
         parts, counts, stride = self.exchange(buf, n)
         dropped = self.r.split_merge(self.scene_id, parts, counts, stride)
-        out.update(self.r.split_resolve(self.scene_id, camera, f, [k for k in want if k in _IMAGE_OUTPUTS]))
+        images = {k: self._image(k, fc) for k in want if k in _IMAGE_OUTPUTS}
+        if hasattr(self.r, "split_resolve_into"):
+            self.r.split_resolve_into(self.scene_id, camera, f, images)
+            out.update(images)
+        else:
+            out.update(self.r.split_resolve(self.scene_id, camera, f, list(images)))
         if gather:
             for k in list(out):
                 a = out[k]
