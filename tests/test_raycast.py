@@ -84,7 +84,7 @@ def scenes(ve, oracle):
     words, depth, *_ = helpers.small_setup()
     out.append((r.upload_scene(words, depth), depth))
     rng = np.random.default_rng(11)
-    for depth, density in ((5, 0.2), (8, 0.002), (9, 0.0005)):
+    for depth, density in ((5, 0.2), (8, 0.002), (9, 0.0005), (10, 0.00005)):
         xyzm = helpers.random_voxels(rng, depth, density)
         out.append((r.build_scene(xyzm, depth), depth))
     yield r, [(sid, r.download_scene(sid), depth) for sid, depth in out]
@@ -106,6 +106,39 @@ def test_device_rays_match_oracle(ve, oracle, scenes, full_walk):
                 bad = np.nonzero((dev != ref).any(1))[0]
                 assert bad.size == 0, (depth, name, cc, bad[:5].tolist(), o[bad[:1]].tolist(), d[bad[:1]].tolist(),
                                        dev[bad[:1]].tolist(), ref[bad[:1]].tolist())
+
+
+@pytest.mark.gpu
+def test_depth10_terrain_rays_match_oracle(ve, oracle):
+    """The benchmark's depth-10 terrain (77.6M node words): rays from the
+    orbit camera's eye, from inside the volume and from surface points."""
+    import ve_b200.workloads as wl
+
+    W = wl.LARGE
+    words, _ = ve.terrain_words(W.depth, W.variant, W.seed)
+    r = ve.Renderer(hash_log2=16)
+    try:
+        sid = r.upload_scene(words, W.depth)
+        dev_words = r.download_scene(sid)
+        rng = np.random.default_rng(21)
+        eye, _ = wl.orbit_camera(0, W.frames, W.seed)
+        n = 20000
+        target = rng.uniform((0.0, 0.0, 0.0), (1024.0, 128.0, 1024.0), (n, 3))
+        d = target - np.float64(eye)
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        sets = {"eye": (np.repeat(np.float32(eye)[None], n, 0), d)}
+        sets.update(ray_sets(rng, W.depth, n))
+        sets["shading"] = shading_rays(rng, dev_words, W.depth, oracle, 4000)
+        for name, (o, dd) in sets.items():
+            for full in (False, True):
+                dev = r.raycast_batch(sid, o, dd, W.bounce_controlchecks, full_walk=full)
+                ref = oracle.raycast_batch(dev_words, W.depth, o, dd, W.bounce_controlchecks)
+                bad = np.nonzero((dev != ref).any(1))[0]
+                assert bad.size == 0, (name, full, bad[:5].tolist())
+                if name == "eye":
+                    assert (ref[:, 0] == 0).mean() > 0.3  # rays from the eye toward the terrain hit it
+    finally:
+        r.close()
 
 
 @pytest.mark.gpu
