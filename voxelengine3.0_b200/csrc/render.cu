@@ -1010,8 +1010,11 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
 // hit in registers (the same shade_step the shade pass runs), appending its
 // rays and live entry for trace pass 0 / shade pass 1 — the frame's largest
 // shade pass never round-trips the path state through memory.
+// 4 CTAs/SM (64 registers, ~110 B of spills in the plain instance): the
+// kernel is latency-bound, and the extra warps beat the spills (0.49 -> 0.44
+// ms per 1080p depth-10 frame).
 template <bool COUNT, bool FUSED, int MODE = 0>
-__global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
+__global__ void __launch_bounds__(256, 4) k_primary(FrameArgs a) {
     __shared__ DepSlot dep[FUSED ? 256 : 1];
     const uint32_t tile = blockIdx.x;
     const uint32_t vi = find_view(a.views, a.n_views, tile);
@@ -1115,8 +1118,13 @@ __global__ void __launch_bounds__(256, 3) k_primary(FrameArgs a) {
     }
 }
 
+// 4 CTAs/SM, as k_primary (latency-bound on the path-state loads: 0.50 ->
+// 0.45 ms per 1080p depth-10 frame).  Every instance, and k_sched_emit, which
+// runs on the same grid, shares this bound: the shade grid is sized from the
+// plain instance's occupancy, and an instance with fewer resident CTAs per SM
+// would run part of that grid as a second wave.
 template <int MODE = 0>
-__global__ void __launch_bounds__(256, 3) k_shade(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
@@ -1297,7 +1305,7 @@ __global__ void k_sched_threshold(float* rank, const DevView* views) {
 // primary hit, list index i seeding the RNG; its first shading step runs
 // here as in the fused primary pass.
 template <int MODE = 0>
-__global__ void __launch_bounds__(256, 3) k_sched_emit(FrameArgs a) {
+__global__ void __launch_bounds__(256, 4) k_sched_emit(FrameArgs a) {
     __shared__ DepSlot dep[256];
     const DevView& v = a.views[0];
     const uint32_t n = a.counters[CNT_SCHED];
