@@ -394,7 +394,9 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
 // Persistent kernel with per-lane refill: a lane whose ray has finished takes
 // the next queue entry (one warp-aggregated atomicAdd on a per-pass cursor
 // serves all idle lanes of the warp, once `refill` of them are idle or none is
-// busy), so warps stay full although ray lengths differ by 100x.
+// busy), so warps stay full although ray lengths differ by 100x.  One ballot
+// per step: once a refill hands out the queue's last entry the warp stops
+// refilling (a warp-uniform flag) and runs its remaining rays out.
 // EM: the batch has VE_FRAME_EMISSIVE views (shadow rays toward lights).
 template <bool COUNT, bool EM = false>
 __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
@@ -404,7 +406,8 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
     const uint32_t n = n_ext + a.counters[CNT_RAYSH + pass];
     uint32_t* cursor = &a.counters[CNT_CURSOR + pass];
     const uint32_t lane = lane_id();
-    bool active = false, exhausted = false;
+    bool active = false;
+    bool drained = false;  // warp-uniform: every ray of the pass has been handed out
     uint32_t e = 0, D = 0, T0 = 0;
     const uint32_t* nodes = nullptr;
     const uint32_t* top = nullptr;
@@ -416,16 +419,17 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
         Hit h;
         h.status = kEscaped;
         h.id = h.material = h.x = h.y = h.z = 0u;
-        const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
         const unsigned busy = __ballot_sync(0xffffffffu, active);
-        if (idle == 0u && busy == 0u) break;
+        if (drained && busy == 0u) break;
+        const unsigned idle = drained ? 0u : ~busy;
         bool finished = false;
         if (idle != 0u && (uint32_t(__popc(idle)) >= a.refill || busy == 0u)) {
             const int leader = __ffs(idle) - 1;
             uint32_t first_idx = 0;
             if (int(lane) == leader) first_idx = atomicAdd(cursor, uint32_t(__popc(idle)));
             first_idx = __shfl_sync(0xffffffffu, first_idx, leader);
-            if (!active && !exhausted) {
+            drained = first_idx + uint32_t(__popc(idle)) >= n;
+            if (!active) {
                 const uint32_t idx = first_idx + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (idx < n) {
                     e = idx < n_ext ? a.rayq[idx] : a.rayq_sh[idx - n_ext];
@@ -443,8 +447,6 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                     if (EM && (e >> 31) && (v.flags & VE_FRAME_EMISSIVE)) d = ld3(a.p_sdir[p]);
                     finished = dda_init(s, o, d, v.cc_bounce, D, h);
                     active = !finished;
-                } else {
-                    exhausted = true;
                 }
             }
         }
