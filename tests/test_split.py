@@ -353,6 +353,8 @@ def test_split_rejects(ve, ranks):
     assert n > 64
     with pytest.raises(ve.VeError):  # more records than the stride
         r.split_merge(sid, buf, [65], 64)
+    with pytest.raises(ve.VeError):  # a stride whose part offsets would overflow
+        r.split_merge(sid, buf, [1, 1], 1 << 62)
     with pytest.raises(ve.VeError):  # the resolve's view differs from the frame's
         r.split_resolve(sid, cam, dataclasses.replace(f, row_end=f.row_end + 1), ("rgb",))
     r.render(sid, cam, fc, outputs=())  # a plain frame ends the split state

@@ -3654,15 +3654,15 @@ static int check_device_range(ve_ctx* c, const void* p, uint64_t bytes, const ch
         return fail(VE_ERR_INVALID, std::string(what) + ": not device memory of the context's GPU");
     }
     using RangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
-    static RangeFn range = nullptr;
-    if (!range) {
+    static const RangeFn range = []() -> RangeFn {  // looked up once (thread-safe static init)
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q{};
         if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &q) ==
                 cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            range = reinterpret_cast<RangeFn>(fn);
-    }
+            return reinterpret_cast<RangeFn>(fn);
+        return nullptr;
+    }();
     if (!range) return fail(VE_ERR_CUDA, std::string(what) + ": cannot query allocation ranges");
     CUdeviceptr base = 0;
     size_t size = 0;
@@ -3705,6 +3705,9 @@ int ve_split_merge(ve_ctx* c, int32_t id, const void* dev_parts, const uint64_t*
                    uint64_t stride, uint64_t* dropped) {
     if (int rc = split_scene_ok(c, id, "split_merge")) return rc;
     if (n_parts && !counts) return fail(VE_ERR_INVALID, "split_merge: null counts");
+    // bounds that keep part offsets (k * stride records) far from overflow
+    if (n_parts > 65536u) return fail(VE_ERR_INVALID, "split_merge: at most 65536 parts");
+    if (stride > (uint64_t(1) << 36)) return fail(VE_ERR_INVALID, "split_merge: stride beyond any allocation");
     const uint64_t N = uint64_t(1) << c->cfg.hash_log2;
     uint64_t end = 0;
     for (uint32_t k = 0; k < n_parts; k++) {
