@@ -141,14 +141,16 @@ def rays_of(st):
 
 
 def cpu_baseline(ve, W, words, mats, budget_s):
-    """Oracle on all host cores over a bounded band of rows of frame 0."""
-    from oracle.oracle import Oracle, OracleRenderer, frame_params
+    """Oracle on all host cores over whole frames of the orbit (frame 0 first;
+    rows of it when one frame exceeds the budget), plus a 1-thread figure on
+    a band of rows of frame 0 and the CPU model."""
+    from oracle.oracle import Oracle, OracleRenderer
+    from oracle import scenes
 
     orc = Oracle()
     threads = os.cpu_count() or 1
-    eye, d = _orbit(W, 0)
-    cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
-    fp = frame_params(frame_config(ve, W, 0))
+    cam = scenes.large_camera(orc, 0)
+    fp = scenes.large_params(0)
     mid = W.height // 2
     rows = max(threads, 8)
     total_rays = 0
@@ -164,72 +166,88 @@ def cpu_baseline(ve, W, words, mats, budget_s):
         if dt * 2.5 > budget_s or rows >= W.height:
             break
         rows = min(W.height, int(rows * max(2.0, budget_s / max(dt, 1e-3) * 0.5)))
+    # one thread: a band of rows of frame 0 sized to about a fifth of the budget
+    rows1 = 2
+    while True:
+        r1 = mid - rows1 // 2
+        t = time.perf_counter()
+        o1 = OracleRenderer(orc).render(words, W.depth, mats, cam, fp, threads=1, rows=(r1, r1 + rows1),
+                                        want_rgb=False)
+        dt1 = time.perf_counter() - t
+        n1 = rays_of_oracle(o1["stats"])
+        if dt1 * 2.5 > budget_s / 5 or rows1 >= W.height:
+            break
+        rows1 = min(W.height, rows1 * 2)
     return {"value": total_rays / total_t / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
             "sample": f"frame 0 rows {r0}-{r0 + rows - 1} of {W.width}x{W.height}, {W.spp} spp x {W.bounces} "
-                      f"bounces, {total_rays} rays in {total_t:.1f} s"}
+                      f"bounces, {total_rays} rays in {total_t:.1f} s",
+            "threads_1": {"value": n1 / dt1 / 1e6, "unit": "Mrays/s", "cores": 1,
+                          "sample": f"frame 0 rows {r1}-{r1 + rows1 - 1}, {n1} rays in {dt1:.1f} s"},
+            "cpu_model": scenes.cpu_model(), "nproc": threads}
 
 
-def _orbit(W, f):
-    import ve_b200.workloads as w
+def large_config(n_voxels, n_words):
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": "large: depth-10 (1024^3) terrain + overhangs, 1920x1080, 4 spp x 3 bounces, "
+                        "hash 2^22, decay 0.95, orbit r=600 (one whole frame per step)",
+            "voxels": int(n_voxels), "node_words": int(n_words), "controlchecks": [300, 300],
+            "frames": "orbit frames 0, 1, 2, ... (warm-up first)",
+            "l2": "inputs larger than L2 (310 MB node array, ~1 GB path state)",
+            "parallelism": "replicas"}
 
-    return w.orbit_camera(f, W.frames, W.seed)
 
-
-def run_reference(args, W, rank, world):
-    """The reference's path on the host CPU (oracle port, all threads)."""
+def run_reference(args, rank, world):
+    """The reference's path on the host CPU: the oracle port of its passes on
+    all host threads, whole frames of the large workload, the same frames as
+    rank 0 of the device arm.  Maps no product library: the scene, materials,
+    camera and frame parameters come from oracle/ (oracle/scenes.py)."""
     if rank != 0:
         return 0
-    ve = load_package()
-    import ve_b200.workloads  # noqa: F401
-    from oracle.oracle import Oracle, OracleRenderer, frame_params
+    from oracle.oracle import Oracle, OracleRenderer
+    from oracle import scenes
 
-    words, nv = ve.terrain_words(W.depth, W.variant, W.seed)
-    mats = ve.terrain_materials(W.seed)
+    W = scenes.LARGE
     orc = Oracle()
-    # normals as the device pass computes them (3x3x3 occupancy gradient)
-    words = _words_with_normals(orc, words, W.depth)
     threads = os.cpu_count() or 1
+    words, nv = scenes.terrain_words(orc, W.depth, W.variant, W.seed, threads)
+    # normals as the device pass computes them (3x3x3 occupancy gradient)
+    words = orc.fill_normals(words, W.depth, fast=True, threads=threads)
+    mats = scenes.terrain_materials(orc, W.seed)
     rr = OracleRenderer(orc)
-    rows_per_step = max(threads, 16)
 
     def step(f):
-        eye, d = _orbit(W, f % W.frames)
-        cam = ve.camera_ubo(eye, d, W.fov, W.width / W.height)
-        r0 = (W.height // 2 - rows_per_step // 2)
+        cam = scenes.large_camera(orc, f)
         t = time.perf_counter()
-        out = rr.render(words, W.depth, mats, cam, frame_params(frame_config(ve, W, f)), threads=threads,
-                        rows=(r0, r0 + rows_per_step), want_rgb=False)
+        out = rr.render(words, W.depth, mats, cam, scenes.large_params(f % W.frames), threads=threads)
         return time.perf_counter() - t, rays_of_oracle(out["stats"])
 
     for f in range(args.warmup):
         step(f)
     tt = 0.0
     rays = 0
-    for f in range(args.steps):
-        dt, n = step(args.warmup + f)
+    for i in range(args.steps):
+        dt, n = step(args.warmup + i)
         tt += dt
         rays += n
     v = rays / tt / 1e6
-    sample = (f"{rows_per_step} rows x {W.width} px per frame (frames {args.warmup}..{args.warmup + args.steps - 1} "
-              f"of the orbit), {W.spp} spp x {W.bounces} bounces")
+    sample = (f"whole {W.width}x{W.height} frames {args.warmup}..{args.warmup + args.steps - 1} of the orbit "
+              f"(after {args.warmup} warm-up frames), {W.spp} spp x {W.bounces} bounces, GBuffer + paths + "
+              f"FP64 radiance cache + AvgPass, {rays} rays in {tt:.1f} s")
     line = {"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tt / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain)",
-            "impl": "reference",
-            "config": {"workload": "large: depth-10 terrain 1920x1080 4 spp x 3 bounces (row band per step)"},
-            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded value-noise terrain, seeded orbit camera)", "impl": "reference",
+            "config": large_config(nv, words.size),
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": "port", "sample": sample,
+                             "cpu_model": scenes.cpu_model(), "nproc": threads},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "rays_per_step": rays / args.steps}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def rays_of_oracle(s):
     return s["rays_primary"] + s["rays_bounce"] + s["rays_shadow"]
-
-
-def _words_with_normals(orc, words, depth):
-    """Leaf normals filled on the CPU by the oracle (bitmask occupancy)."""
-    return orc.fill_normals(words, depth, fast=True, threads=os.cpu_count() or 1)
 
 
 def run_batching(args, rank, world):
@@ -913,12 +931,12 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
     ve = load_package()
     import ve_b200.workloads as wl
 
     W = wl.LARGE
-    if args.impl == "reference":
-        return run_reference(args, W, rank, world)
     if args.workload == "batching":
         return run_batching(args, rank, world)
     if args.workload == "serving":
@@ -1052,15 +1070,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded value-noise terrain, seeded orbit camera)",
-            "config": {
-                "workload": "large: depth-10 (1024^3) terrain + overhangs, 66.2M voxels, 1920x1080, "
-                            "4 spp x 3 bounces, hash 2^22, decay 0.95, orbit r=600",
-                "voxels": int(nv), "node_words": int(words.size),
-                "controlchecks": [W.primary_controlchecks, W.bounce_controlchecks],
-                "l2": "inputs larger than L2 (310 MB node array, ~1 GB path state)",
-                "rays_per_step": rays_of(tot) / K,
-                "ray_mix_per_step": {k: tot[k] / K for k in ("rays_primary", "rays_bounce", "rays_shadow")},
-                "parallelism": f"replicas x{world}"},
+            "config": large_config(nv, words.size),
+            "rays_per_step": rays_of(tot) / K,
+            "ray_mix_per_step": {k: tot[k] / K for k in ("rays_primary", "rays_bounce", "rays_shadow")},
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": etot["h2d_bytes"] / K,
                     "d2h_bytes_per_step": etot["d2h_bytes"] / K},
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce + shadow DDA)", "achieved": achieved,

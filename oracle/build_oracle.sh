@@ -5,5 +5,5 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 g++ -std=c++17 -O2 -ffp-contract=off -fno-fast-math -fPIC -shared -pthread -Wall -Wno-unused-function \
-    "$HERE/ve_oracle.cpp" -o "$HERE/liboracle.so"
+    "$HERE/ve_oracle.cpp" "$HERE/terrain_oracle.cpp" -o "$HERE/liboracle.so"
 echo "build_oracle: wrote $HERE/liboracle.so"

@@ -49,8 +49,9 @@ class Stats(ctypes.Structure):
 
 
 def build_oracle(force: bool = False) -> str:
-    src = os.path.join(HERE, "ve_oracle.cpp")
-    if force or not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("ve_oracle.cpp", "terrain_oracle.cpp", "ve_oracle.h")]
+    if force or not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(ORACLE_LIB) < os.path.getmtime(s)
+                                                       for s in srcs):
         subprocess.check_call(["bash", os.path.join(HERE, "build_oracle.sh")])
     return ORACLE_LIB
 
