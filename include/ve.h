@@ -264,6 +264,21 @@ int ve_scene_refresh(ve_ctx* ctx, int32_t scene_id, const uint32_t* xyz, uint64_
  * VE_SCENE_KEEP_NORMALS.  The scene's radiance cache is kept. */
 int ve_scene_apply_edits(ve_ctx* ctx, int32_t scene_id, const uint32_t* slots, const uint32_t* words, uint64_t n,
                          uint32_t flags);
+/* Per-voxel normal mode of a scene (replaces the normalPrecision uniform of
+ * the reference's normal pass, src/renderer/core.hpp:88 and
+ * src/shd/normal.comp:55-95).  radius 0: the 3x3x3 occupancy gradient (the
+ * default at upload).  radius R >= 1: the reference's computeRefinedNormal —
+ * the offsets of the empty neighbours with 0 < |d|^2 <= R^2 around the
+ * voxel's even-aligned corner (normal.comp:147-152), out-of-volume neighbours
+ * empty, normalized ((0,1,0) for a zero sum), 10-10-10 packed
+ * (packNormalAccum); the scene keeps the sorted table of its distinct codes
+ * and each leaf's normal field (bits 8-30, bit 31 clear) holds its code's
+ * index + 1.  Recomputes every leaf now; later full normal passes
+ * (ve_scene_apply_edits without VE_SCENE_KEEP_NORMALS) keep the mode, and
+ * ve_scene_refresh is refused (VE_ERR_STATE) for ball-mode scenes.  Scenes of
+ * depth <= 11; VE_ERR_INVALID for radius > VE_NORMAL_BALL_MAX_RADIUS. */
+#define VE_NORMAL_BALL_MAX_RADIUS 16u
+int ve_scene_normal_mode(ve_ctx* ctx, int32_t scene_id, uint32_t radius);
 int ve_scene_download(ve_ctx* ctx, int32_t scene_id, uint32_t* out, uint64_t cap, uint64_t* n_words);
 
 /* A batch of independent rays through the device DDA that the frame kernels
@@ -372,17 +387,28 @@ int ve_reset_total_stats(ve_ctx* ctx);
  * reference renders one interactive view per Renderer::run)
  * ==================================================================== */
 
-/* Requests are admitted first come first served while their framebuffer
- * (pixel_capacity pool) and path-state (path_capacity pool) ranges fit — the
- * per-request part of the HBM budget; scenes and radiance caches stay
- * resident — and join the in-flight wavefront at the next bounce pass.  The
- * server owns the context's stream while it exists. */
+/* Requests are admitted while their framebuffer (pixel_capacity pool) and
+ * path-state (path_capacity pool) ranges fit — the per-request part of the
+ * HBM budget; scenes and radiance caches stay resident — and join the
+ * in-flight wavefront at the next bounce pass.  Admission takes queued
+ * requests in arrival order and passes over one that does not fit yet, unless
+ * it has waited longer than max_bypass_ms: then nothing behind it is admitted
+ * until it fits (the pools drain for it).  Each step starts the primary pass
+ * of at most step_path_budget paths: a larger request's tiles are spread over
+ * several steps, so no step grows long enough to hold up the small requests
+ * in flight.  VE_SERVER_FIFO restores strict first-come-first-served
+ * admission with each request's whole primary pass in one step.  The server
+ * owns the context's stream while it exists. */
+#define VE_SERVER_FIFO 1u
 typedef struct ve_server ve_server;
 typedef struct ve_server_config {
-    uint64_t pixel_capacity; /* pooled pixels: GBuffer + outputs, 48 B each */
-    uint64_t path_capacity;  /* pooled path states, 144 B each */
-    uint32_t max_requests;   /* view slots (requests on the GPU at once) */
-    uint32_t flags;
+    uint64_t pixel_capacity;   /* pooled pixels: GBuffer + outputs, 48 B each */
+    uint64_t path_capacity;    /* pooled path states, 144 B each */
+    uint32_t max_requests;     /* view slots (requests on the GPU at once) */
+    uint32_t flags;            /* VE_SERVER_FIFO */
+    uint64_t step_path_budget; /* paths whose primary pass one step may start (0: 2^22) */
+    uint32_t max_bypass_ms;    /* how long a request that does not fit may be passed over (0: 50 ms) */
+    uint32_t reserved;
 } ve_server_config;
 typedef struct ve_request_info {
     uint64_t request_id;
@@ -473,9 +499,14 @@ int ve_scene_set_nrc(ve_ctx* ctx, int scene_id, ve_nrc* nrc);
  * (frontiers + occupancy bitmask), present on every GPU that loads the
  * library until the process exits, which limits the scene to depth <= 7
  * (VE_ERR_CAPACITY beyond).  The first call on a device looks up that array's
- * device address with the device current; make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
- * GPU (on different streams, or from several threads) race on it. */
+ * device address with the device current, and so does the first call after
+ * the current context changed (cudaDeviceReset, or another context made
+ * current); make those calls before any stream capture.  All calls share the
+ * one array: calls that overlap on the GPU (on different streams, or from
+ * several threads) race on it.  A well-formed depth-7 array never outgrows
+ * the scratch; a malformed one (blocks that point back up the tree) can, and
+ * then the cells beyond the scratch are skipped: the call still returns
+ * VE_OK with only some normals filled. */
 #define VE_NOALLOC_MAX_DEPTH 7
 #define VE_NOALLOC_SCRATCH_BYTES (256u + 2u * (1u << 18) * 8u + (1u << 21) / 8u)
 int ve_fill_normals_noalloc(uint32_t* device_words, uint64_t n_words, uint32_t depth, void* stream);

@@ -74,6 +74,9 @@ class Oracle:
         L.oracle_build.argtypes = [_U32, _np(np.uint32), _U64, _np(np.uint32), _U64, ctypes.POINTER(_U32)]
         L.oracle_fill_normals.argtypes = [_np(np.uint32), _U64, _U32]
         L.oracle_fill_normals_mode.argtypes = [_np(np.uint32), _U64, _U32, ctypes.c_int, _U32]
+        L.oracle_fill_normals_ball.restype = _U64
+        L.oracle_fill_normals_ball.argtypes = [_np(np.uint32), _U64, _U32, _U32, _U32, _P, _U64]
+        L.oracle_renderer_set_normal_codes.argtypes = [_P, _P, _U64]
         L.oracle_lookup_occupied.restype = ctypes.c_int
         L.oracle_lookup_occupied.argtypes = [_np(np.uint32), _U64, _U32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int64]
@@ -118,6 +121,15 @@ class Oracle:
         w = np.ascontiguousarray(words, np.uint32).copy()
         self.lib.oracle_fill_normals_mode(w, w.size, depth, 1 if fast else 0, threads)
         return w
+
+    def fill_normals_ball(self, words: np.ndarray, depth: int, radius: int, threads: int = 1):
+        """The reference's normal mode (normal.comp's L2 ball of `radius`):
+        (words with the leaves' code indices, the sorted code table)."""
+        w = np.ascontiguousarray(words, np.uint32).copy()
+        n = self.lib.oracle_fill_normals_ball(w.copy(), w.size, depth, radius, threads, None, 0)
+        codes = np.zeros(max(n, 1), np.uint32)
+        self.lib.oracle_fill_normals_ball(w, w.size, depth, radius, threads, codes.ctypes.data, n)
+        return w, codes[:n]
 
     def occupied(self, words, depth, x, y, z) -> bool:
         return bool(self.lib.oracle_lookup_occupied(np.ascontiguousarray(words, np.uint32), words.size, depth,
@@ -215,6 +227,11 @@ class OracleRenderer:
         assert rc == 0
         stats = {k: getattr(st, k) for k, _ in Stats._fields_}
         return {"gbuffer": gbuf, "rgb": rgb, "mapped": mapped, "path_rgb": path_rgb, "stats": stats}
+
+    def set_normal_codes(self, codes: Optional[np.ndarray]) -> None:
+        """The code table of a ball-normal scene (None: a gradient-normal scene)."""
+        c = np.ascontiguousarray(codes if codes is not None else np.zeros(0), np.uint32)
+        self.o.lib.oracle_renderer_set_normal_codes(self.h, c.ctypes.data if c.size else None, c.size)
 
     def lbuffer(self) -> np.ndarray:
         """Occupied lBuffer slots, (n, 14) u32 rows {row, slot, 12 slot words}."""

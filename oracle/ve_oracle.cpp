@@ -67,6 +67,9 @@ struct Scene {
     const uint32_t* words;
     uint64_t n;
     uint32_t depth;
+    // ball-normal scenes: the 10-10-10 normal codes their leaves index
+    const uint32_t* ncodes = nullptr;
+    uint64_t n_ncodes = 0;
     // texelFetch on a buffer texture: out-of-range reads return 0.
     uint32_t fetch(uint64_t off) const { return off < n ? words[off] : 0u; }
 };
@@ -428,7 +431,22 @@ inline int sext5(uint32_t v) { return (v & 16u) ? int(v) - 32 : int(v); }
 // packNormalAccum (normal.comp:90-95) -> UnpackNormal (internal.glsl:22-28)
 // -> normalize, as shade.comp:267 reads it.  Leaves without a stored normal
 // use the face-normal fallback of lookupNormal (shade.comp:271-274).
-f3 shading_normal(uint32_t leaf_word, f3 ray_dir) {
+// UnpackNormal (internal.glsl:22-28) of a 10-10-10 code, then normalize.
+f3 unpack_normal(uint32_t p) {
+    const f3 u = mk(float((p >> 22) & 0x3FFu) / 511.0f - 1.0f, float((p >> 12) & 0x3FFu) / 511.0f - 1.0f,
+                    float((p >> 2) & 0x3FFu) / 511.0f - 1.0f);
+    return normalize(u);
+}
+
+// index + 1 of a ball-normal leaf's code in the scene's table (0: none)
+inline uint32_t ball_index(uint32_t leaf_word) { return (leaf_word >> 31) ? 0u : (leaf_word >> 8) & 0x7FFFFFu; }
+
+// whether the leaf word carries a stored normal (either mode)
+inline bool has_normal(uint32_t leaf_word) { return (leaf_word >> 31) || ball_index(leaf_word) != 0u; }
+
+f3 shading_normal(const Scene& s, uint32_t leaf_word, f3 ray_dir) {
+    const uint32_t bi = ball_index(leaf_word);
+    if (bi != 0u && bi - 1u < s.n_ncodes) return unpack_normal(s.ncodes[bi - 1u]);
     if (!(leaf_word >> 31)) {
         const f3 a = mk(std::fabs(ray_dir.x), std::fabs(ray_dir.y), std::fabs(ray_dir.z));
         auto sgn = [](float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); };
@@ -880,7 +898,7 @@ void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_
         const uint32_t mi = hit.material < n_mats ? hit.material : 0u;
         const Material& m = mats[mi];
         const f3 albedo = mk(m.color[0], m.color[1], m.color[2]);
-        const f3 N = shading_normal(s.fetch(hit.id), dir);
+        const f3 N = shading_normal(s, s.fetch(hit.id), dir);
         if (m.emissive) {  // shade.comp:576-583
             const float k = m.emissive_intensity;
             f3 e = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
@@ -1133,6 +1151,7 @@ struct Renderer {
     std::unordered_set<uint32_t> em_claimed;
     std::unordered_map<uint32_t, Reservoir> res;
     std::vector<uint32_t> lb;  // lBuffer frames: kLbWidth rows x 32 slots x 12 words
+    std::vector<uint32_t> ncodes;  // ball-normal scenes: the code table their leaf words index
     Avg lookup(bool lbm, uint32_t vid) const { return lbm ? lb_lookup(lb, vid) : lookup_avg(cache, vid); }
 };
 
@@ -1389,6 +1408,95 @@ void oracle_fill_normals(uint32_t* words, uint64_t n, uint32_t depth) {
     oracle_fill_normals_mode(words, n, depth, 0, 1);
 }
 
+// The reference's own normal mode, normal.comp:55-95 (computeRefinedNormal
+// with packNormalAccum): the sum of the offsets d of the EMPTY neighbours
+// with 0 < |d|^2 <= R^2 (R = normalPrecision), out-of-volume neighbours
+// counted as empty, around the voxel's even-aligned corner — the pass reads
+// the position back from the GBuffer's half coordinates times two
+// (normal.comp:147-152, generate_primary.comp:73-77); normalize, or (0,1,0)
+// when the sum vanishes; 10-10-10 code round((c + 1) * 511).  The codes of all
+// leaves, sorted and made unique, form the scene's code table; each leaf's
+// normal field (bits 8-30, bit 31 clear) holds its code's index + 1.
+// Occupancy by tree descents (lookupOccupied, normal.comp:55-70).  Writes
+// the words in place and up to `cap` table codes; returns the table size.
+uint64_t oracle_fill_normals_ball(uint32_t* words, uint64_t n, uint32_t depth, uint32_t radius, uint32_t threads,
+                                  uint32_t* codes_out, uint64_t cap) {
+    std::vector<uint32_t> copy(words, words + n);
+    Scene s{copy.data(), n, depth};
+    const uint32_t L = 1u << depth;
+    struct E { uint32_t off, level, x, y, z; };
+    std::vector<E> leaves;
+    std::vector<E> st;
+    for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t half = L >> 1;
+        st.push_back({1u + i, 1u, (i & 4) ? half : 0u, (i & 2) ? half : 0u, (i & 1) ? half : 0u});
+    }
+    while (!st.empty()) {
+        E e = st.back();
+        st.pop_back();
+        const uint32_t raw = s.fetch(e.off);
+        if (raw & 1u) {
+            if (e.level >= depth) continue;
+            const uint32_t next = node_next(raw);
+            const uint32_t half = L >> (e.level + 1);
+            for (uint32_t i = 0; i < 8; i++)
+                st.push_back({next + i, e.level + 1, e.x + ((i & 4) ? half : 0u), e.y + ((i & 2) ? half : 0u),
+                              e.z + ((i & 1) ? half : 0u)});
+        } else if (node_material(raw) != 0u && e.level == depth) {
+            leaves.push_back(e);
+        }
+    }
+    const int R = int(radius);
+    std::vector<uint32_t> code(leaves.size());
+    auto pack = [](float c) {
+        int v = int(std::round((c + 1.0f) * 511.0f));
+        v = v < 0 ? 0 : (v > 1022 ? 1022 : v);
+        return uint32_t(v);
+    };
+    auto work = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; i++) {
+            const int64_t px = leaves[i].x & ~1u, py = leaves[i].y & ~1u, pz = leaves[i].z & ~1u;
+            int ax = 0, ay = 0, az = 0;
+            for (int dx = -R; dx <= R; dx++)
+                for (int dy = -R; dy <= R; dy++)
+                    for (int dz = -R; dz <= R; dz++) {
+                        if (dx == 0 && dy == 0 && dz == 0) continue;
+                        if (dx * dx + dy * dy + dz * dz > R * R) continue;
+                        if (!lookup_occupied(s, px + dx, py + dy, pz + dz)) {
+                            ax += dx; ay += dy; az += dz;
+                        }
+                    }
+            const f3 acc = mk(float(ax), float(ay), float(az));
+            const float len = std::sqrt(dot(acc, acc));
+            const f3 nv = len > 0.001f ? divs(acc, len) : mk(0.0f, 1.0f, 0.0f);
+            code[i] = (pack(nv.x) << 22) | (pack(nv.y) << 12) | (pack(nv.z) << 2);
+        }
+    };
+    if (threads <= 1) {
+        work(0, leaves.size());
+    } else {
+        std::vector<std::thread> th;
+        for (uint32_t t = 0; t < threads; t++)
+            th.emplace_back(work, leaves.size() * t / threads, leaves.size() * (t + 1) / threads);
+        for (auto& x : th) x.join();
+    }
+    std::vector<uint32_t> table(code);
+    std::sort(table.begin(), table.end());
+    table.erase(std::unique(table.begin(), table.end()), table.end());
+    for (size_t i = 0; i < leaves.size(); i++) {
+        const uint32_t idx = uint32_t(std::lower_bound(table.begin(), table.end(), code[i]) - table.begin());
+        words[leaves[i].off] = (copy[leaves[i].off] & 0xFFu) | ((idx + 1u) << 8);
+    }
+    if (codes_out) std::memcpy(codes_out, table.data(), std::min<uint64_t>(cap, table.size()) * 4);
+    return table.size();
+}
+
+// The code table the next frames' ball-normal leaves index (n = 0: none).
+void oracle_renderer_set_normal_codes(void* rp, const uint32_t* codes, uint64_t n) {
+    Renderer* R = static_cast<Renderer*>(rp);
+    R->ncodes.assign(codes, codes + n);
+}
+
 int oracle_lookup_occupied(const uint32_t* words, uint64_t n, uint32_t depth, int64_t x, int64_t y, int64_t z) {
     Scene s{words, n, depth};
     return lookup_occupied(s, x, y, z) ? 1 : 0;
@@ -1465,7 +1573,8 @@ void oracle_sincos_turn(const float* u, uint64_t n, float* s, float* c) {
 }
 
 void oracle_shading_normal(uint32_t leaf_word, const float dir[3], float out[3]) {
-    f3 v = shading_normal(leaf_word, mk(dir[0], dir[1], dir[2]));
+    const Scene none{nullptr, 0, 0};
+    f3 v = shading_normal(none, leaf_word, mk(dir[0], dir[1], dir[2]));
     out[0] = v.x; out[1] = v.y; out[2] = v.z;
 }
 
@@ -1548,6 +1657,8 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                         float* path_rgb, ov_stats* stats_out) {
     Renderer* R = static_cast<Renderer*>(rp);
     Scene s{words, n_words, depth};
+    s.ncodes = R->ncodes.data();
+    s.n_ncodes = R->ncodes.size();
     const Material* mats = static_cast<const Material*>(materials);
     const uint32_t W = P->width, H = P->height;
     if (row_end == 0 || row_end > H) row_end = H;
@@ -1732,9 +1843,9 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                         if (vid == 0) miss();
                         else {
                             const uint32_t w = s.fetch(node);
-                            if (w >> 31) {
+                            if (has_normal(w)) {
                                 const f3 nd = mk(0, 0, 1);
-                                f3 nn = shading_normal(w, nd);
+                                f3 nn = shading_normal(s, w, nd);
                                 col[0] = nn.x * 0.5 + 0.5; col[1] = nn.y * 0.5 + 0.5; col[2] = nn.z * 0.5 + 0.5;
                             }
                         }

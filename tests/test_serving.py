@@ -119,3 +119,49 @@ def test_admission_waits_for_pool_space(ve, world):
         assert e.value.code == ve.VE_ERR_CAPACITY
     for o in out[1:]:
         assert np.array_equal(o["voxel_id"], out[0]["voxel_id"])
+
+
+def test_step_budget_spreads_large_requests_without_changing_results(ve, world):
+    """A request whose primary tiles are started a few per step (a tiny
+    per-step path budget) gives the results of the whole-request primary pass."""
+    r, scenes, reqs = world
+    sid, cam, fc = reqs[2]  # 96 x 64, 24 tiles
+    outs = []
+    for kw in ({"fifo": True}, {"step_path_budget": 256 * fc.spp}, {"step_path_budget": 3 * 256 * fc.spp}):
+        reset(r, scenes)
+        with ve.Server(r, pixel_capacity=1 << 16, path_capacity=1 << 18, max_requests=8, **kw) as srv:
+            outs.append(srv.wait(srv.submit(sid, cam, fc)))
+            st = srv.stats()
+        if "step_path_budget" in kw and kw["step_path_budget"] == 256 * fc.spp:
+            assert st["steps"] >= 24  # one tile per step
+    for o in outs[1:]:
+        assert np.array_equal(o["voxel_id"], outs[0]["voxel_id"])
+        assert close_rel(o["rgb"], outs[0]["rgb"]).all()
+
+
+@pytest.mark.parametrize("fifo", [False, True])
+def test_small_request_passes_a_large_one_that_does_not_fit(ve, world, fifo):
+    """Pools that hold one large request and a small one: a second large
+    request waits for space; a small request queued behind it is admitted
+    first unless admission is strict first come first served."""
+    r, scenes, reqs = world
+    sid, depth = scenes[1]
+    w = helpers.workloads()
+    eye, d = w.random_pose(np.random.default_rng(4), depth)
+    big_fc = ve.FrameConfig(width=256, height=256, spp=4, bounces=3, primary_controlchecks=200,
+                            bounce_controlchecks=200)
+    big = (sid, ve.camera_ubo(eye, d, 70.0, 1.0), big_fc)
+    small = reqs[1]  # 64 x 48
+    with ve.Server(r, pixel_capacity=256 * 256 + 256 * 128, path_capacity=1 << 22, max_requests=8, fifo=fifo,
+                   max_bypass_ms=60000) as srv:
+        a = srv.submit(*big)
+        b = srv.submit(*big)
+        c = srv.submit(*small)
+        ra, rb, rc = srv.wait(a), srv.wait(b), srv.wait(c)
+    assert rb["admit_s"] >= ra["done_s"] - 1e-3  # b waited for a's pixels
+    if fifo:
+        assert rc["admit_s"] >= rb["admit_s"]
+    else:
+        assert rc["admit_s"] < rb["admit_s"]
+        assert rc["done_s"] < rb["done_s"]
+    assert np.array_equal(ra["voxel_id"], rb["voxel_id"])

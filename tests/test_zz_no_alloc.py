@@ -27,14 +27,19 @@ def upload_path_normals(ve, words, depth):
         return r.download_scene(sid)
 
 
-def noalloc_normals(ve, words, depth):
+def noalloc_normals(ve, words, depth, stream=None):
+    """Runs the entry point on `stream` (a torch.cuda.Stream; None = the
+    legacy default stream) and reads the node array back."""
     import torch
 
     lib = ve.load_library()
     dev = torch.from_numpy(np.ascontiguousarray(words, np.uint32).view(np.int32).copy()).cuda()
     torch.cuda.synchronize()
-    rc = lib.ve_fill_normals_noalloc(ctypes.c_void_p(dev.data_ptr()), words.size, depth, None)
+    handle = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+    rc = lib.ve_fill_normals_noalloc(ctypes.c_void_p(dev.data_ptr()), words.size, depth, handle)
     assert rc == ve.VE_OK, lib.ve_last_error().decode()
+    if stream is not None:
+        stream.synchronize()
     torch.cuda.synchronize()
     return dev.cpu().numpy().view(np.uint32)
 
@@ -54,6 +59,24 @@ def test_noalloc_normals_match_upload_path_twice(ve):
         want = upload_path_normals(ve, words, depth)
         assert np.array_equal(got, want)
         assert (got >> 31).any()
+
+
+def test_noalloc_on_a_stream_and_shallow_scenes(ve):
+    """On a non-default stream, and on depth-1 and depth-2 scenes (no frontier
+    expansion runs for depth 1), still equal to the upload path."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    s = torch.cuda.Stream()
+    for depth, density in ((1, 0.5), (2, 0.4), (6, 0.05)):
+        c = ve.OctreeCPU(depth)
+        c.insert_many(helpers.random_voxels(rng, depth, density))
+        o = ve.Octree(depth)
+        o.set(c)
+        words = o.words()[: max(o.size, 9)]
+        for stream in (s, None):
+            got = noalloc_normals(ve, words, depth, stream)
+            assert np.array_equal(got, upload_path_normals(ve, words, depth)), (depth, stream)
 
 
 def test_noalloc_rejects_scenes_beyond_the_scratch_limit(ve):

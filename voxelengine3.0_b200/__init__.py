@@ -57,6 +57,7 @@ RESTIR_TEMPORAL = 2
 RESTIR_SPATIAL = 4
 RAYCAST_FULL_WALK = 1
 CFG_NO_GRAPHS = 1
+SERVER_FIFO = 1
 
 
 class VeError(RuntimeError):
@@ -125,7 +126,9 @@ class FrameStatsC(ctypes.Structure):
 
 class ServerConfigC(ctypes.Structure):
     _fields_ = [("pixel_capacity", ctypes.c_uint64), ("path_capacity", ctypes.c_uint64),
-                ("max_requests", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
+                ("max_requests", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("step_path_budget", ctypes.c_uint64), ("max_bypass_ms", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class RequestInfoC(ctypes.Structure):
@@ -210,6 +213,7 @@ _SIGNATURES = {
     "ve_scene_set_nrc": ([_P, ctypes.c_int, _P], ctypes.c_int),
     "ve_scene_build": ([_P, _P, _U64, _U32, _U32, _PTR(ctypes.c_int32), _PTR(_U64)], ctypes.c_int),
     "ve_scene_refresh": ([_P, ctypes.c_int32, _P, _U64, _U32], ctypes.c_int),
+    "ve_scene_normal_mode": ([_P, ctypes.c_int32, _U32], ctypes.c_int),
     "ve_nrc_stats": ([_P, _PTR(ctypes.c_float), _PTR(_U64), _PTR(_U64)], ctypes.c_int),
     "ve_server_create": ([_P, _PTR(ServerConfigC), _PTR(_P)], ctypes.c_int),
     "ve_server_submit": ([_P, _PTR(ViewC), _P, _P, _PTR(_U64)], ctypes.c_int),
@@ -618,6 +622,12 @@ class Renderer:
                                           RAYCAST_FULL_WALK if full_walk else 0, _ptr(out)))
         return out
 
+    def set_normal_mode(self, scene_id: int, radius: int) -> None:
+        """radius 0: 3x3x3 occupancy-gradient normals (the default); R >= 1:
+        the reference's normal pass with normalPrecision = R (normal.comp's
+        L2 ball).  Recomputes the scene's leaf normals."""
+        _check(self._lib.ve_scene_normal_mode(self._h, scene_id, radius))
+
     def download_scene(self, scene_id: int) -> np.ndarray:
         n = _U64()
         _check(self._lib.ve_scene_download(self._h, scene_id, None, 0, ctypes.byref(n)))
@@ -789,10 +799,16 @@ class Renderer:
 class Server:
     """Render server with continuous batching over one Renderer's context."""
 
-    def __init__(self, renderer: "Renderer", pixel_capacity: int, path_capacity: int, max_requests: int = 64):
+    def __init__(self, renderer: "Renderer", pixel_capacity: int, path_capacity: int, max_requests: int = 64,
+                 fifo: bool = False, step_path_budget: int = 0, max_bypass_ms: int = 0):
+        """fifo: strict first-come-first-served admission, each request's
+        primary pass in one step.  Otherwise a step starts at most
+        `step_path_budget` paths (0: 2^22) and admission may pass over a
+        request that does not fit for up to `max_bypass_ms` (0: 50 ms)."""
         self._lib = load_library()
         self.renderer = renderer
-        cfg = ServerConfigC(pixel_capacity, path_capacity, max_requests, 0)
+        cfg = ServerConfigC(pixel_capacity, path_capacity, max_requests, SERVER_FIFO if fifo else 0,
+                            step_path_budget, max_bypass_ms, 0)
         h = _P()
         _check(self._lib.ve_server_create(renderer._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -66,6 +66,8 @@ struct DevScene {
     EmLight* em_stage;    // lights found this frame, appended at its end
     ResEntry* res;        // per-voxel ReSTIR reservoirs, 2^kResLog2 entries
     uint32_t* lbuf;       // the dual-channel lBuffer (VE_FRAME_LBUFFER; null until first used)
+    const float4* ntab;   // ball-normal scenes: unit normal per code index (null: 3x3x3 gradient)
+    uint32_t n_ntab;
 };
 
 struct DevMaterial {
@@ -173,6 +175,7 @@ struct FrameArgs {
     float* path_rgb;
     uint32_t refill;       // idle lanes at which a trace warp takes new rays
     uint32_t view_offset;  // index of views[0] in the view table the paths refer to
+    uint32_t tile_offset;  // primary pass: block b covers tile b + tile_offset (serving spreads a request's tiles)
     uint32_t* remaining;   // per view slot: paths not yet deposited (serving), or null
     // learned radiance cache (views with VE_FRAME_LEARNED / _TERMINATE_HASH / _TRAIN)
     nrc::QRec* nq;         // queries: paths ended at their second vertex by the network
@@ -411,7 +414,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
     uint32_t e = 0, D = 0, T0 = 0;
     const uint32_t* nodes = nullptr;
     const uint32_t* top = nullptr;
-    uint64_t n_words = 0;
+    uint32_t n_words = 0;
     Dda s;
     RayCount rc;
     for (;;) {
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                     const DevView& v = a.views[meta.z & 0xFFFFu];
                     const DevScene S = a.scenes[v.scene];
                     nodes = S.nodes;
-                    n_words = S.n_words;
+                    n_words = word_bound(S.n_words);
                     D = S.depth;
                     top = S.top;
                     T0 = S.top_level;
@@ -759,7 +762,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
             const f3 albedo = mk(m.albedo_rough.x, m.albedo_rough.y, m.albedo_rough.z);
             const float roughness = m.albedo_rough.w, metallic = m.params.x, spec = m.params.y;
             const bool emissive = m.params.z != 0.0f;
-            const f3 N = shading_normal(hit.y, dir);
+            const f3 N = shading_normal(hit.y, dir, S.ntab, S.n_ntab);
             if (emissive) {  // shade.comp:576-583
                 const float k = m.params.w;
                 f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
@@ -1018,7 +1021,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
 template <bool COUNT, bool FUSED, int MODE = 0>
 __global__ void __launch_bounds__(256, 4) k_primary(FrameArgs a) {
     __shared__ DepSlot dep[FUSED ? 256 : 1];
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = blockIdx.x + a.tile_offset;
     const uint32_t vi = find_view(a.views, a.n_views, tile);
     const DevView& v = a.views[vi];
     uint32_t px, py;
@@ -1617,8 +1620,8 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
             if (vid == 0u) col = miss();
             else {
                 const uint32_t w = fetch_node(S.nodes, S.n_words, node);
-                if (w >> 31) {
-                    const f3 nn = shading_normal(w, mk(0.0f, 0.0f, 1.0f));
+                if ((w >> 31) || (S.ntab && ball_index(w) != 0u)) {
+                    const f3 nn = shading_normal(w, mk(0.0f, 0.0f, 1.0f), S.ntab, S.n_ntab);
                     col = mk(nn.x * 0.5f + 0.5f, nn.y * 0.5f + 0.5f, nn.z * 0.5f + 0.5f);
                 }
             }
@@ -1770,6 +1773,86 @@ __global__ void __launch_bounds__(256) k_leaf_pass(uint32_t* nodes, uint64_t n_w
     }
 }
 
+// The reference's own normal mode (normal.comp:55-95, computeRefinedNormal +
+// packNormalAccum) for the leaves below each level-(D-1) node of `in`: the
+// offsets d of the empty neighbours with 0 < |d|^2 <= R^2 around the voxel's
+// even-aligned corner (the reference rebuilds the position from the
+// GBuffer's half coordinates times two, normal.comp:147-152 — the corner of
+// the level-(D-1) cell, shared by its 8 leaves), neighbours outside the
+// volume counted as empty; normalize, or (0, 1, 0) when the sum vanishes; the
+// 10-10-10 code is written at each leaf's slot of `codes`.  The sum is
+// integer (exact), so its order does not matter.
+__global__ void __launch_bounds__(256) k_ball_codes(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                                    const unsigned long long* in, const uint32_t* in_cnt,
+                                                    const uint32_t* __restrict__ occ, int R, uint32_t* codes,
+                                                    uint32_t cap) {
+    const uint32_t n = min(*in_cnt, cap);
+    const int L = int(1u << D);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long e = in[i];
+        const uint32_t word = fetch_node(nodes, n_words, uint32_t(e & 0xFFFFFFFull));
+        if (!(word & 1u)) continue;
+        const uint32_t next = word >> 4;
+        uint32_t leaves = 0;  // children that are leaves with a material
+        for (uint32_t c = 0; c < 8u; c++) {
+            if (uint64_t(next) + c >= n_words) break;
+            const uint32_t lw = nodes[next + c];
+            if (!(lw & 1u) && ((lw >> 1) & 0x7Fu) != 0u) leaves |= 1u << c;
+        }
+        if (!leaves) continue;
+        const int x = int((e >> 28) & 2047u), y = int((e >> 39) & 2047u), z = int((e >> 50) & 2047u);
+        int ax = 0, ay = 0, az = 0;
+        for (int dx = -R; dx <= R; dx++)
+            for (int dy = -R; dy <= R; dy++)
+                for (int dz = -R; dz <= R; dz++) {
+                    if ((dx | dy | dz) == 0 || dx * dx + dy * dy + dz * dz > R * R) continue;
+                    const int nx = x + dx, ny = y + dy, nz = z + dz;
+                    bool occd = false;
+                    if (nx >= 0 && ny >= 0 && nz >= 0 && nx < L && ny < L && nz < L) {
+                        const uint64_t bi = occ_index(uint32_t(nx), uint32_t(ny), uint32_t(nz), D);
+                        occd = (__ldg(occ + (bi >> 5)) >> (bi & 31u)) & 1u;
+                    }
+                    if (!occd) { ax += dx; ay += dy; az += dz; }
+                }
+        const f3 acc = mk(float(ax), float(ay), float(az));
+        const float len = sqrtf(dot(acc, acc));
+        const f3 nv = len > 0.001f ? divs(acc, len) : mk(0.0f, 1.0f, 0.0f);
+        const uint32_t code = (pack1022(nv.x) << 22) | (pack1022(nv.y) << 12) | (pack1022(nv.z) << 2);
+        for (uint32_t c = 0; c < 8u; c++)
+            if (leaves & (1u << c)) codes[next + c] = code;
+    }
+}
+
+// UnpackNormal (internal.glsl:22-28) + normalize of every table code.
+__global__ void __launch_bounds__(256) k_ball_table(const uint32_t* __restrict__ code, uint32_t n, float4* ntab) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = code[i];
+        const f3 u = normalize(mk(float((p >> 22) & 0x3FFu) / 511.0f - 1.0f, float((p >> 12) & 0x3FFu) / 511.0f - 1.0f,
+                                  float((p >> 2) & 0x3FFu) / 511.0f - 1.0f));
+        ntab[i] = make_float4(u.x, u.y, u.z, 0.0f);
+    }
+}
+
+// Each leaf's normal field := index + 1 of its code in the sorted table.
+__global__ void __launch_bounds__(256) k_ball_apply(uint32_t* nodes, uint64_t n_words, const uint32_t* __restrict__ codes,
+                                                    const uint32_t* __restrict__ table, uint32_t n) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_words;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t code = codes[i];
+        if (code == 0u) continue;
+        uint32_t lo = 0, hi = n;  // first entry >= code
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (table[mid] < code) lo = mid + 1u; else hi = mid;
+        }
+        nodes[i] = (nodes[i] & 0xFFu) | ((lo + 1u) << 8);
+    }
+}
+
+struct NonZero {
+    __host__ __device__ bool operator()(uint32_t v) const { return v != 0u; }
+};
+
 // ---------------------------------------------------------------------------
 // allocation-free leaf normal pass: its scratch lives in this fixed device
 // array (the frontiers and the occupancy bitmask of a depth <= 7 scene),
@@ -1824,6 +1907,11 @@ struct SceneSlot {
     ve::EmLight* em_stage = nullptr;
     ve::ResEntry* res = nullptr;
     uint32_t* lbuf = nullptr;  // dual-channel lBuffer (first VE_FRAME_LBUFFER frame)
+    // normal mode: 0 = 3x3x3 occupancy gradient in the leaf words; R > 0 = the
+    // reference's L2 ball of radius R, the leaf words indexing `ntab`
+    uint32_t normal_radius = 0;
+    float4* ntab = nullptr;
+    uint32_t n_ntab = 0;
 };
 
 template <typename T>
@@ -1976,7 +2064,7 @@ static int sync_scenes(ve_ctx* c) {
         const SceneSlot& s = c->scenes[i];
         h[i] = DevScene{s.nodes,     s.n_words,   s.cache,    s.depth,    c->cfg.hash_log2, c->cfg.hash_probes,
                         s.top_level, s.top,       s.em_list, s.em_claim, s.em_state,       s.em_stage,
-                        s.res,       s.lbuf};
+                        s.res,       s.lbuf,      s.ntab,    s.n_ntab};
     }
     const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
@@ -2134,10 +2222,81 @@ static int compute_normals(ve_ctx* c, SceneSlot& s) {
     }
     const uint32_t* lc = cnt + (D - 1);
     k_leaf_pass<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, 0, uint32_t(cap));
-    k_leaf_pass<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, 1, uint32_t(cap));
+    if (s.normal_radius == 0u) {
+        k_leaf_pass<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, 1, uint32_t(cap));
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        cleanup();
+        if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("normal pass: ") + cudaGetErrorString(e));
+        if (s.ntab) {  // back from the ball mode
+            cudaFree(s.ntab);
+            s.ntab = nullptr;
+            s.n_ntab = 0;
+            c->scenes_dirty = true;
+        }
+        return VE_OK;
+    }
+    // the reference's ball mode: a code per leaf, then the sorted table of
+    // distinct codes, and every leaf's index into it
+    if (s.n_words > uint64_t(INT32_MAX)) {
+        cleanup();
+        return fail(VE_ERR_CAPACITY, "normal pass (ball): more than 2^31 words");
+    }
+    const int nw = int(s.n_words);
+    uint32_t *codes = nullptr, *sel = nullptr, *table = nullptr, *nsel = nullptr;
+    void* tmp = nullptr;
+    auto cleanup2 = [&]() {
+        cleanup();
+        for (void* p : {(void*)codes, (void*)sel, (void*)table, (void*)nsel, tmp})
+            if (p) cudaFree(p);
+    };
+    size_t b_sel = 0, b_sort = 0, b_uniq = 0;
+    cub::DeviceSelect::If(nullptr, b_sel, codes, sel, nsel, nw, NonZero(), c->stream);
+    cub::DeviceRadixSort::SortKeys(nullptr, b_sort, sel, table, nw, 2, 32, c->stream);
+    cub::DeviceSelect::Unique(nullptr, b_uniq, table, sel, nsel + 1, nw, c->stream);
+    const size_t b_tmp = std::max(b_sel, std::max(b_sort, b_uniq));
+    if (cudaMalloc(&codes, size_t(nw) * 4) != cudaSuccess || cudaMalloc(&sel, size_t(nw) * 4) != cudaSuccess ||
+        cudaMalloc(&table, size_t(nw) * 4) != cudaSuccess || cudaMalloc(&nsel, 2 * 4) != cudaSuccess ||
+        cudaMalloc(&tmp, std::max<size_t>(b_tmp, 16)) != cudaSuccess) {
+        cleanup2();
+        return fail(VE_ERR_NOMEM, "normal pass (ball): device allocation failed");
+    }
+    cudaMemsetAsync(codes, 0, size_t(nw) * 4, c->stream);
+    k_ball_codes<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, D, in, lc, occ, int(s.normal_radius), codes,
+                                              uint32_t(cap));
+    uint32_t h_n[2] = {0, 0};
+    size_t bt = b_tmp;
+    cub::DeviceSelect::If(tmp, bt, codes, sel, nsel, nw, NonZero(), c->stream);
+    cudaMemcpyAsync(&h_n[0], nsel, 4, cudaMemcpyDeviceToHost, c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);
-    cleanup();
-    if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("normal pass: ") + cudaGetErrorString(e));
+    if (e == cudaSuccess && h_n[0] > 0u) {
+        bt = b_tmp;
+        cub::DeviceRadixSort::SortKeys(tmp, bt, sel, table, int(h_n[0]), 2, 32, c->stream);
+        bt = b_tmp;
+        cub::DeviceSelect::Unique(tmp, bt, table, sel, nsel + 1, int(h_n[0]), c->stream);
+        cudaMemcpyAsync(&h_n[1], nsel + 1, 4, cudaMemcpyDeviceToHost, c->stream);
+        e = cudaStreamSynchronize(c->stream);
+    }
+    if (e != cudaSuccess) {
+        cleanup2();
+        return fail(VE_ERR_CUDA, std::string("normal pass (ball): ") + cudaGetErrorString(e));
+    }
+    if (s.ntab) cudaFree(s.ntab);
+    s.ntab = nullptr;
+    s.n_ntab = 0;
+    if (h_n[1] > 0u) {
+        if (cudaMalloc(&s.ntab, size_t(h_n[1]) * sizeof(float4)) != cudaSuccess) {
+            s.ntab = nullptr;
+            cleanup2();
+            return fail(VE_ERR_NOMEM, "normal pass (ball): table allocation failed");
+        }
+        s.n_ntab = h_n[1];
+        k_ball_table<<<grid, 256, 0, c->stream>>>(sel, h_n[1], s.ntab);
+        k_ball_apply<<<grid, 256, 0, c->stream>>>(s.nodes, s.n_words, codes, sel, h_n[1]);
+    }
+    e = cudaStreamSynchronize(c->stream);
+    cleanup2();
+    c->scenes_dirty = true;
+    if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("normal pass (ball): ") + cudaGetErrorString(e));
     return VE_OK;
 }
 
@@ -3096,6 +3255,7 @@ int ve_ctx_destroy(ve_ctx* c) {
         if (s.top) cudaFree(s.top);
         if (s.rank) cudaFree(s.rank);
         if (s.lbuf) cudaFree(s.lbuf);
+        if (s.ntab) cudaFree(s.ntab);
         free_emissive(s);
     }
     c->d_scenes.release(); c->d_mats.release(); c->d_views.release();
@@ -3431,6 +3591,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
     if (s.top) cudaFree(s.top);
     if (s.rank) cudaFree(s.rank);
     if (s.lbuf) cudaFree(s.lbuf);
+    if (s.ntab) cudaFree(s.ntab);
     free_emissive(s);
     s = SceneSlot();
     c->scenes_dirty = true;
@@ -3472,6 +3633,9 @@ int ve_scene_refresh(ve_ctx* c, int32_t id, const uint32_t* xyz, uint64_t n, uin
     if (n && !xyz) return fail(VE_ERR_INVALID, "scene_refresh: null positions");
     if (n > (1ull << 26)) return fail(VE_ERR_CAPACITY, "scene_refresh: at most 2^26 positions per call");
     SceneSlot& s = c->scenes[id];
+    if (s.normal_radius)
+        return fail(VE_ERR_STATE, "scene_refresh: a ball-normal scene recomputes its normals with "
+                                  "ve_scene_apply_edits (without VE_SCENE_KEEP_NORMALS) or ve_scene_normal_mode");
     const uint32_t L = 1u << s.depth;
     for (uint64_t i = 0; i < 3 * n; i++)
         if (xyz[i] >= L) return fail(VE_ERR_INVALID, "scene_refresh: position outside the scene");
@@ -3487,6 +3651,19 @@ int ve_scene_refresh(ve_ctx* c, int32_t id, const uint32_t* xyz, uint64_t n, uin
     cudaFree(d);
     if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("scene_refresh: ") + cudaGetErrorString(e));
     return VE_OK;
+}
+
+int ve_scene_normal_mode(ve_ctx* c, int32_t id, uint32_t radius) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_normal_mode: unknown scene");
+    if (radius > VE_NORMAL_BALL_MAX_RADIUS)
+        return fail(VE_ERR_INVALID, "scene_normal_mode: radius above VE_NORMAL_BALL_MAX_RADIUS");
+    SceneSlot& s = c->scenes[id];
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    s.normal_radius = radius;
+    if (int rc = compute_normals(c, s)) return rc;
+    return sync_scenes(c);
 }
 
 int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t* n_words) {
@@ -3921,10 +4098,34 @@ int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
 }
 
 // Allocation-free variant of the leaf normal pass (see include/ve.h).  The
-// scratch is the file-scope g_noalloc_scratch; its device address is looked up
-// once per device (first call on that device, with that device current).
-static void* g_noalloc_ptr[64] = {};
+// scratch is the file-scope g_noalloc_scratch; its device address belongs to
+// the context that loaded the module, so it is cached per device together
+// with that context and looked up again (cudaGetSymbolAddress, with the
+// device current) on the first call on a device and whenever the current
+// context differs from the cached one (after cudaDeviceReset, or under
+// another context the caller made current).
+struct NoAllocSlot {
+    void* ctx;
+    void* ptr;
+};
+static NoAllocSlot g_noalloc_slot[64] = {};
 static std::mutex g_noalloc_mu;
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// the calling thread's current driver context (null when none is current)
+static void* noalloc_current_ctx() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 int ve_fill_normals_noalloc(uint32_t* words, uint64_t n_words, uint32_t depth, void* stream) {
     if (!words) return fail(VE_ERR_INVALID, "fill_normals_noalloc: null node array");
@@ -3939,15 +4140,19 @@ int ve_fill_normals_noalloc(uint32_t* words, uint64_t n_words, uint32_t depth, v
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
+        NoAllocSlot& slot = g_noalloc_slot[dev];
+        void* ctx = noalloc_current_ctx();
+        if (!slot.ptr || !ctx || ctx != slot.ctx) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess)
                 return fail(VE_ERR_CUDA, std::string("fill_normals_noalloc: cudaGetSymbolAddress: ") +
                                              cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = p;
+            // the lookup makes the device's primary context current when none was
+            slot.ctx = ctx ? ctx : noalloc_current_ctx();
+            slot.ptr = p;
         }
-        base = g_noalloc_ptr[dev];
+        base = slot.ptr;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned char* b = static_cast<unsigned char*>(base);

@@ -84,6 +84,7 @@ struct ServeRequest {
     uint32_t slot = 0;
     uint64_t pix_off = 0, path_off = 0, pixels = 0, paths = 0;
     uint32_t tiles = 0;
+    uint32_t tiles_started = 0;  // tiles whose primary pass has been launched
     double t_submit = 0, t_admit = 0, t_done = 0;
     cudaEvent_t done_ev = nullptr;
 };
@@ -166,16 +167,26 @@ static void serve_loop(ve_server* s) {
                 s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
                 if (s->stop && s->queue.empty() && s->active.empty()) break;
             }
-            // 1. admission: FIFO while the request fits the pools and a slot is free
-            while (!s->queue.empty() && !s->free_slots.empty()) {
-                ServeRequest* r = s->queue.front();
+            // 1. admission in arrival order while a slot is free; a request
+            // that does not fit the pools is passed over unless it has waited
+            // longer than the bypass bound (strict FIFO: never)
+            const bool fifo = (s->cfg.flags & VE_SERVER_FIFO) != 0u;
+            const double bypass_s = 1e-3 * double(s->cfg.max_bypass_ms ? s->cfg.max_bypass_ms : 50u);
+            const double t_now = now_s();
+            for (auto it = s->queue.begin(); it != s->queue.end() && !s->free_slots.empty();) {
+                ServeRequest* r = *it;
                 uint64_t po = 0, qo = 0;
-                if (!s->pix_pool.alloc(r->pixels, &po)) break;
-                if (!s->path_pool.alloc(r->paths, &qo)) {
+                bool fits = s->pix_pool.alloc(r->pixels, &po);
+                if (fits && !s->path_pool.alloc(r->paths, &qo)) {
                     s->pix_pool.release(po, r->pixels);
-                    break;
+                    fits = false;
                 }
-                s->queue.pop_front();
+                if (!fits) {
+                    if (fifo || t_now - r->t_submit > bypass_s) break;
+                    ++it;
+                    continue;
+                }
+                it = s->queue.erase(it);
                 r->pix_off = po;
                 r->path_off = qo;
                 r->slot = s->free_slots.back();
@@ -220,17 +231,34 @@ static void serve_loop(ve_server* s) {
             d.path_base = r->path_off;
             cudaMemcpyAsync(c->d_views.p + r->slot, &d, sizeof(DevView), cudaMemcpyHostToDevice, st);
             cudaMemsetAsync(s->d_remaining + r->slot, 0, 4, st);
-            FrameArgs ap = a;
-            ap.views = c->d_views.p + r->slot;
-            ap.n_views = 1;
-            ap.total_tiles = r->tiles;
-            ap.view_offset = r->slot;
-            // primary paths join the live queue this step's shade pass reads:
-            // queue live[ps & 1], count at CNT_LIVE + ps (k_primary appends to
-            // live[0] / CNT_LIVE + 0 of the arguments it is given)
-            ap.counters = c->counters.p + ps;
-            ap.live[0] = (ps & 1u) ? c->live1.p : c->live0.p;
-            k_primary<false, false, 0><<<r->tiles, 256, 0, st>>>(ap);
+        }
+        // primary passes: requests in admission order start their next tiles
+        // until the step's path budget is spent (FIFO: whole requests)
+        {
+            const bool fifo = (s->cfg.flags & VE_SERVER_FIFO) != 0u;
+            uint64_t budget = s->cfg.step_path_budget ? s->cfg.step_path_budget : (1ull << 22);
+            for (ServeRequest* r : s->active) {
+                if (r->state != 1 || r->tiles_started >= r->tiles) continue;
+                if (!fifo && budget == 0) break;
+                const uint64_t per_tile = 256ull * r->view.frame.spp;
+                const uint32_t left = r->tiles - r->tiles_started;
+                uint32_t n = left;
+                if (!fifo) n = uint32_t(std::min<uint64_t>(left, std::max<uint64_t>(1, budget / per_tile)));
+                FrameArgs ap = a;
+                ap.views = c->d_views.p + r->slot;
+                ap.n_views = 1;
+                ap.total_tiles = r->tiles;
+                ap.view_offset = r->slot;
+                ap.tile_offset = r->tiles_started;
+                // primary paths join the live queue this step's shade pass
+                // reads: queue live[ps & 1], count at CNT_LIVE + ps (k_primary
+                // appends to live[0] / CNT_LIVE + 0 of the arguments it is given)
+                ap.counters = c->counters.p + ps;
+                ap.live[0] = (ps & 1u) ? c->live1.p : c->live0.p;
+                k_primary<false, false, 0><<<n, 256, 0, st>>>(ap);
+                r->tiles_started += n;
+                budget -= std::min<uint64_t>(budget, uint64_t(n) * per_tile);
+            }
         }
         // 2. one shade + one trace pass over every live path
         k_shade<0><<<c->grid_shade, 256, 0, st>>>(a, ps);
@@ -255,7 +283,7 @@ static void serve_loop(ve_server* s) {
             s->steps_run++;
             for (size_t i = 0; i < s->active.size();) {
                 ServeRequest* r = s->active[i];
-                if (r->state == 1 && s->h_remaining[r->slot] == 0) {
+                if (r->state == 1 && r->tiles_started == r->tiles && s->h_remaining[r->slot] == 0) {
                     r->state = 2;
                     finished.push_back(r);
                 }

@@ -295,7 +295,22 @@ __device__ float4 g_normal_table[19 * 19 * 19];
 
 __device__ __forceinline__ f3 shading_normal_compute(uint32_t leaf_word, f3 ray_dir);
 
-__device__ __forceinline__ f3 shading_normal(uint32_t leaf_word, f3 ray_dir) {
+// Index + 1 of a leaf's entry in its scene's ball-normal table (the
+// reference's normal mode): bits 8-30 of a leaf word whose bit 31 is clear;
+// 0 when the leaf has none.
+__device__ __forceinline__ uint32_t ball_index(uint32_t leaf_word) {
+    return (leaf_word >> 31) ? 0u : (leaf_word >> 8) & 0x7FFFFFu;
+}
+
+// `ntab`/`n_ntab`: the scene's ball-normal table (null for a scene in the
+// 3x3x3-gradient mode).
+__device__ __forceinline__ f3 shading_normal(uint32_t leaf_word, f3 ray_dir, const float4* ntab = nullptr,
+                                             uint32_t n_ntab = 0u) {
+    const uint32_t bi = ball_index(leaf_word);
+    if (ntab && bi != 0u && bi - 1u < n_ntab) {
+        const float4 n = __ldg(ntab + (bi - 1u));
+        return mk(n.x, n.y, n.z);
+    }
     if (leaf_word >> 31) {
         const int ix = sext5((leaf_word >> 8) & 31u), iy = sext5((leaf_word >> 13) & 31u),
                   iz = sext5((leaf_word >> 18) & 31u);
