@@ -61,16 +61,15 @@ METRIC = "Mrays/s at 1080p depth-10 octree"
 
 
 def measured_trace_traffic():
-    """DRAM bytes per k_trace launch of this workload from the committed ncu
-    capture summary (profiles/k_trace_traffic_1080p_depth10.md), or None."""
-    p = os.path.join(ROOT, "profiles", "k_trace_traffic_1080p_depth10.md")
+    """DRAM bytes per k_trace launch of this workload, measured by ncu on the
+    960x540 reduced case and scaled to 1080p (profiles/k_trace_traffic.json):
+    (bytes, source) or (None, None)."""
+    p = os.path.join(ROOT, "profiles", "k_trace_traffic.json")
     try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+        d = json.load(open(p))
+        return float(d["dram_bytes_per_launch_1080p"]), d.get("source")
+    except (OSError, KeyError, ValueError):
+        return None, None
 
 
 def peaks():
@@ -1026,6 +1025,7 @@ def main():
     launches = tot["trace_launches"]
     achieved = trace_bytes / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
     peak, peak_kind = peaks()
+    traffic, traffic_src = measured_trace_traffic()
 
     # ---- e2e: public API, host outputs, view upload each step --------------
     # outputs copied on the renderer's copy stream while the next frame
@@ -1077,9 +1077,7 @@ def main():
                     "d2h_bytes_per_step": etot["d2h_bytes"] / K},
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce + shadow DDA)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "peak_kind": peak_kind, "traffic": measured_trace_traffic(),
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                           "profiles/k_trace_traffic_1080p_depth10.md",
+                         "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
                          "algorithmic_bytes_per_launch": trace_bytes / max(launches, 1),
                          "ms_per_launch": trace_ms / max(launches, 1)},
             "gpu_launches": int(tot["kernel_launches"]),
