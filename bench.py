@@ -378,7 +378,8 @@ def run_serving(args, rank, world):
         hr = torch.empty(3 * max_px, dtype=torch.float32, pin_memory=True).numpy()
         bufs.append((hv, hr))
         pool.put(i)
-    cfg = {"pixel_capacity": 8 * max_px, "path_capacity": 1 << 27, "max_requests": 64}
+    cfg = {"pixel_capacity": 8 * max_px, "path_capacity": 1 << 27, "max_requests": 64,
+           "fifo": bool(args.serve_fifo)}
     srv = ve.Server(r, **cfg)
     st0 = srv.stats()
 
@@ -923,6 +924,8 @@ def main():
     ap.add_argument("--capacity-requests", type=int, default=400, help="serving: closed-loop capacity sample")
     ap.add_argument("--serial-requests", type=int, default=400, help="serving: serial plain comparison sample")
     ap.add_argument("--serial-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-fifo", action="store_true",
+                    help="serving: strict first-come-first-served admission, whole primary passes per step")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

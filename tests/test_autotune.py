@@ -45,7 +45,7 @@ def test_autotune_legal_and_result_preserving(ve):
         assert r.launch_config()["trace_blocks_per_sm"] == 1 and r.launch_config()["refill_threshold"] == 4
         forced = _frames(r, views)
         r.set_launch_config(default["trace_blocks_per_sm"], default["shade_blocks_per_sm"],
-                            default["refill_threshold"] or 24)
+                            default["refill_threshold"] or 12)
     for b, a, f, (s, c, fc) in zip(before, after, forced, views):
         hit = np.repeat(b["gbuffer"][..., 3].reshape(-1) != 0, fc.spp)
         assert hit.any()

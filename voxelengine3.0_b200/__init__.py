@@ -755,7 +755,7 @@ class Renderer:
         return {k: getattr(c, k) for k, _ in LaunchConfigC._fields_}
 
     def set_launch_config(self, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
-                          refill_threshold: int = 24) -> None:
+                          refill_threshold: int = 12) -> None:
         c = LaunchConfigC(trace_blocks_per_sm, shade_blocks_per_sm, refill_threshold, 0)
         _check(self._lib.ve_set_launch_config(self._h, ctypes.byref(c)))
 
