@@ -48,7 +48,6 @@ struct Dda {
     f3 o, d, inv, r;
     uint32_t q, cc;
     uint32_t lux, luy, luz, e_last;
-    bool first;
     uint32_t base[17];
 };
 
@@ -65,8 +64,10 @@ __device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlche
     s.q = 0;
     s.cc = controlchecks;
     s.base[0] = 0u;
-    s.lux = s.luy = s.luz = s.e_last = 0;
-    s.first = true;
+    // no position yet: every bit differs from the first step's, which
+    // therefore restarts at level 0
+    s.lux = s.luy = s.luz = 0xFFFFFFFFu;
+    s.e_last = 0;
     if (in_bounds(s.o, Lf)) {
         s.r = s.o;
     } else {
@@ -114,7 +115,7 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
     const uint32_t ux = uint32_t(s.r.x), uy = uint32_t(s.r.y), uz = uint32_t(s.r.z);
     bool reuse = false;
     uint32_t start = 0;
-    if (!s.first) {
+    {
         const uint32_t xd = (ux ^ s.lux) | (uy ^ s.luy) | (uz ^ s.luz);
         if (xd == 0u) {
             reuse = true;
@@ -126,7 +127,6 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
     }
     uint32_t k = s.e_last;
     if (!reuse) {
-        s.first = false;
         s.lux = ux; s.luy = uy; s.luz = uz;
         bool found = false;
         uint32_t off = 0;

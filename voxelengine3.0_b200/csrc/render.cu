@@ -748,7 +748,9 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
     const uint32_t flags = meta.z >> 24;
     uint32_t nf = flags & F_TRAIN;
     uint32_t train_slot = 0xFFFFFFFFu;
-    const DevView& v = a.views[vi];
+    // vi indexes the whole view table; `a.views` starts view_offset entries
+    // into it when the caller passed one view (the serving primary pass)
+    const DevView& v = a.views[vi - a.view_offset];
     if (flags & F_TERM) {
         o.do_dep = true;
     } else {

@@ -2,11 +2,13 @@
 // translation unit: it drives the same kernels).
 //
 // A worker thread owns the context's stream.  Each iteration it
-//   1. admits queued requests, first come first served, while their
-//      framebuffer and path-state ranges fit the pooled device memory (the
-//      HBM budget set at creation) and a view slot is free; each admitted
-//      request writes its view into the device view table and runs its
-//      primary pass, which appends its paths to the shared live-path queue;
+//   1. admits queued requests while their framebuffer and path-state
+//      ranges fit the pooled device memory (the HBM budget set at creation)
+//      and a view slot is free (a request that does not fit is passed over
+//      for a bounded time); each admitted request writes its view into the
+//      device view table; primary passes (with each new path's first
+//      shading step) start up to a per-step path budget of tiles and append
+//      the paths to the shared live-path queue;
 //   2. runs one shade pass and one trace pass over every live path — paths of
 //      all admitted requests at whatever bounce they are — so a request that
 //      arrives while others are on the GPU joins at the next pass;
@@ -250,12 +252,15 @@ static void serve_loop(ve_server* s) {
                 ap.total_tiles = r->tiles;
                 ap.view_offset = r->slot;
                 ap.tile_offset = r->tiles_started;
-                // primary paths join the live queue this step's shade pass
-                // reads: queue live[ps & 1], count at CNT_LIVE + ps (k_primary
-                // appends to live[0] / CNT_LIVE + 0 of the arguments it is given)
+                // the primary pass takes each new path's first shading step
+                // (as a plain frame's does): survivors join the queue this
+                // step's shade pass writes (live[(ps + 1) & 1], count at
+                // CNT_LIVE + ps + 1) and their rays this step's trace pass
+                // (CNT_RAY + ps); k_primary appends relative to the counters
+                // it is given
                 ap.counters = c->counters.p + ps;
-                ap.live[0] = (ps & 1u) ? c->live1.p : c->live0.p;
-                k_primary<false, false, 0><<<n, 256, 0, st>>>(ap);
+                ap.live[1] = ((ps + 1u) & 1u) ? c->live1.p : c->live0.p;
+                k_primary<false, true, 0><<<n, 256, 0, st>>>(ap);
                 r->tiles_started += n;
                 budget -= std::min<uint64_t>(budget, uint64_t(n) * per_tile);
             }
