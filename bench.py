@@ -379,7 +379,7 @@ def run_serving(args, rank, world):
         bufs.append((hv, hr))
         pool.put(i)
     cfg = {"pixel_capacity": 8 * max_px, "path_capacity": 1 << 27, "max_requests": 64,
-           "fifo": bool(args.serve_fifo)}
+           "fifo": bool(args.serve_fifo), "step_path_budget": int(args.serve_budget)}
     srv = ve.Server(r, **cfg)
     st0 = srv.stats()
 
@@ -459,6 +459,18 @@ def run_serving(args, rank, world):
         n_serial += 1
     serial_wall = time.monotonic() - t0
     serial_rays = rays_of(r.total_stats())
+    # slowdown: a request's served latency over its latency rendered alone
+    # (the serial pass above renders jobs[0..n_serial) one at a time)
+    sd = [(info["done_s"] - t_arr) / serial_lat[j] for (j, t_arr, info) in done if j < n_serial]
+    slowdown = {"requests": len(sd), "p50": _pct(sd, 50), "p90": _pct(sd, 90), "p99": _pct(sd, 99)} if sd else None
+    # latency by request size (paths = pixels x spp)
+    by_size = {}
+    for name, lo, hi in (("small (< 2^18 paths)", 0, 1 << 18), ("medium", 1 << 18, 1 << 23),
+                         ("large (>= 2^23 paths)", 1 << 23, 1 << 62)):
+        ls = [info["done_s"] - t_arr for (j, t_arr, info) in done
+              if lo <= jobs[j][2].width * jobs[j][2].height * jobs[j][2].spp < hi]
+        if ls:
+            by_size[name] = {"requests": len(ls), "p50": 1e3 * _pct(ls, 50), "p99": 1e3 * _pct(ls, 99)}
     r.close()
     mrays = rays / wall / 1e6
     line = {"metric": "served p50/p99 latency (Poisson at 80% of capacity) and Mrays/s",
@@ -481,6 +493,8 @@ def run_serving(args, rank, world):
                              "requests_per_s": n_serial / serial_wall,
                              "latency_ms_p50": 1e3 * _pct(serial_lat, 50),
                              "latency_ms_p99": 1e3 * _pct(serial_lat, 99)},
+            "slowdown": slowdown,
+            "latency_ms_by_size": by_size,
             "clocks": clk.summary()}
     lines = [None] * world
     if world > 1:
@@ -924,6 +938,8 @@ def main():
     ap.add_argument("--capacity-requests", type=int, default=400, help="serving: closed-loop capacity sample")
     ap.add_argument("--serial-requests", type=int, default=400, help="serving: serial plain comparison sample")
     ap.add_argument("--serial-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-budget", type=int, default=0,
+                    help="serving: primary paths a step may start (0: the server's default, 2^23)")
     ap.add_argument("--serve-fifo", action="store_true",
                     help="serving: strict first-come-first-served admission, whole primary passes per step")
     args = ap.parse_args()

@@ -406,7 +406,7 @@ typedef struct ve_server_config {
     uint64_t path_capacity;    /* pooled path states, 144 B each */
     uint32_t max_requests;     /* view slots (requests on the GPU at once) */
     uint32_t flags;            /* VE_SERVER_FIFO */
-    uint64_t step_path_budget; /* paths whose primary pass one step may start (0: 2^22) */
+    uint64_t step_path_budget; /* paths whose primary pass one step may start (0: 2^23) */
     uint32_t max_bypass_ms;    /* how long a request that does not fit may be passed over (0: 50 ms) */
     uint32_t reserved;
 } ve_server_config;

@@ -803,7 +803,7 @@ class Server:
                  fifo: bool = False, step_path_budget: int = 0, max_bypass_ms: int = 0):
         """fifo: strict first-come-first-served admission, each request's
         primary pass in one step.  Otherwise a step starts at most
-        `step_path_budget` paths (0: 2^22) and admission may pass over a
+        `step_path_budget` paths (0: 2^23) and admission may pass over a
         request that does not fit for up to `max_bypass_ms` (0: 50 ms)."""
         self._lib = load_library()
         self.renderer = renderer

@@ -130,7 +130,13 @@ enum : uint32_t {
     ST_RES_WRITES,   // emissive frames: reservoirs committed
     ST_TOTAL = 19
 };
-enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u };
+// path flags (meta.z bits 24-31); F_DZERO / F_IZERO: the path's direct /
+// indirect radiance is +0 in every channel and its p_direct / p_indirect slot
+// was not written (loads of the slot are discarded)
+enum : uint32_t { F_PENDING = 1u, F_TERM = 2u, F_TRAIN = 4u, F_DZERO = 8u, F_IZERO = 16u };
+__device__ __forceinline__ bool pos_zero(f3 v) {
+    return (__float_as_uint(v.x) | __float_as_uint(v.y) | __float_as_uint(v.z)) == 0u;
+}
 // Shading-kernel instances: emissive NEE (VE_FRAME_EMISSIVE) and the
 // dual-channel lBuffer AccumPass (VE_FRAME_LBUFFER) compile into their own
 // instances so the plain kernels keep their registers.
@@ -738,9 +744,12 @@ __device__ __forceinline__ void emissive_nee(const FrameArgs& a, const DevView& 
 // F_TERM), tp/direct/indirect the path state after any pending sun term was
 // resolved.  Writes the continuing path's state; the queue appends and the
 // AccumPass deposit are left to shade_emit.
+// `direct_stored`: `direct` equals the path's p_direct slot (the store is
+// skipped while it stays so).
 template <int MODE>
 __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4 meta, f3 tp, f3 direct,
-                                           f3 indirect, f3 dir, uint4 hit, ShadeOut& o) {
+                                           f3 indirect, f3 dir, uint4 hit, ShadeOut& o,
+                                           bool direct_stored = false) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     constexpr bool LB = (MODE & kModeLb) != 0;
     const uint32_t vi = meta.z & 0xFFFFu;
@@ -769,7 +778,12 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                 const float k = m.params.w;
                 f3 em = mul(mk(albedo.x * k, albedo.y * k, albedo.z * k), tp);
                 em = mk(gmin(em.x, 20.0f), gmin(em.y, 20.0f), gmin(em.z, 20.0f));
-                if (b == 0u) direct = add(direct, em); else indirect = add(indirect, em);
+                if (b == 0u) {
+                    direct = add(direct, em);
+                    direct_stored = false;
+                } else {
+                    indirect = add(indirect, em);
+                }
                 // a light seen by a primary ray joins the registry at the end
                 // of the frame (shade.comp:585-613)
                 if (EM && (v.flags & VE_FRAME_EMISSIVE) && b == 0u) {
@@ -919,8 +933,12 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                 a.p_ray_o[p] = st3(sp);
                 a.p_ray_d[p] = st3(dir);
                 a.p_tp[p] = st3(tp);
-                a.p_direct[p] = st3(direct);
-                a.p_indirect[p] = st3(indirect);
+                // radiance that is +0 is flagged instead of stored; direct
+                // radiance already in its slot is not stored again
+                if (pos_zero(direct)) nf |= F_DZERO;
+                else if (!direct_stored) a.p_direct[p] = st3(direct);
+                if (pos_zero(indirect)) nf |= F_IZERO;
+                else a.p_indirect[p] = st3(indirect);
                 meta.y = rng;
                 meta.z = vi | (b << 16) | (nf << 24);
                 a.p_meta[p] = meta;
@@ -1105,10 +1123,8 @@ __global__ void __launch_bounds__(256, 4) k_primary(FrameArgs a) {
             const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
             a.p_ray_d[p] = st3(dir);
             a.p_tp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            a.p_direct[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            a.p_indirect[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             a.p_hit[p] = make_uint4(kHit, word, h.x | (h.y << 16), h.z | (h.material << 16));
-            a.p_meta[p] = make_uint4(vid, rng, vi + a.view_offset, pix);
+            a.p_meta[p] = make_uint4(vid, rng, (vi + a.view_offset) | ((F_DZERO | F_IZERO) << 24), pix);
             a.live[0][q + s] = uint32_t(p);
         }
     }
@@ -1152,17 +1168,25 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
             const float4 pe = a.p_pend[p];  // read with the rest: no load waits on the flags
             const uint32_t want = EM ? __float_as_uint(a.p_sdir[p].w) : 0xFFFFFFFFu;
             const uint32_t flags = meta.z >> 24;
-            f3 direct = ld3(a.p_direct[p]);
-            f3 indirect = ld3(a.p_indirect[p]);
+            // issued with the rest and discarded when flagged: no load waits on the flags
+            const float4 d4 = a.p_direct[p], i4 = a.p_indirect[p];
+            f3 direct = (flags & F_DZERO) ? mk(0.0f, 0.0f, 0.0f) : ld3(d4);
+            f3 indirect = (flags & F_IZERO) ? mk(0.0f, 0.0f, 0.0f) : ld3(i4);
+            bool direct_stored = !(flags & F_DZERO);
             if ((flags & F_PENDING) && __float_as_uint(pe.w) == want) {
                 // the sun term belongs to the bounce that cast the shadow ray:
                 // the stored one when the path ended there, else the one before
                 const uint32_t b = (meta.z >> 16) & 0xFFu;
-                if (((flags & F_TERM) ? b : b - 1u) == 0u) direct = add(direct, ld3(pe));
-                else indirect = add(indirect, ld3(pe));
+                if (((flags & F_TERM) ? b : b - 1u) == 0u) {
+                    direct = add(direct, ld3(pe));
+                    direct_stored = false;
+                } else {
+                    indirect = add(indirect, ld3(pe));
+                }
             }
             const uint4 hit = (flags & F_TERM) ? make_uint4(0u, 0u, 0u, 0u) : a.p_hit[p];
-            shade_step<MODE>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o);
+            shade_step<MODE>(a, p, meta, ld3(a.p_tp[p]), direct, indirect, ld3(a.p_ray_d[p]), hit, o,
+                             direct_stored);
         }
         shade_emit<MODE>(a, p, o, live_out, live_cnt, ray_cnt, dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
     }

@@ -238,7 +238,7 @@ static void serve_loop(ve_server* s) {
         // until the step's path budget is spent (FIFO: whole requests)
         {
             const bool fifo = (s->cfg.flags & VE_SERVER_FIFO) != 0u;
-            uint64_t budget = s->cfg.step_path_budget ? s->cfg.step_path_budget : (1ull << 22);
+            uint64_t budget = s->cfg.step_path_budget ? s->cfg.step_path_budget : (1ull << 23);
             for (ServeRequest* r : s->active) {
                 if (r->state != 1 || r->tiles_started >= r->tiles) continue;
                 if (!fifo && budget == 0) break;
