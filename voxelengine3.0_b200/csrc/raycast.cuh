@@ -45,7 +45,8 @@ __device__ __forceinline__ uint32_t word_bound(uint64_t n) { return n < 0xFFFFFF
 // `while (inBounds(r_pos) && q++ <= controlchecks)`.  Both return true when
 // the ray is finished, with the result in `h`.
 struct Dda {
-    f3 o, d, inv, r;
+    f3 o, d, inv;
+    float t;  // the position is d * t + o (recomputed each step: the same operations as storing it)
     uint32_t q, cc;
     uint32_t lux, luy, luz, e_last;
     uint32_t base[17];
@@ -69,7 +70,7 @@ __device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlche
     s.lux = s.luy = s.luz = 0xFFFFFFFFu;
     s.e_last = 0;
     if (in_bounds(s.o, Lf)) {
-        s.r = s.o;
+        s.t = 0.0f;
     } else {
         const f3 t1 = mul(mk((0.0f - s.o.x) + 0.001f, (0.0f - s.o.y) + 0.001f, (0.0f - s.o.z) + 0.001f), s.inv);
         const f3 t2 = mul(mk((Lf - s.o.x) - 0.001f, (Lf - s.o.y) - 0.001f, (Lf - s.o.z) - 0.001f), s.inv);
@@ -80,7 +81,7 @@ __device__ __forceinline__ bool dda_init(Dda& s, f3 o, f3 d, uint32_t controlche
             h.checks = s.q;
             return true;
         }
-        s.r = add(muls(d, t_enter), s.o);
+        s.t = t_enter;
     }
     return false;
 }
@@ -101,7 +102,8 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
                                          const uint32_t* __restrict__ top, uint32_t T0, Hit& h, RayCount& rc) {
     const uint32_t L = 1u << D;
     const float Lf = float(L);
-    if (!in_bounds(s.r, Lf)) {
+    const f3 r = add(muls(s.d, s.t), s.o);
+    if (!in_bounds(r, Lf)) {
         h.status = kEscaped;
         h.checks = s.q;
         return true;
@@ -112,7 +114,7 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
         return true;
     }
     if (COUNT) rc.steps++;
-    const uint32_t ux = uint32_t(s.r.x), uy = uint32_t(s.r.y), uz = uint32_t(s.r.z);
+    const uint32_t ux = uint32_t(r.x), uy = uint32_t(r.y), uz = uint32_t(r.z);
     bool reuse = false;
     uint32_t start = 0;
     {
@@ -131,6 +133,8 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
         bool found = false;
         uint32_t off = 0;
         k = start;
+        // child index at level k: bit D-k of x, y, z as bits 2, 1, 0
+        const uint32_t sx = ux << 2, sy = uy << 1;
         // inBounds admits a coordinate equal to 2^D; level 0 then selects
         // another root child than the table's, so such a position walks
         // every level as the reference's descent does
@@ -145,7 +149,8 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
             }
         }
         for (; !found && k < D; k++) {
-            off = s.base[k] + locate(ux, uy, uz, L >> k);
+            const uint32_t b = D - k;  // the position bit level k tests
+            off = s.base[k] + (((sx >> b) & 4u) | ((sy >> b) & 2u) | ((uz >> b) & 1u));
             const uint32_t raw = fetch_node(nodes, n_words, off);
             if (COUNT) rc.fetch++;
             if (!(raw & 1u)) {
@@ -156,7 +161,7 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
         }
         s.e_last = k;
         if (!found) {
-            off = s.base[D] + locate(ux, uy, uz, 1u);
+            off = s.base[D] + ((sx & 4u) | (sy & 2u) | (uz & 1u));
             const uint32_t raw = fetch_node(nodes, n_words, off);
             if (COUNT) rc.fetch++;
             const uint32_t mat = (raw & 254u) >> 1;
@@ -184,7 +189,7 @@ __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ no
     const float ty = ((float(py + (ay ? size : 0u)) - s.o.y) + (ay ? 0.001f : -0.001f)) * s.inv.y;
     const float tz = ((float(pz + (az ? size : 0u)) - s.o.z) + (az ? 0.001f : -0.001f)) * s.inv.z;
     const float t_exit = gmin(gmin(tx, ty), tz);
-    s.r = add(muls(s.d, t_exit), s.o);
+    s.t = t_exit;
     return false;
 }
 
