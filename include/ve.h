@@ -398,7 +398,9 @@ int ve_reset_total_stats(ve_ctx* ctx);
  * several steps, so no step grows long enough to hold up the small requests
  * in flight.  VE_SERVER_FIFO restores strict first-come-first-served
  * admission with each request's whole primary pass in one step.  The server
- * owns the context's stream while it exists. */
+ * owns the context's stream while it exists.  Requests render the plain
+ * method: the PATH_RGB, SCHEDULED, EMISSIVE, LBUFFER, SPLIT, LEARNED, TRAIN
+ * and TERMINATE_HASH frame flags are ignored. */
 #define VE_SERVER_FIFO 1u
 typedef struct ve_server ve_server;
 typedef struct ve_server_config {

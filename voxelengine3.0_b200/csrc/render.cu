@@ -140,7 +140,10 @@ __device__ __forceinline__ bool pos_zero(f3 v) {
 // Shading-kernel instances: emissive NEE (VE_FRAME_EMISSIVE) and the
 // dual-channel lBuffer AccumPass (VE_FRAME_LBUFFER) compile into their own
 // instances so the plain kernels keep their registers.
-constexpr int kModeEm = 1, kModeLb = 2;
+// kModeNrc: the batch ends paths at their second vertex (VE_FRAME_LEARNED /
+// _TERMINATE_HASH / _TRAIN); only the shade pass needs that instance, since
+// the primary and scheduled-emit passes shade vertex 0 only.
+constexpr int kModeEm = 1, kModeLb = 2, kModeNrc = 4;
 // a cached voxel average ends a path (VE_FRAME_TERMINATE_HASH, and the
 // learned cache's fallback) only when at least this many deposits made it
 constexpr uint32_t kHashTermMinCount = 8;
@@ -752,6 +755,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                                            bool direct_stored = false) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     constexpr bool LB = (MODE & kModeLb) != 0;
+    constexpr bool NRC = (MODE & kModeNrc) != 0;
     const uint32_t vi = meta.z & 0xFFFFu;
     uint32_t b = (meta.z >> 16) & 0xFFu;
     const uint32_t flags = meta.z >> 24;
@@ -802,7 +806,8 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
             // second path vertex: a training path is recorded here, other
             // paths may end with a cached radiance estimate
             bool ended = false;
-            if (b == 1u && !emissive && (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN))) {
+            if (NRC && b == 1u && !emissive &&
+                (v.flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN))) {
                 const uint32_t hx = hit.z & 0xFFFFu, hy = hit.z >> 16, hz = hit.w & 0xFFFFu;
                 const uint32_t cell = hash32((hx >> 3) | ((hy >> 3) << 10) | ((hz >> 3) << 20));
                 if ((v.flags & VE_FRAME_TRAIN) && a.ns &&
@@ -953,7 +958,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
             deposit_value(direct, mk(0.0f, 0.0f, 0.0f), o.dr, o.dg, o.db, z);
             deposit_value(mk(0.0f, 0.0f, 0.0f), indirect, o.ir, o.ig, o.ib, z);
         }
-        if ((flags | nf) & F_TRAIN) {  // training path: its target
+        if (NRC && ((flags | nf) & F_TRAIN)) {  // training path: its target
             const uint32_t k = (nf & F_TRAIN) && !(flags & F_TRAIN) ? train_slot : a.p_aux[p];
             if (k < a.ns_cap) {
                 nrc::TRec* t = a.nt + k;
@@ -980,6 +985,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
                                            EmitCounts& cnt) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     constexpr bool LB = (MODE & kModeLb) != 0;
+    constexpr bool NRC = (MODE & kModeNrc) != 0;
     const uint3 s = block_append3(o.app_live, o.app_ext, o.app_sh, live_cnt, ray_cnt,
                                   ray_cnt + (CNT_RAYSH - CNT_RAY), q);
     if (o.app_live) live_out[s.x] = p;
@@ -987,7 +993,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
     if (o.app_sh) a.rayq_sh[s.z] = p | 0x80000000u;
     cnt.ext += o.app_ext ? 1u : 0u;
     cnt.sh += o.app_sh ? 1u : 0u;
-    if (a.nq || a.ns) {
+    if (NRC && (a.nq || a.ns)) {
         // learned cache: query records move from the path's ray slots into
         // the query queue (capacity = paths, never full)
         const uint32_t kq = warp_append(o.want_q, &a.counters[CNT_NRC_Q]);
@@ -1001,7 +1007,7 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
         warp_add_stat(&a.stats[ST_NRC_QUERIES], o.want_q ? 1u : 0u);
         warp_add_stat(&a.stats[ST_NRC_SAMPLES], o.sampled ? 1u : 0u);
     }
-    warp_add_stat(&a.stats[ST_NRC_HASH], o.hash_term ? 1u : 0u);
+    if (NRC) warp_add_stat(&a.stats[ST_NRC_HASH], o.hash_term ? 1u : 0u);
     if (EM) {
         const uint32_t kr = warp_append(o.app_res, &a.counters[CNT_RES]);
         if (o.app_res) a.res_list[kr] = p;
@@ -1507,10 +1513,11 @@ __global__ void __launch_bounds__(256) k_iota(uint32_t* v, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
-// Launches of the shading kernels' instances for a mode (kModeEm | kModeLb).
+// Launches of the shading kernels' instances for a mode (kModeEm | kModeLb,
+// or kModeNrc alone: the API refuses cache-terminated paths with the others).
 template <bool COUNT>
 static void launch_primary(int mode, uint32_t grid, cudaStream_t st, const FrameArgs& a) {
-    switch (mode) {
+    switch (mode & ~kModeNrc) {
         case 0: k_primary<COUNT, true, 0><<<grid, 256, 0, st>>>(a); break;
         case kModeEm: k_primary<COUNT, true, kModeEm><<<grid, 256, 0, st>>>(a); break;
         case kModeLb: k_primary<COUNT, true, kModeLb><<<grid, 256, 0, st>>>(a); break;
@@ -1522,11 +1529,12 @@ static void launch_shade(int mode, uint32_t grid, cudaStream_t st, const FrameAr
         case 0: k_shade<0><<<grid, 256, 0, st>>>(a, pass); break;
         case kModeEm: k_shade<kModeEm><<<grid, 256, 0, st>>>(a, pass); break;
         case kModeLb: k_shade<kModeLb><<<grid, 256, 0, st>>>(a, pass); break;
+        case kModeNrc: k_shade<kModeNrc><<<grid, 256, 0, st>>>(a, pass); break;
         default: k_shade<kModeEm | kModeLb><<<grid, 256, 0, st>>>(a, pass); break;
     }
 }
 static void launch_sched_emit(int mode, uint32_t grid, cudaStream_t st, const FrameArgs& a) {
-    switch (mode) {
+    switch (mode & ~kModeNrc) {
         case 0: k_sched_emit<0><<<grid, 256, 0, st>>>(a); break;
         case kModeEm: k_sched_emit<kModeEm><<<grid, 256, 0, st>>>(a); break;
         case kModeLb: k_sched_emit<kModeLb><<<grid, 256, 0, st>>>(a); break;
@@ -2851,7 +2859,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     }
     const bool em = (flags & VE_FRAME_EMISSIVE) != 0;
     const bool lbm = (flags & VE_FRAME_LBUFFER) != 0;
-    const int mode = (em ? kModeEm : 0) | (lbm ? kModeLb : 0);
+    const bool nrcm = (flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN)) != 0;
+    const int mode = (em ? kModeEm : 0) | (lbm ? kModeLb : 0) | (nrcm ? kModeNrc : 0);
     // the frame's kernel sequence (no host synchronisation inside)
     auto enqueue = [&]() {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);

@@ -220,8 +220,9 @@ static void serve_loop(ve_server* s) {
             d.W = f.width; d.H = f.height; d.spp = f.spp;
             d.bounces = f.bounces; d.cc_primary = f.primary_controlchecks; d.cc_bounce = f.bounce_controlchecks;
             d.recon_radius = f.reconstruction_radius; d.render_type = f.render_type; d.frame_index = f.frame_index;
+            // served requests render the plain method
             d.flags = f.flags & ~(VE_FRAME_PATH_RGB | VE_FRAME_SCHEDULED | VE_FRAME_EMISSIVE | VE_FRAME_LBUFFER |
-                                  VE_FRAME_SPLIT);
+                                  VE_FRAME_SPLIT | VE_FRAME_LEARNED | VE_FRAME_TRAIN | VE_FRAME_TERMINATE_HASH);
             set_rows(d, f, false);
             d.tiles_x = (f.width + 15) / 16;
             for (int k = 0; k < 3; k++) { d.sun[k] = f.sun_dir[k]; d.sky[k] = f.sky[k]; }
