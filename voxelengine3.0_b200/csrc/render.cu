@@ -1147,13 +1147,15 @@ __global__ void __launch_bounds__(256, 4) k_primary(FrameArgs a) {
     }
 }
 
-// 4 CTAs/SM, as k_primary (latency-bound on the path-state loads: 0.50 ->
-// 0.45 ms per 1080p depth-10 frame).  Every instance, and k_sched_emit, which
-// runs on the same grid, shares this bound: the shade grid is sized from the
-// plain instance's occupancy, and an instance with fewer resident CTAs per SM
-// would run part of that grid as a second wave.
+// Latency-bound on the path-state loads: more resident warps win as long as
+// the spills stay small.  The plain instance runs 5 CTAs/SM (48 registers,
+// 0.414 -> 0.397 ms per 1080p depth-10 frame against 4); the emissive,
+// lBuffer and learned instances keep 4 (at 5 they would spill 190-340 B).
+// Each instance's grid is sized from its own occupancy (shade_grid), so none
+// runs part of its grid as a second wave.
+constexpr int shade_ctas(int mode) { return mode == 0 ? 5 : 4; }
 template <int MODE = 0>
-__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a, uint32_t pass) {
+__global__ void __launch_bounds__(256, shade_ctas(MODE)) k_shade(FrameArgs a, uint32_t pass) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     __shared__ DepSlot dep[256];
     const uint32_t n = a.counters[CNT_LIVE + pass];
@@ -2044,6 +2046,8 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> ray_out;  // ve_raycast_batch: 8 words per ray
     int grid_trace = 0, grid_trace_count = 0, grid_shade = 0;
     int occ_trace = 1, occ_trace_count = 1, occ_shade = 1;  // occupancy maxima (blocks/SM)
+    int occ_shade_mode[8] = {1, 1, 1, 1, 1, 1, 1, 1};       // ... per shading instance (kModeEm | kModeLb | kModeNrc)
+    int occ_emit_mode[4] = {1, 1, 1, 1};                    // ... per scheduled-emit instance
     ve_launch_config launch{0, 0, ve::kDefaultRefill, 0};
     // per-frame CUDA-event sets in a ring: elapsed times are read when the
     // slot is reused or the stats are queried, so timed frames never wait
@@ -2499,6 +2503,14 @@ static void apply_launch(ve_ctx* c) {
     if (c->launch.refill_threshold == 0 || c->launch.refill_threshold > 32) c->launch.refill_threshold = kDefaultRefill;
 }
 
+// Grid of a shading instance: the configured blocks per SM, capped at what
+// that instance keeps resident (so the grid is one wave).
+static uint32_t shade_grid(const ve_ctx* c, int mode, bool emit) {
+    const int occ = emit ? c->occ_emit_mode[mode & 3] : c->occ_shade_mode[mode & 7];
+    const int want = int(c->launch.shade_blocks_per_sm);
+    return uint32_t(c->num_sms * ((want == 0 || want > occ) ? occ : want));
+}
+
 // Row ranges of a view: a split frame's band and, for its primary rays, the
 // band widened by the rows the AvgPass reads around a pixel (the
 // reconstruction radius, and 1 for the 4-neighbour filter).
@@ -2894,13 +2906,13 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, b, a.sched_n, a.sched_off, int(pixels), st);
             k_sched_list<<<g, 256, 0, st>>>(a);
             k_sched_threshold<<<1, 1, 0, st>>>(a.rank, a.views);
-            launch_sched_emit(mode, c->grid_shade, st, a);
+            launch_sched_emit(mode, shade_grid(c, mode & ~kModeNrc, true), st, a);
             launches += 6;
         }
         rec();
         for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
             if (pass > 0) {  // pass 0 runs inside the fused primary
-                launch_shade(mode, c->grid_shade, st, a, pass);
+                launch_shade(mode, shade_grid(c, mode, false), st, a, pass);
                 launches++;
             }
             rec();
@@ -3255,10 +3267,26 @@ int ve_ctx_create(const ve_renderer_config* cfg, ve_ctx** out) {
     int bt = 0, btc = 0, bs = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k_trace<false>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&btc, k_trace<true>, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bs, k_shade<0>, 256, 0);
     x->occ_trace = std::max(bt, 1);
     x->occ_trace_count = std::max(btc, 1);
     x->occ_shade = std::max(bs, 1);
+    {
+        int o[8] = {0};
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], k_shade<0>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[kModeEm], k_shade<kModeEm>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[kModeLb], k_shade<kModeLb>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[kModeEm | kModeLb], k_shade<kModeEm | kModeLb>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[kModeNrc], k_shade<kModeNrc>, 256, 0);
+        for (int m = 0; m < 8; m++) x->occ_shade_mode[m] = std::max(o[m], 1);
+        int e[4] = {0};
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e[0], k_sched_emit<0>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e[kModeEm], k_sched_emit<kModeEm>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e[kModeLb], k_sched_emit<kModeLb>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e[kModeEm | kModeLb], k_sched_emit<kModeEm | kModeLb>, 256,
+                                                      0);
+        for (int m = 0; m < 4; m++) x->occ_emit_mode[m] = std::max(e[m], 1);
+    }
     apply_launch(x);
     int rc = 0;
     for (auto& e : x->staging_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
