@@ -294,6 +294,15 @@ int ve_raycast_batch(ve_ctx* ctx, int32_t scene_id, const float* origins, const 
                      uint32_t controlchecks, uint32_t flags, uint32_t* out);
 /* device bytes held by a scene (node array + radiance cache) */
 int ve_scene_footprint(ve_ctx* ctx, int32_t scene_id, uint64_t* bytes);
+/* The box bounce rays are clipped to (no reference counterpart: a bound the
+ * trace derives from the top table).  A bounce ray whose escape and timeout
+ * shade alike ends, as escaped, once it has left the box of the top-table
+ * cells that hold voxels, widened by one voxel: it can hit nothing after
+ * that.  *bounded = 0 (lo/hi = -/+1e30) when no box applies: scenes without
+ * a top table (depth < 3), deeper than 12, or whose faces {x, y or z = 2^D}
+ * (inside the DDA's bounds test, read through root words 1..7) hold a
+ * voxel.  Recomputed by every upload, build and edit. */
+int ve_scene_clip_box(ve_ctx* ctx, int32_t scene_id, float lo[3], float hi[3], uint32_t* bounded);
 
 /* MaterialPool UBO (src/renderer/material.cpp:17-49): n entries of 64 B
  * (std140 Material), index 0 reserved. */

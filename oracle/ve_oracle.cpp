@@ -1345,11 +1345,9 @@ void oracle_fill_normals_mode(uint32_t* words, uint64_t n, uint32_t depth, int m
     struct E { uint32_t off, level, x, y, z; };
     std::vector<E> leaves;
     std::vector<E> st;
-    // root block: slots 1..8 are the root's children at CPU level 2
-    for (uint32_t i = 0; i < 8; i++) {
-        const uint32_t half = L >> 1;
-        st.push_back({1u + i, 1u, (i & 4) ? half : 0u, (i & 2) ? half : 0u, (i & 1) ? half : 0u});
-    }
+    // from the root word (slot 0) through its child pointer, as every
+    // descent reads it (Octree::set puts the root's children at slots 1..8)
+    st.push_back({0u, 0u, 0u, 0u, 0u});
     while (!st.empty()) {
         E e = st.back();
         st.pop_back();

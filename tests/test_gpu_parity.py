@@ -152,6 +152,10 @@ EDGE_CASES = {
     "inside_volume": (5, [(x, y, 0, 4) for x in range(32) for y in range(32)], (16.0, 16.0, 20.0),
                       (16.0, 16.0, 0.0)),
     "depth1": (1, [(0, 0, 0, 1), (1, 1, 1, 2)], (3.0, 3.0, -3.0), (1.0, 1.0, 1.0)),
+    # a cube floating in an empty volume: most bounce rays leave the box of
+    # the cells that can hold a voxel long before the volume's boundary
+    "floating_cube": (6, [(x, y, z, 1 + (x + 2 * y + z) % 7) for x in range(28, 36) for y in range(27, 36)
+                          for z in range(29, 36)], (20.0, 44.0, -14.0), (32.0, 31.0, 32.0)),
 }
 
 
@@ -182,6 +186,122 @@ def test_edge_cases(ve, renderer, oracle, case, cc):
         vids, counts, _ = renderer.cache_dump(sid)
         ovids, ocounts, _ = orc.cache()
         assert np.array_equal(vids, ovids) and np.array_equal(counts.astype(np.uint64), ocounts)
+    finally:
+        renderer.release_scene(sid)
+
+
+def words_with_root_copies(depth, voxels):
+    """Octree words whose root word (word 0, child block at word 8) is
+    repeated in words 1..7.  A position with a coordinate equal to 2^D reads
+    one of those at level 0, so the face {x = 2^D} holds the voxels of the
+    plane x = 0, and likewise for y and z."""
+    occ = {(int(x), int(y), int(z)): int(m) for x, y, z, m in voxels}
+    words = [0] * 8
+
+    def build(level, ox, oy, oz):
+        size = 1 << (depth - level)
+        if level == depth:
+            return (occ.get((ox, oy, oz), 0) & 0x7F) << 1
+        if not any(ox <= x < ox + size and oy <= y < oy + size and oz <= z < oz + size for x, y, z in occ):
+            return 0
+        block = len(words)
+        words.extend([0] * 8)
+        half = size >> 1
+        for c in range(8):
+            words[block + c] = build(level + 1, ox + ((c >> 2) & 1) * half, oy + ((c >> 1) & 1) * half,
+                                     oz + (c & 1) * half)
+        return (block << 4) | 1
+
+    root = build(0, 0, 0, 0)
+    words[0:8] = [root] * 8
+    return np.asarray(words, np.uint32)
+
+
+def test_clip_box(ve, renderer, oracle):
+    """The box is the top-table cells holding voxels widened by one voxel, and
+    no box applies when the faces at 2^D (read through root words 1..7) hold
+    voxels."""
+    cube = [(x, y, z, 2) for x in range(28, 36) for y in range(27, 36) for z in range(29, 35)]
+    sid = renderer.upload_scene(scene_from_voxels(ve, 6, cube), 6)
+    try:
+        lo, hi, bounded = renderer.clip_box(sid)
+        # depth 6: the table resolves 5 levels, cells of 4 voxels
+        assert bounded
+        assert lo.tolist() == [27.0, 23.0, 27.0] and hi.tolist() == [37.0, 37.0, 37.0]
+    finally:
+        renderer.release_scene(sid)
+    depth = 4
+    inner = [(x, y, z, 1 + (x + y) % 5) for x in range(3, 9) for y in range(1, 7) for z in range(2, 12)]
+    faces = inner + [(5, 0, 5, 3)]  # mirrored onto the face y = 16
+    mats = ve.terrain_materials(3)
+    renderer.set_materials(mats)
+    for vox, want in ((inner, True), (faces, False)):
+        words = words_with_root_copies(depth, vox)
+        sid = renderer.upload_scene(words, depth)
+        try:
+            assert renderer.clip_box(sid)[2] == want
+            dev_words = renderer.download_scene(sid)
+            assert np.array_equal(dev_words, oracle.fill_normals(words, depth))
+            eye = np.array([10.0, 9.0, 0.5], np.float32)
+            cam = ve.camera_ubo(eye, ve.look_at(eye, (6.0, 3.0, 7.0)), 70.0, 40 / 24)
+            fc = ve.FrameConfig(width=40, height=24, spp=4, bounces=3, primary_controlchecks=90,
+                                bounce_controlchecks=90, flags=ve.FRAME_PATH_RGB)
+            _, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 1,
+                               want=("gbuffer", "path_rgb"))
+            g, st, ref = outs[0]
+            assert np.array_equal(g["gbuffer"], ref["gbuffer"])
+            hit = np.repeat(ref["gbuffer"][..., 3].reshape(-1) != 0, fc.spp)
+            assert hit.mean() > 0.1
+            assert np.array_equal(g["path_rgb"][hit].view(np.uint32), ref["path_rgb"][hit].view(np.uint32))
+        finally:
+            renderer.release_scene(sid)
+
+
+def test_clip_box_follows_edits(ve, renderer, oracle):
+    """Bounce rays end on leaving the box of the cells that can hold a voxel;
+    edits that add voxels far outside it (a floor under a floating cube) must
+    widen it, so paths then bounce off the floor exactly as in the oracle."""
+    depth = 6
+    cube = [(x, y, z, 1 + (x + y + z) % 7) for x in range(28, 36) for y in range(28, 36) for z in range(28, 36)]
+    floor = [(x, 2, z, 3) for x in range(64) for z in range(64)]
+    c = ve.OctreeCPU(depth)
+    c.insert_many(np.asarray(cube + floor, np.uint32))
+    o = ve.Octree(depth)
+    o.set(c)
+    for x, y, z, _ in floor:
+        c.remove(x, y, z)
+    o.apply_edits(c)
+    mats = ve.terrain_materials(3)
+    renderer.set_materials(mats)
+    sid = renderer.upload_scene(o.words(), depth)
+    eye = np.array([38.0, 40.0, 17.0], np.float32)
+    cam = ve.camera_ubo(eye, ve.look_at(eye, (32.0, 30.0, 32.0)), 60.0, 48 / 32)
+    fc = ve.FrameConfig(width=48, height=32, spp=4, bounces=3, primary_controlchecks=200,
+                        bounce_controlchecks=200, flags=ve.FRAME_PATH_RGB)
+    try:
+        for step in range(2):
+            if step == 1:
+                for v in floor:
+                    c.insert(*v)
+                cap = o.capacity
+                slots = o.apply_edits(c)
+                assert o.capacity == cap  # the blocks freed above are reused: the edit path is taken
+                renderer.apply_edits(sid, slots, o.words()[slots])
+            lo, hi, bounded = renderer.clip_box(sid)
+            # depth 6: cells of 4 voxels, widened by one voxel
+            assert bounded and lo[1] == (27.0 if step == 0 else -1.0) and hi[1] == 37.0
+            renderer.cache_reset(sid)
+            dev_words = renderer.download_scene(sid)
+            assert np.array_equal(dev_words, oracle.fill_normals(o.words(), depth))
+            _, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 1,
+                               want=("gbuffer", "path_rgb"))
+            g, st, ref = outs[0]
+            assert np.array_equal(g["gbuffer"], ref["gbuffer"])
+            hit = np.repeat(ref["gbuffer"][..., 3].reshape(-1) != 0, fc.spp)
+            assert hit.mean() > 0.1
+            assert np.array_equal(g["path_rgb"][hit].view(np.uint32), ref["path_rgb"][hit].view(np.uint32))
+            assert st["rays_bounce"] == ref["stats"]["rays_bounce"]
+            assert st["rays_shadow"] == ref["stats"]["rays_shadow"]
     finally:
         renderer.release_scene(sid)
 

@@ -191,6 +191,7 @@ _SIGNATURES = {
     "ve_scene_apply_edits": ([_P, _I32, _P, _P, _U64, _U32], ctypes.c_int),
     "ve_scene_download": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
     "ve_scene_footprint": ([_P, _I32, _PTR(_U64)], ctypes.c_int),
+    "ve_scene_clip_box": ([_P, _I32, _P, _P, _PTR(_U32)], ctypes.c_int),
     "ve_raycast_batch": ([_P, _I32, _P, _P, _U64, _U32, _U32, _P], ctypes.c_int),
     "ve_lbuffer_dump": ([_P, _I32, _P, _U64, _PTR(_U64)], ctypes.c_int),
     "ve_set_materials": ([_P, _P, _U32], ctypes.c_int),
@@ -639,6 +640,14 @@ class Renderer:
         b = _U64()
         _check(self._lib.ve_scene_footprint(self._h, scene_id, ctypes.byref(b)))
         return b.value
+
+    def clip_box(self, scene_id: int):
+        """(lo, hi, bounded): the box bounce rays are clipped to (ve_scene_clip_box)."""
+        lo = np.zeros(3, np.float32)
+        hi = np.zeros(3, np.float32)
+        b = ctypes.c_uint32()
+        _check(self._lib.ve_scene_clip_box(self._h, scene_id, _ptr(lo), _ptr(hi), ctypes.byref(b)))
+        return lo, hi, bool(b.value)
 
     def set_materials(self, materials: np.ndarray) -> None:
         m = np.ascontiguousarray(materials, np.float32).reshape(-1, 16)

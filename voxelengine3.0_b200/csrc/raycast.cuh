@@ -47,6 +47,7 @@ __device__ __forceinline__ uint32_t word_bound(uint64_t n) { return n < 0xFFFFFF
 struct Dda {
     f3 o, d, inv;
     float t;  // the position is d * t + o (recomputed each step: the same operations as storing it)
+    float t_end;  // CLIP: past this distance the ray can hit nothing (set by the caller)
     uint32_t q, cc;
     uint32_t lux, luy, luz, e_last;
     uint32_t base[17];
@@ -97,13 +98,15 @@ __device__ __forceinline__ uint32_t top_index(uint32_t x, uint32_t y, uint32_t z
 
 // WORD: a hit reports the leaf's node word in h.id instead of its slot (the
 // bounce trace keeps the word for shading; the slot is the GBuffer's field).
-template <bool COUNT, bool WORD = false>
+// CLIP: the ray also ends, as escaped, once its distance passes s.t_end —
+// for callers to whom an escape and a timeout are the same result.
+template <bool COUNT, bool WORD = false, bool CLIP = false>
 __device__ __forceinline__ bool dda_step(Dda& s, const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
                                          const uint32_t* __restrict__ top, uint32_t T0, Hit& h, RayCount& rc) {
     const uint32_t L = 1u << D;
     const float Lf = float(L);
     const f3 r = add(muls(s.d, s.t), s.o);
-    if (!in_bounds(r, Lf)) {
+    if (!in_bounds(r, Lf) || (CLIP && s.t > s.t_end)) {
         h.status = kEscaped;
         h.checks = s.q;
         return true;

@@ -68,6 +68,9 @@ struct DevScene {
     uint32_t* lbuf;       // the dual-channel lBuffer (VE_FRAME_LBUFFER; null until first used)
     const float4* ntab;   // ball-normal scenes: unit normal per code index (null: 3x3x3 gradient)
     uint32_t n_ntab;
+    // the box of the cells that can hold a voxel, widened by one voxel on
+    // every side (bounce rays end when they leave it; see k_trace)
+    float clip_lo[3], clip_hi[3];
 };
 
 struct DevMaterial {
@@ -458,12 +461,26 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                     f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
                     if (EM && (e >> 31) && (v.flags & VE_FRAME_EMISSIVE)) d = ld3(a.p_sdir[p]);
                     finished = dda_init(s, o, d, v.cc_bounce, D, h);
+                    if (!COUNT) {
+                        // a bounce ray that escapes or times out shades as
+                        // sky alike, so it ends on leaving the box of the
+                        // cells that can hold a voxel (exit of its slab);
+                        // shadow rays walk on (there a timeout is a shadow)
+                        float te = __int_as_float(0x7f800000);
+                        if (!(e >> 31)) {
+                            const float tx = ((s.inv.x > 0.0f ? S.clip_hi[0] : S.clip_lo[0]) - s.o.x) * s.inv.x;
+                            const float ty = ((s.inv.y > 0.0f ? S.clip_hi[1] : S.clip_lo[1]) - s.o.y) * s.inv.y;
+                            const float tz = ((s.inv.z > 0.0f ? S.clip_hi[2] : S.clip_lo[2]) - s.o.z) * s.inv.z;
+                            te = gmin(gmin(tx, ty), tz);
+                        }
+                        s.t_end = te;
+                    }
                     active = !finished;
                 }
             }
         }
         if (active) {
-            finished = dda_step<COUNT, true>(s, nodes, n_words, D, top, T0, h, rc);
+            finished = dda_step<COUNT, true, !COUNT>(s, nodes, n_words, D, top, T0, h, rc);
             if (finished) active = false;
         }
         if (finished) {
@@ -1948,6 +1965,9 @@ struct SceneSlot {
     uint32_t normal_radius = 0;
     float4* ntab = nullptr;
     uint32_t n_ntab = 0;
+    // bounce-ray clip box (DevScene::clip_lo/hi), from the top table build;
+    // unbounded when the scene has no top table
+    float clip_lo[3] = {-1e30f, -1e30f, -1e30f}, clip_hi[3] = {1e30f, 1e30f, 1e30f};
 };
 
 template <typename T>
@@ -2102,7 +2122,9 @@ static int sync_scenes(ve_ctx* c) {
         const SceneSlot& s = c->scenes[i];
         h[i] = DevScene{s.nodes,     s.n_words,   s.cache,    s.depth,    c->cfg.hash_log2, c->cfg.hash_probes,
                         s.top_level, s.top,       s.em_list, s.em_claim, s.em_state,       s.em_stage,
-                        s.res,       s.lbuf,      s.ntab,    s.n_ntab};
+                        s.res,       s.lbuf,      s.ntab,    s.n_ntab,
+                        {s.clip_lo[0], s.clip_lo[1], s.clip_lo[2]},
+                        {s.clip_hi[0], s.clip_hi[1], s.clip_hi[2]}};
     }
     const void* old = c->d_scenes.p;
     int rc = c->d_scenes.ensure(h.size());
@@ -2117,12 +2139,23 @@ static int sync_scenes(ve_ctx* c) {
 // Top table of the DDA descent: one word per cell of the level-(T0-1) grid,
 // found by walking levels 0..T0-1 of the node words exactly as the descent
 // does (out-of-range words read as zero).
+//
+// Also the box of the cells that can hold a voxel: a descent that ends above
+// level D steps over an empty cell (only level-D words are tested for a
+// material), so only cells internal down to level T0 can be hit.  box[0..2]
+// = smallest, box[3..5] = largest such cell coordinate (box[0] > box[3]: no
+// such cell).  Positions with a coordinate equal to 2^D lie outside the
+// table; k_face_hits covers them.
 __global__ void k_build_top(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D, uint32_t T0,
-                            uint32_t* __restrict__ top) {
+                            uint32_t* __restrict__ top, uint32_t* __restrict__ box) {
+    __shared__ uint32_t sb[6];
+    if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? 0xFFFFFFFFu : 0u;
     const uint32_t b = T0 - 1u, n = 1u << (3u * b);
     const uint32_t sh = D - T0 + 1u, L = 1u << D;
+    uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t x = (i >> (2u * b)) << sh, y = ((i >> b) & ((1u << b) - 1u)) << sh, z = (i & ((1u << b) - 1u)) << sh;
+        const uint32_t cx = i >> (2u * b), cy = (i >> b) & ((1u << b) - 1u), cz = i & ((1u << b) - 1u);
+        const uint32_t x = cx << sh, y = cy << sh, z = cz << sh;
         uint32_t base = 0, ent = 0;
         bool terminal = false;
         for (uint32_t k = 0; k < T0; k++) {
@@ -2135,7 +2168,56 @@ __global__ void k_build_top(const uint32_t* __restrict__ nodes, uint64_t n_words
             base = raw >> 4;
         }
         top[i] = terminal ? ent : ((base << 1) | 1u);
+        if (!terminal) {
+            lo[0] = min(lo[0], cx); lo[1] = min(lo[1], cy); lo[2] = min(lo[2], cz);
+            hi[0] = max(hi[0], cx); hi[1] = max(hi[1], cy); hi[2] = max(hi[2], cz);
+        }
     }
+    __syncthreads();
+    for (int a = 0; a < 3; a++) {
+        const uint32_t wl = __reduce_min_sync(0xFFFFFFFFu, lo[a]), wh = __reduce_max_sync(0xFFFFFFFFu, hi[a]);
+        if ((threadIdx.x & 31u) == 0u) {
+            atomicMin(&sb[a], wl);
+            atomicMax(&sb[3 + a], wh);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&box[threadIdx.x], sb[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&box[threadIdx.x], sb[threadIdx.x]);
+}
+
+// The DDA's bounds test admits a coordinate equal to 2^D, whose bit D sends
+// the level-0 read to root words 1..7 instead of word 0 (internal.glsl's
+// locate at octreeLength).  Sets *hit when any integer position on the three
+// faces {x, y or z = 2^D} ends its descent on a material voxel — the only
+// positions outside the top table's cells that can be hit.
+__global__ void __launch_bounds__(256) k_face_hits(const uint32_t* __restrict__ nodes, uint64_t n_words, uint32_t D,
+                                                   uint32_t* hit) {
+    const uint32_t L = 1u << D, side = L + 1u;
+    const uint64_t per_face = uint64_t(side) * side;
+    bool any = false;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < 3u * per_face;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t f = uint32_t(i / per_face);
+        const uint64_t j = i % per_face;
+        const uint32_t u = uint32_t(j / side), v = uint32_t(j % side);
+        const uint32_t x = f == 0 ? L : u, y = f == 1 ? L : (f == 0 ? u : v), z = f == 2 ? L : v;
+        // the descent of dda_step without the top table
+        uint32_t base = 0;
+        bool internal = true;
+        for (uint32_t k = 0; k < D && internal; k++) {
+            const uint32_t b = D - k;
+            const uint32_t raw = dev::fetch_node(nodes, n_words,
+                                                 base + ((((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u)));
+            internal = (raw & 1u) != 0u;
+            base = raw >> 4;
+        }
+        if (internal) {
+            const uint32_t raw = dev::fetch_node(nodes, n_words, base + (((x & 1u) << 2) | ((y & 1u) << 1) | (z & 1u)));
+            any |= ((raw & 254u) >> 1) != 0u;
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, any) && (threadIdx.x & 31u) == 0u) atomicOr(hit, 1u);
 }
 
 // Octree::applyEdits upload (octree.cpp:228-314): words[i] -> nodes[slots[i]].
@@ -2214,14 +2296,44 @@ static uint32_t top_levels(uint32_t D) { return D < 3u ? 0u : std::min(9u, D - 1
 
 static int build_top(ve_ctx* c, SceneSlot& s) {
     const uint32_t T0 = top_levels(s.depth);
+    c->scenes_dirty = true;
+    for (int a = 0; a < 3; a++) {  // unbounded until the table says otherwise
+        s.clip_lo[a] = -1e30f;
+        s.clip_hi[a] = 1e30f;
+    }
     if (T0 == 0) return VE_OK;
     const size_t n = size_t(1) << (3u * (T0 - 1u));
     if (!s.top) {
         if (cudaMalloc(&s.top, n * 4) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene: top table allocation failed");
     }
     s.top_level = T0;
-    k_build_top<<<c->num_sms * 8, 256, 0, c->stream>>>(s.nodes, s.n_words, s.depth, T0, s.top);
-    VE_CUDA(cudaGetLastError());
+    uint32_t* d_box = nullptr;
+    if (cudaMalloc(&d_box, 7 * 4) != cudaSuccess) return fail(VE_ERR_NOMEM, "scene: allocation failed");
+    const uint32_t init[7] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u};
+    uint32_t box[7];
+    cudaMemcpyAsync(d_box, init, sizeof(init), cudaMemcpyHostToDevice, c->stream);
+    k_build_top<<<c->num_sms * 8, 256, 0, c->stream>>>(s.nodes, s.n_words, s.depth, T0, s.top, d_box);
+    // faces of more than 3 * 4097^2 positions are not searched: no box then
+    if (s.depth <= 12) k_face_hits<<<c->num_sms * 8, 256, 0, c->stream>>>(s.nodes, s.n_words, s.depth, d_box + 6);
+    cudaMemcpyAsync(box, d_box, sizeof(box), cudaMemcpyDeviceToHost, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_box);
+    if (e != cudaSuccess) return fail(VE_ERR_CUDA, std::string("scene: top table build: ") + cudaGetErrorString(e));
+    if (s.depth > 12) box[6] = 1u;
+    if (!box[6]) {
+        // cells are 2^(D-T0+1) voxels wide; one voxel of margin on each side
+        // keeps the box conservative against rounding of the ray positions
+        const uint32_t sh = s.depth - T0 + 1u;
+        for (int a = 0; a < 3; a++) {
+            if (box[0] > box[3]) {  // no cell can be hit: any box is exact
+                s.clip_lo[a] = -1.0f;
+                s.clip_hi[a] = 1.0f;
+            } else {
+                s.clip_lo[a] = float(box[a] << sh) - 1.0f;
+                s.clip_hi[a] = float((box[3 + a] + 1u) << sh) + 1.0f;
+            }
+        }
+    }
     return VE_OK;
 }
 
@@ -3775,6 +3887,19 @@ int ve_scene_footprint(ve_ctx* c, int32_t id, uint64_t* bytes) {
     const SceneSlot& sl = c->scenes[id];
     const uint64_t top = sl.top_level ? (4ull << (3u * (sl.top_level - 1u))) : 0ull;
     *bytes = (sl.n_words + 8) * 4 + (sizeof(CacheEntry) << c->cfg.hash_log2) + top;
+    return VE_OK;
+}
+
+int ve_scene_clip_box(ve_ctx* c, int32_t id, float lo[3], float hi[3], uint32_t* bounded) {
+    if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
+        return fail(VE_ERR_NOT_FOUND, "scene_clip_box: unknown scene");
+    if (!lo || !hi || !bounded) return fail(VE_ERR_INVALID, "scene_clip_box: null argument");
+    const SceneSlot& sl = c->scenes[id];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = sl.clip_lo[a];
+        hi[a] = sl.clip_hi[a];
+    }
+    *bounded = sl.clip_lo[0] > -1e29f ? 1u : 0u;
     return VE_OK;
 }
 
