@@ -10,11 +10,12 @@ radius 600.  A ray is one DDA traversal (primary, bounce or sun shadow).
 
 * ``value``: device-resident frames back to back (no host outputs), CUDA
   events on the renderer's stream around K frames, max over ranks.
-* ``e2e``: the same frames through the public API with host outputs (voxel-id
-  image + RGB into pinned host memory) and the per-frame view table uploaded;
-  each frame's images are copied on the renderer's copy stream while the next
-  frame renders (VE_FRAME_ASYNC_OUTPUTS, two alternating pinned sets); events
-  around all K steps and the last frame's copies.
+* ``e2e``: the same frames through the public API with each frame's result —
+  its displayed RGBA8 image, final.frag's framebuffer store — read into pinned
+  host memory and the per-frame view table uploaded; each frame's image is
+  copied on the renderer's copy stream while the next frame renders
+  (VE_FRAME_ASYNC_OUTPUTS, two alternating pinned images); events around all K
+  steps and the last frame's copy.
 * ``roofline``: the trace kernel (bounce + shadow DDA): algorithmic bytes
   (4 B per distinct node word read + 48 B ray state per traversal) over its
   CUDA-event time inside the timed frames, against the measured HBM copy
@@ -1047,17 +1048,17 @@ def main():
     traffic, traffic_src = measured_trace_traffic()
 
     # ---- e2e: public API, host outputs, view upload each step --------------
-    # outputs copied on the renderer's copy stream while the next frame
-    # renders (VE_FRAME_ASYNC_OUTPUTS), into two alternating pinned sets;
-    # every frame's images reach host memory inside the timed region
+    # each frame's result is its displayed image — the RGBA8 framebuffer
+    # final.frag writes (the mapped8 output) — copied on the renderer's copy
+    # stream while the next frame renders (VE_FRAME_ASYNC_OUTPUTS), into two
+    # alternating pinned images; every frame's image reaches host memory
+    # inside the timed region
     sets = []
     for _ in range(2):
-        hv = torch.empty((W.height, W.width), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-        hrgb = torch.empty((W.height, W.width, 3), dtype=torch.float32, pin_memory=True).numpy()
+        himg = torch.empty((W.height, W.width, 4), dtype=torch.uint8, pin_memory=True).numpy()
         o = ve.FrameOutputsC()
-        o.voxel_id = hv.ctypes.data
-        o.rgb = hrgb.ctypes.data
-        sets.append((o, hv, hrgb))
+        o.mapped8 = himg.ctypes.data
+        sets.append((o, himg))
     lib = ve.load_library()
     import ctypes
 
@@ -1093,7 +1094,8 @@ def main():
             "rays_per_step": rays_of(tot) / K,
             "ray_mix_per_step": {k: tot[k] / K for k in ("rays_primary", "rays_bounce", "rays_shadow")},
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": etot["h2d_bytes"] / K,
-                    "d2h_bytes_per_step": etot["d2h_bytes"] / K},
+                    "d2h_bytes_per_step": etot["d2h_bytes"] / K,
+                    "outputs": "the displayed RGBA8 image (final.frag's framebuffer store), pinned host memory"},
             "roofline": {"bound": "hbm", "kernel": "k_trace (bounce + shadow DDA)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,

@@ -56,7 +56,7 @@ extern "C" {
                                      on rows [row_begin, row_end) and deposit into a per-frame table
                                      that ve_split_export / ve_split_merge exchange; the AvgPass runs
                                      in ve_split_resolve after the merge */
-#define VE_FRAME_ASYNC_OUTPUTS 1024u /* host outputs (voxel_id, hit_node, rgb, mapped only) are copied on the
+#define VE_FRAME_ASYNC_OUTPUTS 1024u /* host outputs (voxel_id, hit_node, rgb, mapped, mapped8 only) are copied on the
                                      context's copy stream while later frames render: the call returns
                                      once the frame is enqueued, and the host buffers (pinned memory for
                                      the copies to run asynchronously) hold the frame after
@@ -143,6 +143,9 @@ typedef struct ve_frame_outputs {
                            zero for pixels without a primary hit (no path).  With
                            VE_FRAME_SCHEDULED: one per shade-list entry, room for
                            min(shading_budget, 2 * width * height) paths */
+    uint8_t* mapped8;   /* 4 x u8 per pixel: the displayed image, FragColor =
+                           (mapped, 1) as an RGBA8 framebuffer stores it (final.frag:15-18:
+                           clamp to [0, 1], x 255, round to nearest) */
 } ve_frame_outputs;
 
 /* FrameStats (src/renderer/core.hpp:164-185) and the profiler's stage

@@ -36,8 +36,15 @@ def pair(ve):
 def pinned(shape, dtype):
     import torch
 
-    t = torch.empty(shape, dtype=torch.int32 if dtype == np.uint32 else torch.float32, pin_memory=True)
+    tdtype = {np.uint32: torch.int32, np.uint8: torch.uint8, np.float32: torch.float32}[dtype]
+    t = torch.empty(shape, dtype=tdtype, pin_memory=True)
     return t, t.numpy().view(dtype)
+
+
+def quantize(mapped):
+    """The RGBA8 store of (mapped, 1): clamp, x 255, round to nearest (float32 steps)."""
+    m = np.clip(np.asarray(mapped, np.float32), np.float32(0), np.float32(1))
+    return (m * np.float32(255) + np.float32(0.5)).astype(np.uint32).astype(np.uint8)
 
 
 def test_async_frames_equal_sync_frames(ve, pair):
@@ -51,8 +58,9 @@ def test_async_frames_equal_sync_frames(ve, pair):
         tv, v = pinned((H, W), np.uint32)
         tr, rgb = pinned((H, W, 3), np.float32)
         tm, mp = pinned((H, W, 3), np.float32)
-        keep += [tv, tr, tm]
-        outs.append({"voxel_id": v, "rgb": rgb, "mapped": mp})
+        t8, m8 = pinned((H, W, 4), np.uint8)
+        keep += [tv, tr, tm, t8]
+        outs.append({"voxel_id": v, "rgb": rgb, "mapped": mp, "mapped8": m8})
         ff = dataclasses.replace(fc, frame_index=f, flags=ve.FRAME_ASYNC_OUTPUTS)
         ra.render_into(sa, cam, ff, outs[-1])
     ra.synchronize()
@@ -61,6 +69,9 @@ def test_async_frames_equal_sync_frames(ve, pair):
         assert np.array_equal(outs[f]["voxel_id"], ref["voxel_id"]), f
         assert close_rel(outs[f]["rgb"], ref["rgb"]).all(), f
         assert close_rel(outs[f]["mapped"], ref["mapped"]).all(), f
+        # the displayed image: the frame's own mapped radiance stored as RGBA8
+        assert np.array_equal(outs[f]["mapped8"][..., :3], quantize(outs[f]["mapped"])), f
+        assert (outs[f]["mapped8"][..., 3] == 255).all()
     assert outs[-1]["rgb"].max() > 0.05
     # a synchronous frame after asynchronous ones writes the first image set
     g = ra.render(sa, cam, dataclasses.replace(fc, frame_index=6), outputs=("voxel_id",))

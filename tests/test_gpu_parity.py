@@ -97,7 +97,7 @@ def test_sixteen_frames_accumulation(ve, renderer, oracle, small):
     dev_words = renderer.download_scene(sid)
     fc = ve.FrameConfig(**{**fc.__dict__})
     orc, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 16,
-                         want=("gbuffer", "rgb", "mapped"))
+                         want=("gbuffer", "rgb", "mapped", "mapped8"))
     for g, st, o in outs:
         assert np.array_equal(g["gbuffer"], o["gbuffer"])
     # cache: exact counts, FP32 sums vs FP64
@@ -112,6 +112,13 @@ def test_sixteen_frames_accumulation(ve, renderer, oracle, small):
     frac_bad = 1.0 - ok.all(axis=-1).mean()
     assert frac_bad == 0.0, f"{frac_bad:.2e} of pixels beyond 1e-4 relative"
     assert close_rel(g["mapped"], o["mapped"]).all()
+    # the displayed RGBA8 image: the device's mapped radiance stored exactly
+    # (clamp, x 255, round to nearest), within one step of the oracle's
+    m = np.clip(g["mapped"], np.float32(0), np.float32(1))
+    assert np.array_equal(g["mapped8"][..., :3], (m * np.float32(255) + np.float32(0.5)).astype(np.uint8))
+    assert (g["mapped8"][..., 3] == 255).all()
+    om = np.floor(np.clip(o["mapped"], 0.0, 1.0) * 255.0 + 0.5)
+    assert (np.abs(g["mapped8"][..., :3].astype(np.int32) - om.astype(np.int32)) <= 1).all()
     assert g["rgb"].max() > 0.05
 
 

@@ -99,7 +99,8 @@ class ViewC(ctypes.Structure):
 
 class FrameOutputsC(ctypes.Structure):
     _fields_ = [("gbuffer", ctypes.c_void_p), ("voxel_id", ctypes.c_void_p), ("hit_node", ctypes.c_void_p),
-                ("rgb", ctypes.c_void_p), ("mapped", ctypes.c_void_p), ("path_rgb", ctypes.c_void_p)]
+                ("rgb", ctypes.c_void_p), ("mapped", ctypes.c_void_p), ("path_rgb", ctypes.c_void_p),
+                ("mapped8", ctypes.c_void_p)]
 
 
 class LaunchConfigC(ctypes.Structure):
@@ -497,7 +498,9 @@ class FrameConfig:
         return c
 
 
-OUTPUT_KINDS = ("gbuffer", "voxel_id", "hit_node", "rgb", "mapped", "path_rgb")
+OUTPUT_KINDS = ("gbuffer", "voxel_id", "hit_node", "rgb", "mapped", "path_rgb", "mapped8")
+# bytes per pixel of the per-pixel host outputs
+IMAGE_BYTES = {"gbuffer": 16, "voxel_id": 4, "hit_node": 4, "rgb": 12, "mapped": 12, "mapped8": 4}
 
 
 def _dev_ptr(buf) -> Optional[int]:
@@ -519,6 +522,8 @@ def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
             arrays[k] = np.zeros((fc.height, fc.width), np.uint32)
         elif k in ("rgb", "mapped"):
             arrays[k] = np.zeros((fc.height, fc.width, 3), np.float32)
+        elif k == "mapped8":
+            arrays[k] = np.zeros((fc.height, fc.width, 4), np.uint8)
         elif k == "path_rgb":
             n = min(fc.shading_budget, 2 * npx) if fc.flags & FRAME_SCHEDULED else npx * fc.spp
             arrays[k] = np.zeros((n, 3), np.float32)
@@ -528,6 +533,20 @@ def _alloc_outputs(fc: FrameConfig, want: Iterable[str]):
     for k, a in arrays.items():
         setattr(o, k, a.ctypes.data)
     return o, arrays
+
+
+def _image_outputs(fc: FrameConfig, arrays: Dict[str, np.ndarray]) -> "FrameOutputsC":
+    """FrameOutputsC over caller-owned full-size host images (name -> a
+    C-contiguous array of IMAGE_BYTES[name] bytes per pixel)."""
+    npx = fc.width * fc.height
+    o = FrameOutputsC()
+    for k, a in arrays.items():
+        if k not in IMAGE_BYTES:
+            raise ValueError(f"unknown output {k!r}")
+        if not a.flags.c_contiguous or a.nbytes != IMAGE_BYTES[k] * npx:
+            raise ValueError(f"output {k!r}: {IMAGE_BYTES[k] * npx} contiguous bytes expected")
+        setattr(o, k, a.ctypes.data)
+    return o
 
 
 class Renderer:
@@ -690,15 +709,7 @@ class Renderer:
         of the output's size).  With FRAME_ASYNC_OUTPUTS the call returns once
         the frame is enqueued; the arrays (pinned memory for an asynchronous
         copy) hold the frame after synchronize()."""
-        npx = fc.width * fc.height
-        size = {"gbuffer": 4 * npx, "voxel_id": npx, "hit_node": npx, "rgb": 3 * npx, "mapped": 3 * npx}
-        o = FrameOutputsC()
-        for k, a in arrays.items():
-            if k not in size:
-                raise ValueError(f"unknown output {k!r}")
-            if not a.flags.c_contiguous or a.size != size[k] or a.itemsize != 4:
-                raise ValueError(f"output {k!r}: {size[k]} contiguous 32-bit elements expected")
-            setattr(o, k, a.ctypes.data)
+        o = _image_outputs(fc, arrays)
         view = self.make_view(scene_id, camera, fc)
         _check(self._lib.ve_render(self._h, ctypes.byref(view), ctypes.byref(o)))
 
@@ -748,13 +759,7 @@ class Renderer:
                            arrays: Dict[str, np.ndarray]) -> None:
         """split_resolve into caller-owned full-size host arrays (the band's
         rows are written)."""
-        npx = fc.width * fc.height
-        size = {"gbuffer": 4 * npx, "voxel_id": npx, "hit_node": npx, "rgb": 3 * npx, "mapped": 3 * npx}
-        o = FrameOutputsC()
-        for k, a in arrays.items():
-            if k not in size or not a.flags.c_contiguous or a.size != size[k] or a.itemsize != 4:
-                raise ValueError(f"output {k!r}: {size.get(k)} contiguous 32-bit elements expected")
-            setattr(o, k, a.ctypes.data)
+        o = _image_outputs(fc, arrays)
         view = self.make_view(scene_id, camera, fc)
         _check(self._lib.ve_split_resolve(self._h, ctypes.byref(view), ctypes.byref(o)))
 

@@ -184,6 +184,7 @@ struct FrameArgs {
     uint32_t* out_node;
     float* out_rgb;
     float* out_mapped;
+    uchar4* out_mapped8;  // the displayed RGBA8 image (final.frag into the framebuffer)
     float* path_rgb;
     uint32_t refill;       // idle lanes at which a trace warp takes new rays
     uint32_t view_offset;  // index of views[0] in the view table the paths refer to
@@ -1735,11 +1736,18 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
         a.out_rgb[3ull * gp + 1] = col.y;
         a.out_rgb[3ull * gp + 2] = col.z;
     }
+    const f3 m = mk(aces(col.x), aces(col.y), aces(col.z));
     if (a.out_mapped) {
-        a.out_mapped[3ull * gp + 0] = aces(col.x);
-        a.out_mapped[3ull * gp + 1] = aces(col.y);
-        a.out_mapped[3ull * gp + 2] = aces(col.z);
+        a.out_mapped[3ull * gp + 0] = m.x;
+        a.out_mapped[3ull * gp + 1] = m.y;
+        a.out_mapped[3ull * gp + 2] = m.z;
     }
+    // the framebuffer's unsigned-normalised store of FragColor = (mapped, 1):
+    // clamp to [0, 1], scale by 255, round to nearest
+    if (a.out_mapped8)
+        a.out_mapped8[gp] = make_uchar4(uint8_t(uint32_t(gclamp(m.x, 0.0f, 1.0f) * 255.0f + 0.5f)),
+                                        uint8_t(uint32_t(gclamp(m.y, 0.0f, 1.0f) * 255.0f + 0.5f)),
+                                        uint8_t(uint32_t(gclamp(m.z, 0.0f, 1.0f) * 255.0f + 0.5f)), 255);
 }
 
 // ---------------------------------------------------------------------------
@@ -2035,11 +2043,13 @@ struct ve_ctx {
     ve::DevBuf<uint4> gbuf;
     ve::DevBuf<uint32_t> out_vid, out_node;
     ve::DevBuf<float> out_rgb, out_mapped, path_rgb;
+    ve::DevBuf<uchar4> out_m8;
     // VE_FRAME_ASYNC_OUTPUTS: a second set of device images (frames alternate
     // between the sets), the stream their host copies run on, and events
     // that order a set's next resolve after its last copy
     ve::DevBuf<uint32_t> out_vid2, out_node2;
     ve::DevBuf<float> out_rgb2, out_mapped2;
+    ve::DevBuf<uchar4> out_m82;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t frame_done = nullptr, copy_done[2] = {};
     int out_parity = 0;
@@ -2515,15 +2525,15 @@ static int reset_rank(ve_ctx* c, float* rank) {
 
 static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_views) {
     int rc = 0;
-    const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->p_ray_o.p,
-                            c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p, c->p_pend.p, c->p_hit.p,
-                            c->p_meta.p, c->live0.p, c->live1.p, c->rayq.p, c->d_views.p};
+    const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->out_m8.p,
+                            c->p_ray_o.p, c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p, c->p_pend.p,
+                            c->p_hit.p, c->p_meta.p, c->live0.p, c->live1.p, c->rayq.p, c->d_views.p};
     struct GenBump {
         ve_ctx* c;
         const void* const* before;
         ~GenBump() {
             const void* after[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p,
-                                   c->p_ray_o.p, c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p,
+                                   c->out_m8.p, c->p_ray_o.p, c->p_ray_d.p, c->p_tp.p, c->p_direct.p, c->p_indirect.p,
                                    c->p_pend.p, c->p_hit.p, c->p_meta.p, c->live0.p, c->live1.p,
                                    c->rayq.p, c->d_views.p};
             for (size_t i = 0; i < sizeof(after) / sizeof(after[0]); i++)
@@ -2534,7 +2544,8 @@ static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_v
     if (c->copy_stream && (pixels > c->out_vid.cap || 3 * pixels > c->out_rgb.cap))
         cudaStreamSynchronize(c->copy_stream);
     if ((rc = c->gbuf.ensure(pixels)) || (rc = c->out_vid.ensure(pixels)) || (rc = c->out_node.ensure(pixels)) ||
-        (rc = c->out_rgb.ensure(pixels * 3)) || (rc = c->out_mapped.ensure(pixels * 3)))
+        (rc = c->out_rgb.ensure(pixels * 3)) || (rc = c->out_mapped.ensure(pixels * 3)) ||
+        (rc = c->out_m8.ensure(pixels)))
         return rc;
     if ((rc = c->p_ray_o.ensure(paths)) || (rc = c->p_ray_d.ensure(paths)) || (rc = c->p_tp.ensure(paths)) ||
         (rc = c->p_direct.ensure(paths)) || (rc = c->p_indirect.ensure(paths)) || (rc = c->p_pend.ensure(paths)) ||
@@ -2730,7 +2741,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT renders plain path-traced frames only");
         if (f.row_begin >= f.row_end || f.row_end > f.height)
             return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT needs row_begin < row_end <= height");
-        if (outs && (outs[0].rgb || outs[0].mapped || outs[0].voxel_id || outs[0].hit_node))
+        if (outs && (outs[0].rgb || outs[0].mapped || outs[0].mapped8 || outs[0].voxel_id || outs[0].hit_node))
             return fail(VE_ERR_INVALID, "render: a VE_FRAME_SPLIT frame's image comes from ve_split_resolve");
     }
     const bool async_out = (flags & VE_FRAME_ASYNC_OUTPUTS) != 0;
@@ -2738,7 +2749,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (split) return fail(VE_ERR_INVALID, "render: VE_FRAME_SPLIT frames have no images to copy");
         for (uint32_t i = 0; outs && i < nv; i++)
             if (outs[i].gbuffer || outs[i].path_rgb)
-                return fail(VE_ERR_INVALID, "render: VE_FRAME_ASYNC_OUTPUTS copies voxel_id, hit_node, rgb and mapped only");
+                return fail(VE_ERR_INVALID,
+                            "render: VE_FRAME_ASYNC_OUTPUTS copies voxel_id, hit_node, rgb, mapped and mapped8 only");
     }
     if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
     // learned radiance cache: one per batch, attached to the views' scenes
@@ -2761,13 +2773,14 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
                 cudaEventCreateWithFlags(&c->copy_done[1], cudaEventDisableTiming) != cudaSuccess)
                 return fail(VE_ERR_CUDA, "render: copy stream creation failed");
         }
-        const void* before[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p};
+        const void* before[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p, c->out_m82.p};
         if (pixels > c->out_vid2.cap || 3 * pixels > c->out_rgb2.cap) cudaStreamSynchronize(c->copy_stream);
         if ((rc = c->out_vid2.ensure(pixels)) || (rc = c->out_node2.ensure(pixels)) ||
-            (rc = c->out_rgb2.ensure(3 * pixels)) || (rc = c->out_mapped2.ensure(3 * pixels)))
+            (rc = c->out_rgb2.ensure(3 * pixels)) || (rc = c->out_mapped2.ensure(3 * pixels)) ||
+            (rc = c->out_m82.ensure(pixels)))
             return rc;
-        const void* after[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p};
-        for (int i = 0; i < 4; i++)
+        const void* after[] = {c->out_vid2.p, c->out_node2.p, c->out_rgb2.p, c->out_mapped2.p, c->out_m82.p};
+        for (int i = 0; i < 5; i++)
             if (before[i] != after[i]) c->gen++;
         parity = c->out_parity;
     }
@@ -2937,6 +2950,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     a.out_node = parity ? c->out_node2.p : c->out_node.p;
     a.out_rgb = parity ? c->out_rgb2.p : c->out_rgb.p;
     a.out_mapped = parity ? c->out_mapped2.p : c->out_mapped.p;
+    a.out_mapped8 = parity ? c->out_m82.p : c->out_m8.p;
     a.path_rgb = (flags & VE_FRAME_PATH_RGB) ? c->path_rgb.p : nullptr;
     a.refill = c->launch.refill_threshold;
     a.view_offset = 0;
@@ -3184,6 +3198,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             if (o.hit_node) { VE_CUDA(cudaMemcpyAsync(o.hit_node, a.out_node + pb, np * 4, cudaMemcpyDeviceToHost, cs)); d2h += np * 4; }
             if (o.rgb) { VE_CUDA(cudaMemcpyAsync(o.rgb, a.out_rgb + 3 * pb, np * 12, cudaMemcpyDeviceToHost, cs)); d2h += np * 12; }
             if (o.mapped) { VE_CUDA(cudaMemcpyAsync(o.mapped, a.out_mapped + 3 * pb, np * 12, cudaMemcpyDeviceToHost, cs)); d2h += np * 12; }
+            if (o.mapped8) { VE_CUDA(cudaMemcpyAsync(o.mapped8, a.out_mapped8 + pb, np * 4, cudaMemcpyDeviceToHost, cs)); d2h += np * 4; }
             pb += np;
         }
         VE_CUDA(cudaEventRecord(c->copy_done[parity], cs));
@@ -3213,6 +3228,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             if (o.hit_node) { VE_CUDA(cudaMemcpyAsync(o.hit_node, c->out_node.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
             if (o.rgb) { VE_CUDA(cudaMemcpyAsync(o.rgb, c->out_rgb.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st)); d2h += np * 12; }
             if (o.mapped) { VE_CUDA(cudaMemcpyAsync(o.mapped, c->out_mapped.p + 3 * pb, np * 12, cudaMemcpyDeviceToHost, st)); d2h += np * 12; }
+            if (o.mapped8) { VE_CUDA(cudaMemcpyAsync(o.mapped8, c->out_m8.p + pb, np * 4, cudaMemcpyDeviceToHost, st)); d2h += np * 4; }
             if (o.path_rgb && (f.flags & VE_FRAME_PATH_RGB)) {
                 VE_CUDA(cudaMemcpyAsync(o.path_rgb, c->path_rgb.p + 3 * qb, nq * 12, cudaMemcpyDeviceToHost, st));
                 d2h += nq * 12;
@@ -3441,7 +3457,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     c->p_aux.release();
     c->hitinfo.release(); c->claim.release(); c->sched_n.release(); c->shade_list.release(); c->scan_tmp.release();
     c->gbuf.release(); c->out_vid.release(); c->out_node.release(); c->out_rgb.release();
-    c->out_mapped.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
+    c->out_mapped.release(); c->out_m8.release(); c->path_rgb.release(); c->ray_in.release(); c->ray_out.release();
     c->p_sdir.release(); c->p_res.release(); c->res_list.release(); c->em_sort.release(); c->em_sort_tmp.release();
     c->lb_rec.release(); c->lb_keys.release(); c->lb_idx.release(); c->lb_tmp.release();
     c->split_delta.release(); c->d_scenes_split.release(); c->split_cnt.release();
@@ -3453,6 +3469,7 @@ int ve_ctx_destroy(ve_ctx* c) {
     for (auto& e : c->copy_done)
         if (e) cudaEventDestroy(e);
     c->out_vid2.release(); c->out_node2.release(); c->out_rgb2.release(); c->out_mapped2.release();
+    c->out_m82.release();
     for (int k = 0; k < ve_ctx::kStaging; k++) {
         if (c->h_views[k]) cudaFreeHost(c->h_views[k]);
         if (c->staging_ev[k]) cudaEventDestroy(c->staging_ev[k]);
@@ -4130,7 +4147,7 @@ int ve_split_resolve(ve_ctx* c, const ve_view* view, ve_frame_outputs* out) {
     a.mats = c->d_mats.p;
     a.gbuf = c->gbuf.p;
     a.out_vid = c->out_vid.p; a.out_node = c->out_node.p;
-    a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p;
+    a.out_rgb = c->out_rgb.p; a.out_mapped = c->out_mapped.p; a.out_mapped8 = c->out_m8.p;
     k_resolve<<<tiles, 256, 0, st>>>(a);
     VE_CUDA(cudaGetLastError());
     uint64_t d2h = 0;
@@ -4141,6 +4158,7 @@ int ve_split_resolve(ve_ctx* c, const ve_view* view, ve_frame_outputs* out) {
         if (out->hit_node) { VE_CUDA(cudaMemcpyAsync(out->hit_node + r0, c->out_node.p + r0, nr * 4, cudaMemcpyDeviceToHost, st)); d2h += nr * 4; }
         if (out->rgb) { VE_CUDA(cudaMemcpyAsync(out->rgb + 3 * r0, c->out_rgb.p + 3 * r0, nr * 12, cudaMemcpyDeviceToHost, st)); d2h += nr * 12; }
         if (out->mapped) { VE_CUDA(cudaMemcpyAsync(out->mapped + 3 * r0, c->out_mapped.p + 3 * r0, nr * 12, cudaMemcpyDeviceToHost, st)); d2h += nr * 12; }
+        if (out->mapped8) { VE_CUDA(cudaMemcpyAsync(out->mapped8 + r0, c->out_m8.p + r0, nr * 4, cudaMemcpyDeviceToHost, st)); d2h += nr * 4; }
     }
     VE_CUDA(cudaStreamSynchronize(st));
     c->tot_h2d += sizeof(DevView);

@@ -98,7 +98,7 @@ def band_rows(height: int, rank: int, world: int) -> Tuple[int, int]:
     return height * rank // world, height * (rank + 1) // world
 
 
-_IMAGE_OUTPUTS = ("voxel_id", "hit_node", "rgb", "mapped")
+_IMAGE_OUTPUTS = ("voxel_id", "hit_node", "rgb", "mapped", "mapped8")
 _RENDER_OUTPUTS = ("gbuffer", "path_rgb")
 _RECORD_WORDS = 8  # ve_split_record: 8 x 32-bit words
 
@@ -128,17 +128,18 @@ class SplitFrame:
         self.last: Dict[str, object] = {}
 
     def _image(self, name: str, fc):
-        """A pinned full-size host image for output `name` (32-bit elements)."""
+        """A pinned full-size host image for output `name`."""
         import numpy as np
         import torch
 
         shape = {"voxel_id": (fc.height, fc.width), "hit_node": (fc.height, fc.width),
-                 "rgb": (fc.height, fc.width, 3), "mapped": (fc.height, fc.width, 3)}[name]
-        dtype = np.uint32 if name in ("voxel_id", "hit_node") else np.float32
+                 "rgb": (fc.height, fc.width, 3), "mapped": (fc.height, fc.width, 3),
+                 "mapped8": (fc.height, fc.width, 4)}[name]
+        dtype = {"voxel_id": np.uint32, "hit_node": np.uint32, "mapped8": np.uint8}.get(name, np.float32)
+        tdtype = {np.uint32: torch.int32, np.uint8: torch.uint8, np.float32: torch.float32}[dtype]
         t = self._images.get(name)
         if t is None or tuple(t.shape) != shape:
-            t = torch.empty(shape, dtype=torch.int32 if dtype == np.uint32 else torch.float32,
-                            pin_memory=torch.cuda.is_available())
+            t = torch.empty(shape, dtype=tdtype, pin_memory=torch.cuda.is_available())
             self._images[name] = t
         return t.numpy().view(dtype)
 
@@ -186,6 +187,9 @@ class SplitFrame:
 
         if self.dist is None:
             return image
+        if image.dtype == np.uint8 and image.shape[-1] == 4:  # RGBA8: one 32-bit element per pixel
+            flat = np.ascontiguousarray(image).view(np.uint32)[..., 0]
+            return self.gather_rows(flat, lo, hi, height).view(np.uint8).reshape(image.shape)
         rows = max(height * (k + 1) // self.world - height * k // self.world for k in range(self.world))
         band = np.zeros((rows,) + image.shape[1:], image.dtype)
         band[: hi - lo] = image[lo:hi]
