@@ -13,8 +13,10 @@
 //      all admitted requests at whatever bounce they are — so a request that
 //      arrives while others are on the GPU joins at the next pass;
 //   3. reads the per-slot counts of paths not yet deposited; a request whose
-//      count reached zero is resolved (AvgPass + tonemap over its pixels),
-//      copied to the caller's host buffers and released.
+//      count reached zero is resolved (AvgPass + tonemap over its pixels) on
+//      the render stream, and its images are copied to the caller's host
+//      buffers on the server's copy stream while the next steps render; its
+//      pool ranges and view slot are released once that copy has ended.
 // Scenes and their radiance caches stay resident in the context.  The
 // per-frame cache decay of ve_render does not apply: requests accumulate into
 // the persistent per-scene caches.
@@ -89,6 +91,7 @@ struct ServeRequest {
     uint32_t tiles_started = 0;  // tiles whose primary pass has been launched
     double t_submit = 0, t_admit = 0, t_done = 0;
     cudaEvent_t done_ev = nullptr;
+    ve_server* owner = nullptr;
 };
 
 inline double now_s() {
@@ -116,6 +119,8 @@ struct ve_server {
     uint32_t* h_remaining = nullptr;  // pinned
     unsigned long long* h_stats = nullptr;  // pinned copy of the context's per-kind ray counters
     ve::DevView* h_view = nullptr;    // pinned staging, one per slot
+    cudaStream_t copy_st = nullptr;   // output copies of finished requests
+    cudaEvent_t resolve_ev = nullptr; // the resolves the next copies wait for
     uint64_t step = 0;
     // stats
     uint64_t completed = 0, steps_run = 0, max_inflight = 0, admitted = 0, rays = 0;
@@ -131,6 +136,27 @@ static void serve_fail(ve_server* s, int code, const std::string& msg) {
     }
     s->stop = true;
     s->cv_done.notify_all();
+}
+
+// Host function on the copy stream after a finished request's output
+// copies: the request is done, its pool ranges and view slot return to the
+// free lists, and waiters (and an idle serve loop) are woken.  Runs on a
+// CUDA-internal thread: no CUDA calls, only the server's lock.
+static void CUDART_CB serve_copied(void* arg) {
+    ServeRequest* r = static_cast<ServeRequest*>(arg);
+    ve_server* s = r->owner;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->state = 3;
+        r->t_done = now_s();
+        s->pix_pool.release(r->pix_off, r->pixels);
+        s->path_pool.release(r->path_off, r->paths);
+        s->free_slots.push_back(r->slot);
+        s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+        s->completed++;
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
 }
 
 static FrameArgs serve_args(ve_server* s) {
@@ -161,12 +187,19 @@ static void serve_loop(ve_server* s) {
     cudaStream_t st = c->stream;
     constexpr uint32_t kRing = 16;  // counter slots per pass index (even: keeps the live ping-pong parity)
     for (;;) {
-        std::vector<ServeRequest*> admit;
+        std::vector<ServeRequest*> admit, run;  // run: requests with paths to trace or tiles to start
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (s->queue.empty() && s->active.empty()) {
-                if (s->stop) break;
-                s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+            // idle (or only output copies outstanding): wait for a request
+            // or for a copy to end
+            auto busy = [&] {
+                for (ServeRequest* r : s->active)
+                    if (r->state == 1) return true;
+                return false;
+            };
+            if (s->queue.empty() && !busy()) {
+                if (s->stop && s->active.empty()) break;
+                s->cv_work.wait(lk, [&] { return (s->stop && s->active.empty()) || !s->queue.empty(); });
                 if (s->stop && s->queue.empty() && s->active.empty()) break;
             }
             // 1. admission in arrival order while a slot is free; a request
@@ -200,6 +233,17 @@ static void serve_loop(ve_server* s) {
                 s->admitted++;
             }
             s->max_inflight = std::max<uint64_t>(s->max_inflight, s->active.size());
+            for (ServeRequest* r : s->active)
+                if (r->state == 1) run.push_back(r);
+        }
+        if (run.empty()) {
+            // queued requests that do not fit wait for copies to free pool space
+            std::unique_lock<std::mutex> lk(s->mu);
+            const uint64_t done0 = s->completed;
+            const size_t q0 = s->queue.size();
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(5),
+                                [&] { return s->stop || s->completed != done0 || s->queue.size() != q0; });
+            continue;
         }
         const uint32_t ps = uint32_t(s->step % kRing);
         // counters produced by this step's passes; the live count of slot
@@ -240,8 +284,8 @@ static void serve_loop(ve_server* s) {
         {
             const bool fifo = (s->cfg.flags & VE_SERVER_FIFO) != 0u;
             uint64_t budget = s->cfg.step_path_budget ? s->cfg.step_path_budget : (1ull << 23);
-            for (ServeRequest* r : s->active) {
-                if (r->state != 1 || r->tiles_started >= r->tiles) continue;
+            for (ServeRequest* r : run) {
+                if (r->tiles_started >= r->tiles) continue;
                 if (!fifo && budget == 0) break;
                 const uint64_t per_tile = 256ull * r->view.frame.spp;
                 const uint32_t left = r->tiles - r->tiles_started;
@@ -287,46 +331,35 @@ static void serve_loop(ve_server* s) {
             std::lock_guard<std::mutex> lk(s->mu);
             s->rays = s->h_stats[ST_RAYS_PRIMARY] + s->h_stats[ST_RAYS_BOUNCE] + s->h_stats[ST_RAYS_SHADOW];
             s->steps_run++;
-            for (size_t i = 0; i < s->active.size();) {
-                ServeRequest* r = s->active[i];
-                if (r->state == 1 && r->tiles_started == r->tiles && s->h_remaining[r->slot] == 0) {
+            for (ServeRequest* r : run) {
+                if (r->tiles_started == r->tiles && s->h_remaining[r->slot] == 0) {
                     r->state = 2;
                     finished.push_back(r);
                 }
-                i++;
             }
         }
+        // resolves on the render stream (before the next step's passes);
+        // the copies on the copy stream, overlapping the next steps
         for (ServeRequest* r : finished) {
             FrameArgs ar = a;
             ar.views = c->d_views.p + r->slot;
             ar.n_views = 1;
             ar.total_tiles = r->tiles;
             k_resolve<<<r->tiles, 256, 0, st>>>(ar);
-            const uint64_t np = r->pixels;
-            if (r->out_vid)
-                cudaMemcpyAsync(r->out_vid, c->out_vid.p + r->pix_off, np * 4, cudaMemcpyDeviceToHost, st);
-            if (r->out_rgb)
-                cudaMemcpyAsync(r->out_rgb, c->out_rgb.p + 3 * r->pix_off, np * 12, cudaMemcpyDeviceToHost, st);
-            cudaEventRecord(r->done_ev, st);
         }
         if (!finished.empty()) {
-            const cudaError_t e2 = cudaStreamSynchronize(st);
-            if (e2 != cudaSuccess) {
-                serve_fail(s, VE_ERR_CUDA, std::string("serve resolve: ") + cudaGetErrorString(e2));
-                return;
-            }
-            std::lock_guard<std::mutex> lk(s->mu);
-            const double t = now_s();
+            cudaEventRecord(s->resolve_ev, st);
+            cudaStreamWaitEvent(s->copy_st, s->resolve_ev, 0);
             for (ServeRequest* r : finished) {
-                r->state = 3;
-                r->t_done = t;
-                s->pix_pool.release(r->pix_off, r->pixels);
-                s->path_pool.release(r->path_off, r->paths);
-                s->free_slots.push_back(r->slot);
-                s->active.erase(std::find(s->active.begin(), s->active.end(), r));
-                s->completed++;
+                const uint64_t np = r->pixels;
+                if (r->out_vid)
+                    cudaMemcpyAsync(r->out_vid, c->out_vid.p + r->pix_off, np * 4, cudaMemcpyDeviceToHost, s->copy_st);
+                if (r->out_rgb)
+                    cudaMemcpyAsync(r->out_rgb, c->out_rgb.p + 3 * r->pix_off, np * 12, cudaMemcpyDeviceToHost,
+                                    s->copy_st);
+                cudaEventRecord(r->done_ev, s->copy_st);
+                cudaLaunchHostFunc(s->copy_st, serve_copied, r);
             }
-            s->cv_done.notify_all();
         }
     }
 }
@@ -356,7 +389,9 @@ int ve_server_create(ve_ctx* c, const ve_server_config* cfg, ve_server** out) {
     if (cudaMalloc(&s->d_remaining, 4ull * cfg->max_requests) != cudaSuccess ||
         cudaMallocHost(&s->h_remaining, 4ull * cfg->max_requests) != cudaSuccess ||
         cudaMallocHost(&s->h_view, sizeof(DevView) * cfg->max_requests) != cudaSuccess ||
-        cudaMallocHost(&s->h_stats, sizeof(unsigned long long) * ST_TOTAL) != cudaSuccess) {
+        cudaMallocHost(&s->h_stats, sizeof(unsigned long long) * ST_TOTAL) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->copy_st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->resolve_ev, cudaEventDisableTiming) != cudaSuccess) {
         ve_server_destroy(s);
         return fail(VE_ERR_NOMEM, "server_create: allocation failed");
     }
@@ -381,6 +416,7 @@ int ve_server_submit(ve_server* s, const ve_view* v, uint32_t* voxel_id_out, flo
         f.reconstruction_radius > 64)
         return fail(VE_ERR_INVALID, "server_submit: frame configuration out of range");
     ServeRequest* r = new ServeRequest();
+    r->owner = s;
     r->view = *v;
     r->out_vid = voxel_id_out;
     r->out_rgb = rgb_out;
@@ -472,6 +508,11 @@ int ve_server_destroy(ve_server* s) {
     if (s->h_remaining) cudaFreeHost(s->h_remaining);
     if (s->h_view) cudaFreeHost(s->h_view);
     if (s->h_stats) cudaFreeHost(s->h_stats);
+    if (s->copy_st) {
+        cudaStreamSynchronize(s->copy_st);
+        cudaStreamDestroy(s->copy_st);
+    }
+    if (s->resolve_ev) cudaEventDestroy(s->resolve_ev);
     const int err = s->error;
     delete s;
     return err;
