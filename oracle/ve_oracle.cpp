@@ -70,6 +70,8 @@ struct Scene {
     // ball-normal scenes: the 10-10-10 normal codes their leaves index
     const uint32_t* ncodes = nullptr;
     uint64_t n_ncodes = 0;
+    // box that bounce rays are clipped to (scene_clip_box); unbounded by default
+    float clip_lo[3] = {-1e30f, -1e30f, -1e30f}, clip_hi[3] = {1e30f, 1e30f, 1e30f};
     // texelFetch on a buffer texture: out-of-range reads return 0.
     uint32_t fetch(uint64_t off) const { return off < n ? words[off] : 0u; }
 };
@@ -104,7 +106,13 @@ struct RayCounters {
 // reports only hit-or-not.  `fetch_min` counts a node word only when it
 // differs from the word last read at the same descent level (the distinct
 // nodes along the ray's monotone DDA walk).
-Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc) {
+// clip: a bounce ray, for which leaving the volume and running out of
+// controlchecks shade alike (shade.comp:558-564), also ends — as having left
+// the volume — once its distance passes the exit of the scene's clip box
+// along its direction, where it can hit nothing more (scene_clip_box).  This
+// changes no result, only the walk the counters see; the device trace does
+// the same.
+Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc, bool clip = false) {
     const uint32_t D = s.depth;
     const uint32_t L = 1u << D;
     const float Lf = float(L);
@@ -119,6 +127,14 @@ Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc)
     o = add(o, muls(d, 4.0f));  // ray.origin += ray.direction * 4  (:361)
     uint32_t q = 0;
     f3 r;
+    float t = 0.0f;  // r = d * t + o
+    float t_end = 0.0f;
+    if (clip) {
+        const float tx = ((inv.x > 0.0f ? s.clip_hi[0] : s.clip_lo[0]) - o.x) * inv.x;
+        const float ty = ((inv.y > 0.0f ? s.clip_hi[1] : s.clip_lo[1]) - o.y) * inv.y;
+        const float tz = ((inv.z > 0.0f ? s.clip_hi[2] : s.clip_lo[2]) - o.z) * inv.z;
+        t_end = gmin(gmin(tx, ty), tz);
+    }
     if (in_bounds(o, Lf)) {
         r = o;
     } else {
@@ -135,8 +151,10 @@ Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc)
             return h;
         }
         r = add(muls(d, t_enter), o);
+        t = t_enter;
     }
-    while (in_bounds(r, Lf) && q++ <= controlchecks) {
+    bool clipped = false;
+    while (in_bounds(r, Lf) && !(clipped = clip && t > t_end) && q++ <= controlchecks) {
         if (rc) rc->steps++;
         const uint32_t ux = uint32_t(r.x), uy = uint32_t(r.y), uz = uint32_t(r.z);
         uint32_t off = 0, depth = 0, size = 0;
@@ -186,10 +204,71 @@ Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc)
         f3 tmx = mk(gmax(t1.x, t2.x), gmax(t1.y, t2.y), gmax(t1.z, t2.z));
         float t_exit = gmin(gmin(tmx.x, tmx.y), tmx.z);
         r = add(muls(d, t_exit), o);
+        t = t_exit;
     }
-    h.status = in_bounds(r, Lf) ? ST_TIMEOUT : ST_ESCAPED;
+    h.status = (in_bounds(r, Lf) && !clipped) ? ST_TIMEOUT : ST_ESCAPED;
     h.checks = q;
     return h;
+}
+
+// The box bounce rays are clipped to (a bound of this build, not of the
+// reference).  Levels 0..T0-1 (T0 = min(9, D - 1), none below depth 3) are
+// the device's top-table levels; a level-(T0-1) cell whose words at those
+// levels are all internal can end a descent on a material voxel, no other
+// in-range cell can (words above level D are never tested for a material).
+// The box of those cells, widened by one voxel, unless a position with a
+// coordinate equal to 2^D (which the bounds test admits; its level-0 read
+// goes to root words 1..7) ends on a material voxel: then, as for depths
+// above 12 where the faces are not searched, no box applies.
+void scene_clip_box(Scene& s) {
+    const uint32_t D = s.depth;
+    const uint32_t T0 = D < 3u ? 0u : std::min(9u, D - 1u);
+    if (T0 == 0 || D > 12) return;
+    const uint32_t L = 1u << D, sh = D - T0 + 1u;
+    uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+    struct C { uint32_t off, k, x, y, z; };
+    std::vector<C> st{{0u, 0u, 0u, 0u, 0u}};
+    while (!st.empty()) {
+        const C c = st.back();
+        st.pop_back();
+        const uint32_t raw = s.fetch(c.off);
+        if (!(raw & 1u)) continue;
+        if (c.k == T0 - 1u) {
+            const uint32_t v[3] = {c.x >> sh, c.y >> sh, c.z >> sh};
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], v[a]);
+                hi[a] = std::max(hi[a], v[a]);
+            }
+            continue;
+        }
+        const uint32_t next = node_next(raw), half = L >> (c.k + 1u);
+        for (uint32_t i = 0; i < 8; i++)
+            st.push_back({next + i, c.k + 1u, c.x + ((i & 4) ? half : 0u), c.y + ((i & 2) ? half : 0u),
+                          c.z + ((i & 1) ? half : 0u)});
+    }
+    // the faces {x, y or z = 2^D}: the descent of raycast at each integer position
+    for (uint32_t f = 0; f < 3; f++)
+        for (uint32_t u = 0; u <= L; u++)
+            for (uint32_t v = 0; v <= L; v++) {
+                const uint32_t x = f == 0 ? L : u, y = f == 1 ? L : (f == 0 ? u : v), z = f == 2 ? L : v;
+                uint32_t off = 0;
+                bool internal = true;
+                for (uint32_t k = 0; k < D && internal; k++) {
+                    const uint32_t raw = s.fetch(off + locate(x, y, z, L >> k));
+                    internal = node_is_node(raw);
+                    off = node_next(raw);
+                }
+                if (internal && node_material(s.fetch(off + locate(x, y, z, 1u))) != 0u) return;
+            }
+    for (int a = 0; a < 3; a++) {
+        if (lo[0] > hi[0]) {  // no cell can be hit: any box is exact
+            s.clip_lo[a] = -1.0f;
+            s.clip_hi[a] = 1.0f;
+        } else {
+            s.clip_lo[a] = float(lo[a] << sh) - 1.0f;
+            s.clip_hi[a] = float((hi[a] + 1u) << sh) + 1.0f;
+        }
+    }
 }
 
 // hash + voxelKey (internal.glsl:263-291)
@@ -960,7 +1039,7 @@ void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_
         tp = ntp;
         dir = sdir;
         b++;
-        hit = raycast(s, shading_point, sdir, P.bounce_controlchecks, rc);
+        hit = raycast(s, shading_point, sdir, P.bounce_controlchecks, rc, true);
         st->rays_bounce++;
     }
     out->direct = direct;
@@ -1425,10 +1504,9 @@ uint64_t oracle_fill_normals_ball(uint32_t* words, uint64_t n, uint32_t depth, u
     struct E { uint32_t off, level, x, y, z; };
     std::vector<E> leaves;
     std::vector<E> st;
-    for (uint32_t i = 0; i < 8; i++) {
-        const uint32_t half = L >> 1;
-        st.push_back({1u + i, 1u, (i & 4) ? half : 0u, (i & 2) ? half : 0u, (i & 1) ? half : 0u});
-    }
+    // from the root word (slot 0) through its child pointer, as every
+    // descent reads it (Octree::set puts the root's children at slots 1..8)
+    st.push_back({0u, 0u, 0u, 0u, 0u});
     while (!st.empty()) {
         E e = st.back();
         st.pop_back();
@@ -1657,6 +1735,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
     Scene s{words, n_words, depth};
     s.ncodes = R->ncodes.data();
     s.n_ncodes = R->ncodes.size();
+    scene_clip_box(s);
     const Material* mats = static_cast<const Material*>(materials);
     const uint32_t W = P->width, H = P->height;
     if (row_end == 0 || row_end > H) row_end = H;

@@ -462,11 +462,12 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                     f3 d = (e >> 31) ? mk(v.sun[0], v.sun[1], v.sun[2]) : ld3(a.p_ray_d[p]);
                     if (EM && (e >> 31) && (v.flags & VE_FRAME_EMISSIVE)) d = ld3(a.p_sdir[p]);
                     finished = dda_init(s, o, d, v.cc_bounce, D, h);
-                    if (!COUNT) {
+                    {
                         // a bounce ray that escapes or times out shades as
                         // sky alike, so it ends on leaving the box of the
                         // cells that can hold a voxel (exit of its slab);
-                        // shadow rays walk on (there a timeout is a shadow)
+                        // shadow rays walk on (there a timeout is a shadow).
+                        // Fetch-counting frames count this walk too.
                         float te = __int_as_float(0x7f800000);
                         if (!(e >> 31)) {
                             const float tx = ((s.inv.x > 0.0f ? S.clip_hi[0] : S.clip_lo[0]) - s.o.x) * s.inv.x;
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_step<COUNT, true, !COUNT>(s, nodes, n_words, D, top, T0, h, rc);
+            finished = dda_step<COUNT, true, true>(s, nodes, n_words, D, top, T0, h, rc);
             if (finished) active = false;
         }
         if (finished) {
