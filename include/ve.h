@@ -63,6 +63,17 @@ extern "C" {
                                      ve_ctx_synchronize */
 #define VE_CFG_NO_GRAPHS 1u       /* renderer config: enqueue kernels directly instead of
                                      replaying a CUDA graph of the frame's kernel sequence */
+#define VE_CFG_PIPELINE 2u        /* renderer config: consecutive frames alternate between two sets of
+                                     frame buffers on two streams, so that a frame's primary pass and
+                                     first trace pass run while the previous frame finishes (its
+                                     radiance-cache work still follows the previous frame's).  Applies
+                                     to plain frames whose views all have bounces >= 1 and none of the
+                                     flags TIMING, COUNT_FETCH, PATH_RGB, SCHEDULED, EMISSIVE, LBUFFER,
+                                     LEARNED, TRAIN, TERMINATE_HASH, SPLIT; other frames and every other
+                                     call on the context run after the frames in flight.  Costs a
+                                     second copy of the path state.  Work the caller enqueues on the
+                                     context's stream is ordered after pipelined frames only after
+                                     ve_ctx_join (or any other call on the context). */
 
 /* RendererConfig (src/renderer/core.hpp:30-42) plus device sizing.  The
  * radiance cache replaces the lBuffer hash image (renderer.cpp:27-40):
@@ -239,6 +250,9 @@ int ve_ctx_destroy(ve_ctx* ctx);
 /* the context's cudaStream_t, for callers that time or order work on it */
 int ve_ctx_stream(ve_ctx* ctx, void** stream);
 int ve_ctx_synchronize(ve_ctx* ctx);
+/* Orders work enqueued on the context's stream after this call behind every
+ * frame rendered so far (VE_CFG_PIPELINE runs some on a second stream). */
+int ve_ctx_join(ve_ctx* ctx);
 
 /* Octree::set upload (octree.cpp:157-159 glBufferData of Octree::data):
  * `words` verbatim in the reference layout.  Unless VE_SCENE_KEEP_NORMALS,

@@ -57,6 +57,7 @@ RESTIR_TEMPORAL = 2
 RESTIR_SPATIAL = 4
 RAYCAST_FULL_WALK = 1
 CFG_NO_GRAPHS = 1
+CFG_PIPELINE = 2
 SERVER_FIFO = 1
 
 
@@ -187,6 +188,7 @@ _SIGNATURES = {
     "ve_ctx_destroy": ([_P], ctypes.c_int),
     "ve_ctx_stream": ([_P, _PTR(_P)], ctypes.c_int),
     "ve_ctx_synchronize": ([_P], ctypes.c_int),
+    "ve_ctx_join": ([_P], ctypes.c_int),
     "ve_scene_upload": ([_P, _P, _U64, _U32, _U32, _PTR(_I32)], ctypes.c_int),
     "ve_scene_release": ([_P, _I32], ctypes.c_int),
     "ve_scene_apply_edits": ([_P, _I32, _P, _P, _U64, _U32], ctypes.c_int),
@@ -552,9 +554,11 @@ def _image_outputs(fc: FrameConfig, arrays: Dict[str, np.ndarray]) -> "FrameOutp
 class Renderer:
     """The device renderer (one CUDA context stream, owned device memory)."""
 
-    def __init__(self, device: int = 0, hash_log2: int = 22, hash_probes: int = 64, graphs: bool = True):
+    def __init__(self, device: int = 0, hash_log2: int = 22, hash_probes: int = 64, graphs: bool = True,
+                 pipeline: bool = False):
         self._lib = load_library()
-        cfg = RendererConfigC(device, hash_log2, hash_probes, 0 if graphs else CFG_NO_GRAPHS)
+        cfg = RendererConfigC(device, hash_log2, hash_probes,
+                              (0 if graphs else CFG_NO_GRAPHS) | (CFG_PIPELINE if pipeline else 0))
         h = _P()
         _check(self._lib.ve_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -586,6 +590,11 @@ class Renderer:
 
     def synchronize(self) -> None:
         _check(self._lib.ve_ctx_synchronize(self._h))
+
+    def join(self) -> None:
+        """Orders work enqueued on `stream` from now on behind every frame
+        rendered so far (pipelined frames run partly on a second stream)."""
+        _check(self._lib.ve_ctx_join(self._h))
 
     def upload_scene(self, words: np.ndarray, depth: int, keep_normals: bool = False) -> int:
         w = np.ascontiguousarray(words, np.uint32)

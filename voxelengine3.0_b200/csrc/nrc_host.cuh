@@ -424,6 +424,7 @@ int ve_nrc_stats(ve_nrc* m, float* loss, uint64_t* samples, uint64_t* steps) {
 }
 
 int ve_scene_set_nrc(ve_ctx* c, int scene_id, ve_nrc* m) {
+    if (c) ve::join_alt(c);  // after the second frame set's frames in flight
     using namespace ve;
     if (!c) return fail(VE_ERR_INVALID, "scene_set_nrc: null context");
     if (scene_id < 0 || size_t(scene_id) >= c->scenes.size() || !c->scenes[scene_id].live)

@@ -2003,6 +2003,19 @@ struct DevBuf {
 
 }  // namespace ve
 
+// The buffers a plain frame's passes own, for the second of the two sets
+// that pipelined frames (VE_CFG_PIPELINE) alternate between; the first set is
+// the context's own members of the same names.
+struct FrameSet {
+    cudaStream_t stream = nullptr;
+    ve::DevBuf<ve::DevView> d_views;
+    ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
+    ve::DevBuf<uint4> p_hit, p_meta, gbuf;
+    ve::DevBuf<uint32_t> live0, live1, rayq, counters;
+    ve::DevBuf<unsigned long long> stats;
+    unsigned long long* h_stats = nullptr;  // pinned
+};
+
 struct ve_ctx {
     int device = 0;
     int num_sms = 148;
@@ -2054,6 +2067,18 @@ struct ve_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t frame_done = nullptr, copy_done[2] = {};
     int out_parity = 0;
+    // VE_CFG_PIPELINE: the second frame set and the order between the sets.
+    // A pipelined frame's primary and first trace pass touch only its own
+    // set, so they run while the other set's frame finishes; its cache work
+    // (decay, deposits, AvgPass) waits for that frame's (set_cache_done).
+    FrameSet alt;
+    int pipe_next = 0;           // set of the next pipelined frame
+    int last_set = 0;            // set that rendered the last frame (its stats)
+    bool alt_busy = false;       // work of the second set may be in flight
+    bool ops_pending = false;    // main-stream work enqueued since the last second-set frame
+    cudaEvent_t set_cache_done[2] = {};  // end of each set's last frame's cache work
+    cudaEvent_t alt_done = nullptr;      // end of the last second-set frame
+    cudaEvent_t ops_ev = nullptr;        // main-stream point a second-set frame waits for
     ve::DevBuf<float4> p_sdir;          // emissive batches: NEE shadow directions + light vid
     ve::DevBuf<ve::PathRes> p_res;      // emissive batches: bounce-0 reservoirs until the commit
     ve::DevBuf<uint32_t> res_list;      // ... and the paths that hold one
@@ -2120,6 +2145,7 @@ static int set_frame_infer_attributes() {
     return VE_OK;
 }
 }  // namespace nrc
+static void join_alt(ve_ctx* c);
 }  // namespace ve
 
 #include "nrc_host.cuh"
@@ -2524,6 +2550,45 @@ static int reset_rank(ve_ctx* c, float* rank) {
     return VE_OK;
 }
 
+// Exchanges the context's first-set frame buffers (and stream) with the
+// second set's: while swapped, the frame code's c->... members are set 1.
+static void swap_set(ve_ctx* c) {
+    FrameSet& a = c->alt;
+    std::swap(c->stream, a.stream);
+    std::swap(c->d_views, a.d_views);
+    std::swap(c->p_ray_o, a.p_ray_o); std::swap(c->p_ray_d, a.p_ray_d); std::swap(c->p_tp, a.p_tp);
+    std::swap(c->p_direct, a.p_direct); std::swap(c->p_indirect, a.p_indirect); std::swap(c->p_pend, a.p_pend);
+    std::swap(c->p_hit, a.p_hit); std::swap(c->p_meta, a.p_meta); std::swap(c->gbuf, a.gbuf);
+    std::swap(c->live0, a.live0); std::swap(c->live1, a.live1); std::swap(c->rayq, a.rayq);
+    std::swap(c->counters, a.counters);
+    std::swap(c->stats, a.stats);
+    std::swap(c->h_stats, a.h_stats);
+}
+
+// Set 1 swapped in for the scope (a frame of the second set).
+struct SetScope {
+    ve_ctx* c;
+    bool on;
+    SetScope(ve_ctx* cc, bool use) : c(cc), on(use) {
+        if (on) swap_set(c);
+    }
+    ~SetScope() {
+        if (on) swap_set(c);
+    }
+};
+
+// Orders work enqueued next on the main stream after every second-set frame
+// in flight, and the next second-set frame after that work.  Every entry
+// point that enqueues on the context's stream, other than a pipelined frame,
+// calls it first.
+static void join_alt(ve_ctx* c) {
+    if (c->alt_busy) {
+        cudaStreamWaitEvent(c->stream, c->alt_done, 0);
+        c->alt_busy = false;
+    }
+    c->ops_pending = true;
+}
+
 static int ensure_frame(ve_ctx* c, uint64_t pixels, uint64_t paths, uint32_t n_views) {
     int rc = 0;
     const void* before[] = {c->gbuf.p, c->out_vid.p, c->out_node.p, c->out_rgb.p, c->out_mapped.p, c->out_m8.p,
@@ -2697,10 +2762,11 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "render: no views");
     if (nv > 65535u) return fail(VE_ERR_INVALID, "render: at most 65535 views per batch");
     uint64_t pixels = 0, paths = 0;
-    uint32_t tiles = 0, max_b = 0, flags = 0;
+    uint32_t tiles = 0, max_b = 0, min_b = ~0u, flags = 0;
     for (uint32_t i = 0; i < nv; i++) {
         const ve_view& v = views[i];
         const ve_frame_config& f = v.frame;
+        min_b = std::min(min_b, f.bounces);
         if (v.scene_id < 0 || size_t(v.scene_id) >= c->scenes.size() || !c->scenes[v.scene_id].live)
             return fail(VE_ERR_NOT_FOUND, "render: unknown scene id " + std::to_string(v.scene_id));
         if (f.width == 0 || f.height == 0 || f.width > 16384 || f.height > 16384)
@@ -2762,6 +2828,38 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         if (!m) return fail(VE_ERR_STATE, "render: VE_FRAME_LEARNED / VE_FRAME_TRAIN on a scene without a learned cache");
         if (nrc && m != nrc) return fail(VE_ERR_INVALID, "render: at most one learned cache per batch");
         nrc = m;
+    }
+    // VE_CFG_PIPELINE: plain frames whose primary pass takes no path to a
+    // deposit (every view has a bounce) alternate between the two frame sets;
+    // anything else runs on the main stream after the second set's frames
+    const bool pipe = (c->cfg.flags & VE_CFG_PIPELINE) && !split && min_b >= 1 && !c->scenes_dirty &&
+                      !(flags & (VE_FRAME_TIMING | VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
+                                 VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED | VE_FRAME_EMISSIVE |
+                                 VE_FRAME_LBUFFER));
+    if (!pipe) join_alt(c);
+    const int set = pipe ? c->pipe_next : 0;
+    if (pipe) {
+        if (!c->alt.stream) {
+            if (cudaStreamCreateWithFlags(&c->alt.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->set_cache_done[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->set_cache_done[1], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->alt_done, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->ops_ev, cudaEventDisableTiming) != cudaSuccess)
+                return fail(VE_ERR_CUDA, "render: frame-set stream creation failed");
+        }
+        if (!c->alt.h_stats && cudaMallocHost(&c->alt.h_stats, ST_TOTAL * sizeof(unsigned long long)) != cudaSuccess)
+            return fail(VE_ERR_NOMEM, "render: frame-set allocation failed");
+        c->pipe_next ^= 1;
+    }
+    SetScope scope(c, set == 1);  // c->stream and the frame buffers are this set's from here on
+    if (set == 1) {
+        if (int e = c->counters.ensure(CNT_TOTAL)) return e;
+        if (int e = c->stats.ensure(ST_TOTAL)) return e;
+        if (c->ops_pending) {  // main-stream work since this set's last frame comes first
+            VE_CUDA(cudaEventRecord(c->ops_ev, c->alt.stream));
+            VE_CUDA(cudaStreamWaitEvent(c->stream, c->ops_ev, 0));
+            c->ops_pending = false;
+        }
     }
     int rc = ensure_frame(c, pixels, paths, nv);
     if (rc) return rc;
@@ -3001,7 +3099,21 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     const bool nrcm = (flags & (VE_FRAME_LEARNED | VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN)) != 0;
     const int mode = (em ? kModeEm : 0) | (lbm ? kModeLb : 0) | (nrcm ? kModeNrc : 0);
     // the frame's kernel sequence (no host synchronisation inside)
-    auto enqueue = [&]() {
+    // part 0: the whole frame; a pipelined frame runs as part 1 (primary and
+    // trace pass 0, which read no radiance cache) and part 2 (the decay and
+    // everything after), with the wait for the other set's cache work between
+    auto decay = [&]() {
+        for (auto& d : decays) {
+            if (d.second != 1.0f) {
+                const uint32_t n = 1u << c->cfg.hash_log2;
+                k_decay<<<c->num_sms * 8, 256, 0, st>>>(c->scenes[d.first].cache, n, d.second);
+                launches++;
+            }
+        }
+    };
+    auto enqueue = [&](int part) {
+        const bool head = part != 2, tail = part != 1;
+        if (head) {
         cudaMemsetAsync(c->counters.p, 0, CNT_TOTAL * sizeof(uint32_t), st);
         cudaMemsetAsync(c->stats.p, 0, ST_TOTAL * sizeof(unsigned long long), st);
         // paths of pixels without a primary hit are never spawned: their
@@ -3010,13 +3122,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         // lBuffer frames: row 0 (no deposit) for paths that are never spawned
         if (lbm) cudaMemsetAsync(c->lb_keys.p, 0, paths * sizeof(uint32_t), st);
         rec();
-        for (auto& d : decays) {
-            if (d.second != 1.0f) {
-                const uint32_t n = 1u << c->cfg.hash_log2;
-                k_decay<<<c->num_sms * 8, 256, 0, st>>>(c->scenes[d.first].cache, n, d.second);
-                launches++;
-            }
-        }
+        if (part == 0) decay();
         rec();
         if (count) launch_primary<true>(mode, tiles, st, a);
         else launch_primary<false>(mode, tiles, st, a);
@@ -3037,7 +3143,9 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             launches += 6;
         }
         rec();
-        for (uint32_t pass = 0; pass <= max_b + 1u; pass++) {
+        }
+        if (part == 2) decay();
+        for (uint32_t pass = head ? 0u : 1u; pass <= (tail ? max_b + 1u : 0u); pass++) {
             if (pass > 0) {  // pass 0 runs inside the fused primary
                 launch_shade(mode, shade_grid(c, mode, false), st, a, pass);
                 launches++;
@@ -3056,6 +3164,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             }
             rec();
         }
+        if (!tail) return;
         if (learned || train) {
             if (learned) {
                 nrc::launch_infer(nrc, st, nrc::infer_args(nrc, nrc->fq.p, c->counters.p + CNT_NRC_Q, a.nq_cap),
@@ -3118,9 +3227,13 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     // this frame's resolve overwrites an image set whose copy may be pending
     if (c->copy_stream) VE_CUDA(cudaStreamWaitEvent(st, c->copy_done[parity], 0));
     const bool use_graph = !timing && !(c->cfg.flags & VE_CFG_NO_GRAPHS);
-    if (!use_graph) {
-        enqueue();
-    } else {
+    // one part of the frame: enqueued directly, or as the replay of its
+    // cached CUDA graph (captured on first use)
+    auto run = [&](int part) -> int {
+        if (!use_graph) {
+            enqueue(part);
+            return VE_OK;
+        }
         std::vector<uint64_t> key = {c->gen, nv, tiles, max_b,
                                      flags & (VE_FRAME_COUNT_FETCH | VE_FRAME_PATH_RGB | VE_FRAME_LEARNED |
                                               VE_FRAME_TERMINATE_HASH | VE_FRAME_TRAIN | VE_FRAME_SCHEDULED |
@@ -3135,13 +3248,15 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         for (int sc : em_scenes) key.push_back((1ull << 62) | uint64_t(uint32_t(sc)));
         key.push_back((1ull << 61) | uint64_t(parity));
+        key.push_back((1ull << 60) | (uint64_t(set) << 8) | uint64_t(part));
         ve_ctx::GraphEntry* ge = nullptr;
         for (auto& g : c->graphs)
             if (g.key == key) ge = &g;
         if (!ge) {
+            const uint32_t l0 = launches, t0 = trace_launches;
             cudaGraph_t graph = nullptr;
             VE_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            enqueue();
+            enqueue(part);
             const cudaError_t ce = cudaStreamEndCapture(st, &graph);
             if (ce != cudaSuccess) return fail(VE_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
             cudaGraphExec_t exec = nullptr;
@@ -3157,18 +3272,28 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
             ve_ctx::GraphEntry e;
             e.key = key;
             e.exec = exec;
-            e.launches = launches;
-            e.trace_launches = trace_launches;
+            e.launches = launches - l0;
+            e.trace_launches = trace_launches - t0;
             c->graphs.push_back(e);
             ge = &c->graphs.back();
             c->graph_captures++;
         } else {
-            launches = ge->launches;
-            trace_launches = ge->trace_launches;
+            launches += ge->launches;
+            trace_launches += ge->trace_launches;
             c->graph_replays++;
         }
         ge->last_use = ++c->graph_clock;
         VE_CUDA(cudaGraphLaunch(ge->exec, st));
+        return VE_OK;
+    };
+    if (!pipe) {
+        if ((rc = run(0))) return rc;
+    } else {
+        if ((rc = run(1))) return rc;
+        // the other set's frame: its deposits and AvgPass before this decay
+        VE_CUDA(cudaStreamWaitEvent(st, c->set_cache_done[set ^ 1], 0));
+        if ((rc = run(2))) return rc;
+        VE_CUDA(cudaEventRecord(c->set_cache_done[set], st));
     }
     VE_CUDA(cudaGetLastError());
     c->last_launches = launches;
@@ -3239,6 +3364,11 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         VE_CUDA(cudaStreamSynchronize(st));
     }
+    if (set == 1) {
+        VE_CUDA(cudaEventRecord(c->alt_done, st));
+        c->alt_busy = true;
+    }
+    c->last_set = set;
     c->last_h2d = h2d;
     c->last_d2h = d2h;
     c->tot_frames++;
@@ -3477,6 +3607,21 @@ int ve_ctx_destroy(ve_ctx* c) {
     }
     c->totals.release();
     if (c->h_stats) cudaFreeHost(c->h_stats);
+    {
+        FrameSet& a = c->alt;
+        if (a.stream) {
+            cudaStreamSynchronize(a.stream);
+            cudaStreamDestroy(a.stream);
+        }
+        a.d_views.release(); a.p_ray_o.release(); a.p_ray_d.release(); a.p_tp.release(); a.p_direct.release();
+        a.p_indirect.release(); a.p_pend.release(); a.p_hit.release(); a.p_meta.release(); a.gbuf.release();
+        a.live0.release(); a.live1.release(); a.rayq.release(); a.counters.release(); a.stats.release();
+        if (a.h_stats) cudaFreeHost(a.h_stats);
+        for (auto& e : c->set_cache_done)
+            if (e) cudaEventDestroy(e);
+        if (c->alt_done) cudaEventDestroy(c->alt_done);
+        if (c->ops_ev) cudaEventDestroy(c->ops_ev);
+    }
     for (auto& slot : c->timing)
         for (auto& e : slot.ev)
             if (e) cudaEventDestroy(e);
@@ -3493,9 +3638,17 @@ int ve_ctx_stream(ve_ctx* c, void** stream) {
     return VE_OK;
 }
 
+int ve_ctx_join(ve_ctx* c) {
+    if (!c) return fail(VE_ERR_INVALID, "ctx_join: null context");
+    if (c->alt_busy) VE_CUDA(cudaStreamWaitEvent(c->stream, c->alt_done, 0));
+    c->alt_busy = false;
+    return VE_OK;
+}
+
 int ve_ctx_synchronize(ve_ctx* c) {
     if (!c) return fail(VE_ERR_INVALID, "ctx_synchronize: null context");
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->alt.stream) VE_CUDA(cudaStreamSynchronize(c->alt.stream));
     if (c->copy_stream) VE_CUDA(cudaStreamSynchronize(c->copy_stream));
     return VE_OK;
 }
@@ -3666,6 +3819,7 @@ extern "C" {
 
 int ve_scene_build(ve_ctx* c, const uint32_t* xyzm, uint64_t n, uint32_t depth, uint32_t flags, int32_t* scene_id,
                    uint64_t* n_words) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || (!xyzm && n) || !scene_id) return fail(VE_ERR_INVALID, "scene_build: null argument");
     if (depth < 1 || depth > 16) return fail(VE_ERR_INVALID, "scene_build: depth must be in [1, 16]");
     if (n >= (1ull << 32)) return fail(VE_ERR_CAPACITY, "scene_build: at most 2^32 - 1 voxels");
@@ -3722,6 +3876,7 @@ int ve_scene_build(ve_ctx* c, const uint32_t* xyzm, uint64_t n, uint32_t depth, 
 
 int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t depth, uint32_t flags,
                     int32_t* scene_id) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || !words || !scene_id) return fail(VE_ERR_INVALID, "scene_upload: null argument");
     if (n_words < 9) return fail(VE_ERR_INVALID, "scene_upload: a node array has at least 9 words");
     if (depth < 1 || depth > 16) return fail(VE_ERR_INVALID, "scene_upload: depth must be in [1, 16]");
@@ -3775,6 +3930,7 @@ int ve_scene_upload(ve_ctx* c, const uint32_t* words, uint64_t n_words, uint32_t
 }
 
 int ve_scene_release(ve_ctx* c, int32_t id) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_release: unknown scene");
     cudaSetDevice(c->device);
@@ -3795,6 +3951,7 @@ int ve_scene_release(ve_ctx* c, int32_t id) {
 
 int ve_scene_apply_edits(ve_ctx* c, int32_t id, const uint32_t* slots, const uint32_t* words, uint64_t n,
                          uint32_t flags) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_apply_edits: unknown scene");
     if (n && (!slots || !words)) return fail(VE_ERR_INVALID, "scene_apply_edits: null arrays");
@@ -3822,6 +3979,7 @@ int ve_scene_apply_edits(ve_ctx* c, int32_t id, const uint32_t* slots, const uin
 }
 
 int ve_scene_refresh(ve_ctx* c, int32_t id, const uint32_t* xyz, uint64_t n, uint32_t flags) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_refresh: unknown scene");
     if (n && !xyz) return fail(VE_ERR_INVALID, "scene_refresh: null positions");
@@ -3848,6 +4006,7 @@ int ve_scene_refresh(ve_ctx* c, int32_t id, const uint32_t* xyz, uint64_t n, uin
 }
 
 int ve_scene_normal_mode(ve_ctx* c, int32_t id, uint32_t radius) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_normal_mode: unknown scene");
     if (radius > VE_NORMAL_BALL_MAX_RADIUS)
@@ -3861,6 +4020,7 @@ int ve_scene_normal_mode(ve_ctx* c, int32_t id, uint32_t radius) {
 }
 
 int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t* n_words) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "scene_download: unknown scene");
     SceneSlot& s = c->scenes[id];
@@ -3875,6 +4035,7 @@ int ve_scene_download(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64
 // ve_raycast_batch: rays from host memory through k_raycast_batch.
 int ve_raycast_batch(ve_ctx* c, int32_t id, const float* origins, const float* dirs, uint64_t n,
                      uint32_t controlchecks, uint32_t flags, uint32_t* out) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "raycast_batch: unknown scene");
     if (n == 0) return VE_OK;
@@ -3922,6 +4083,7 @@ int ve_scene_clip_box(ve_ctx* c, int32_t id, float lo[3], float hi[3], uint32_t*
 }
 
 int ve_set_materials(ve_ctx* c, const void* entries, uint32_t n) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || (!entries && n)) return fail(VE_ERR_INVALID, "set_materials: null argument");
     if (n > 128) return fail(VE_ERR_CAPACITY, "set_materials: at most 128 materials");
     std::vector<DevMaterial> m(128);
@@ -3942,6 +4104,7 @@ int ve_set_materials(ve_ctx* c, const void* entries, uint32_t n) {
 }
 
 int ve_cache_reset(ve_ctx* c, int32_t id) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "cache_reset: unknown scene");
     VE_CUDA(cudaMemsetAsync(c->scenes[id].cache, 0, sizeof(CacheEntry) << c->cfg.hash_log2, c->stream));
@@ -3961,6 +4124,7 @@ int ve_cache_reset(ve_ctx* c, int32_t id) {
 }
 
 int ve_lbuffer_dump(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t* n) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "lbuffer_dump: unknown scene");
     const SceneSlot& s = c->scenes[id];
@@ -3987,6 +4151,7 @@ int ve_lbuffer_dump(ve_ctx* c, int32_t id, uint32_t* out, uint64_t cap, uint64_t
 }
 
 int ve_cache_dump(ve_ctx* c, int32_t id, uint32_t* vids, uint32_t* counts, float* values, uint64_t cap, uint64_t* n) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || id < 0 || size_t(id) >= c->scenes.size() || !c->scenes[id].live)
         return fail(VE_ERR_NOT_FOUND, "cache_dump: unknown scene");
     const size_t N = size_t(1) << c->cfg.hash_log2;
@@ -4066,6 +4231,7 @@ static int split_scene_ok(ve_ctx* c, int32_t id, const char* what) {
 }
 
 int ve_split_export(ve_ctx* c, int32_t id, void* dev_out, uint64_t cap, uint64_t* n) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (int rc = split_scene_ok(c, id, "split_export")) return rc;
     if (!n) return fail(VE_ERR_INVALID, "split_export: null count");
     cudaSetDevice(c->device);
@@ -4087,6 +4253,7 @@ int ve_split_export(ve_ctx* c, int32_t id, void* dev_out, uint64_t cap, uint64_t
 
 int ve_split_merge(ve_ctx* c, int32_t id, const void* dev_parts, const uint64_t* counts, uint32_t n_parts,
                    uint64_t stride, uint64_t* dropped) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (int rc = split_scene_ok(c, id, "split_merge")) return rc;
     if (n_parts && !counts) return fail(VE_ERR_INVALID, "split_merge: null counts");
     // bounds that keep part offsets (k * stride records) far from overflow
@@ -4121,6 +4288,7 @@ int ve_split_merge(ve_ctx* c, int32_t id, const void* dev_parts, const uint64_t*
 }
 
 int ve_split_resolve(ve_ctx* c, const ve_view* view, ve_frame_outputs* out) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || !view) return fail(VE_ERR_INVALID, "split_resolve: null argument");
     if (int rc = split_scene_ok(c, view->scene_id, "split_resolve")) return rc;
     const ve_frame_config& f = view->frame;
@@ -4182,6 +4350,7 @@ int ve_set_launch_config(ve_ctx* c, const ve_launch_config* cfg) {
 }
 
 int ve_autotune(ve_ctx* c, const ve_view* views, uint32_t nv, uint32_t frames, ve_launch_config* best) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c || !views || nv == 0) return fail(VE_ERR_INVALID, "autotune: no views");
     if (frames == 0) frames = 2;
     cudaSetDevice(c->device);
@@ -4258,6 +4427,7 @@ static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
 int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
     if (!c || !s) return fail(VE_ERR_INVALID, "get_total_stats: null argument");
     unsigned long long h[ST_TOTAL];
+    if (c->alt.stream) VE_CUDA(cudaStreamSynchronize(c->alt.stream));  // the second set's totals
     VE_CUDA(cudaMemcpyAsync(h, c->totals.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
     collect_all_timing(c);
@@ -4277,6 +4447,7 @@ int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {
 }
 
 int ve_reset_total_stats(ve_ctx* c) {
+    if (c) join_alt(c);  // after the second frame set's frames in flight
     if (!c) return fail(VE_ERR_INVALID, "reset_total_stats: null context");
     VE_CUDA(cudaMemsetAsync(c->totals.p, 0, ST_TOTAL * sizeof(unsigned long long), c->stream));
     VE_CUDA(cudaStreamSynchronize(c->stream));
@@ -4291,9 +4462,10 @@ int ve_reset_total_stats(ve_ctx* c) {
 int ve_get_stats(ve_ctx* c, ve_frame_stats* s) {
     if (!c || !s) return fail(VE_ERR_INVALID, "get_stats: null argument");
     VE_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->alt.stream) VE_CUDA(cudaStreamSynchronize(c->alt.stream));
     collect_all_timing(c);
     ve_frame_stats r = c->last;
-    const unsigned long long* h = c->h_stats;
+    const unsigned long long* h = c->last_set == 1 ? c->alt.h_stats : c->h_stats;  // the last frame's set
     fill_counters(r, h);
     r.frames = 1;
     r.h2d_bytes = c->last_h2d;

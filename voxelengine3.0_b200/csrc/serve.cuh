@@ -369,6 +369,7 @@ static void serve_loop(ve_server* s) {
 extern "C" {
 
 int ve_server_create(ve_ctx* c, const ve_server_config* cfg, ve_server** out) {
+    if (c) ve::join_alt(c);  // after the second frame set's frames in flight
     using namespace ve;
     if (!c || !cfg || !out) return fail(VE_ERR_INVALID, "server_create: null argument");
     if (cfg->max_requests == 0 || cfg->max_requests > 4096)
