@@ -273,7 +273,7 @@ def run_batching(args, rank, world):
         scene_words.append((w, depth, nv))
     results = {}
     for mode in ("batched", "per_view"):
-        r = ve.Renderer(device=local, hash_log2=22, graphs=(mode == "batched"))
+        r = ve.Renderer(device=local, hash_log2=22, graphs=(mode == "batched"), pipeline=not args.no_pipeline)
         r.set_materials(ve.terrain_materials(1))
         sids = [r.upload_scene(w, d) for w, d, _ in scene_words]
         views = []
@@ -303,6 +303,7 @@ def run_batching(args, rank, world):
         e0.record(stream)
         for _ in range(args.steps):
             frame()
+        r.join()  # the end event follows the second frame set's stream too
         e1.record(stream)
         e1.synchronize()
         ms = vd.max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
@@ -321,6 +322,7 @@ def run_batching(args, rank, world):
                                        "spp 1-8, bounces 1-4, 4 octrees depth 8/9/10/10",
                            "pixels": int(sum(v["width"] * v["height"] for v in vs))},
                 "batched": results["batched"], "per_view_plain": results["per_view"],
+                "frame_pipeline": not args.no_pipeline,
                 "speedup_vs_per_view": results["batched"]["mrays_s"] / results["per_view"]["mrays_s"]}
         print(json.dumps(line), flush=True)
     vd.shutdown(dist)
@@ -933,7 +935,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-pipeline", action="store_true", help="large: render the frames unpipelined")
+    ap.add_argument("--no-pipeline", action="store_true", help="large, batching: render the frames unpipelined")
     ap.add_argument("--workload", choices=["large", "batching", "serving", "learned", "scheduled", "emissive", "lbuffer", "build",
                                                   "split"], default="large")
     ap.add_argument("--train-frames", type=int, default=48, help="learned: online training frames")
