@@ -1056,7 +1056,7 @@ def main():
     for i in range(K):
         r.render(sid, cam_list[i], frame_config(ve, W, frame(Wm + i), ve.FRAME_COUNT_FETCH), outputs=())
     cnt = r.total_stats()
-    trace_rays = cnt["rays_bounce"] + cnt["rays_shadow"]
+    trace_rays = cnt["rays_bounce"] + cnt["rays_shadow"] - cnt["shadow_shared"]  # traversals the kernel ran
     trace_bytes = 4.0 * cnt["fetch_nodes_trace"] + 48.0 * trace_rays
     trace_ms = ttot["ms_trace"]
     launches = ttot["trace_launches"]
@@ -1118,6 +1118,10 @@ def main():
             "config": large_config(nv, words.size),
             "rays_per_step": rays_of(tot) / K,
             "ray_mix_per_step": {k: tot[k] / K for k in ("rays_primary", "rays_bounce", "rays_shadow")},
+            # rays_shadow counts every path's sun shadow ray; the samples of a
+            # pixel share their first one (same origin and direction), traced once
+            "shadow_rays_shared_per_step": tot["shadow_shared"] / K,
+            "traced_rays_per_step": (rays_of(tot) - tot["shadow_shared"]) / K,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": etot["h2d_bytes"] / K,
                     "d2h_bytes_per_step": etot["d2h_bytes"] / K,
                     "outputs": "the displayed RGBA8 image (final.frag's framebuffer store), pinned host memory"},

@@ -183,6 +183,9 @@ typedef struct ve_frame_stats {
     uint64_t emissive_lights;     /* VE_FRAME_EMISSIVE: registered lights after the call */
     uint64_t nee_emissive;        /* VE_FRAME_EMISSIVE: NEE shadow rays toward lights */
     uint64_t restir_commits;      /* VE_FRAME_EMISSIVE: voxel reservoirs stored */
+    uint64_t shadow_shared;       /* sun shadow rays counted in rays_shadow but not traced: a pixel's
+                                     samples share their first shading step's shadow ray (the same
+                                     origin and direction), traced once, by sample 0 */
 } ve_frame_stats;
 
 typedef struct ve_ctx ve_ctx;
@@ -431,7 +434,7 @@ int ve_reset_total_stats(ve_ctx* ctx);
 typedef struct ve_server ve_server;
 typedef struct ve_server_config {
     uint64_t pixel_capacity;   /* pooled pixels: GBuffer + outputs, 48 B each */
-    uint64_t path_capacity;    /* pooled path states, 144 B each */
+    uint64_t path_capacity;    /* pooled path states, 144 B each (below 2^30) */
     uint32_t max_requests;     /* view slots (requests on the GPU at once) */
     uint32_t flags;            /* VE_SERVER_FIFO */
     uint64_t step_path_budget; /* paths whose primary pass one step may start (0: 2^23) */

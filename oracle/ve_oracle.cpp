@@ -956,7 +956,7 @@ void emissive_nee(const Scene& s, const ov_frame_params& P, EmFrame& em, uint32_
 // dormant in scenes without emissive voxels).
 void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_frame_params& P,
                 const Hit& primary, f3 primary_dir, uint32_t pix_index, uint32_t list_idx, PathOut* out,
-                ov_stats* st, RayCounters* rc, EmFrame* em = nullptr) {
+                ov_stats* st, RayCounters* rc, EmFrame* em = nullptr, bool shared_sun0 = false) {
     const uint32_t max_bounces = P.bounces + 1u;  // MAX_BOUNCES (wavefront.glsl:23)
     // emit.comp:171-174; list_idx is pixel * spp + sample in the per-pixel
     // method and the shade-list index in the scheduled one
@@ -996,7 +996,10 @@ void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_
         } else if (!m.emissive && b < 2u && dot(N, sun) > 0.0f) {
             // NEE gate of shade.comp:631 (non-emissive surface, bounce < 2),
             // with the sun's cosine test of shade.comp:811-815
-            const Hit sh = raycast(s, shading_point, sun, P.bounce_controlchecks, rc);
+            // shared_sun0: a pixel's later sample, whose first shadow ray is
+            // sample 0's (the same origin and direction): its walk is not
+            // counted again (the device traces it once)
+            const Hit sh = raycast(s, shading_point, sun, P.bounce_controlchecks, (b == 0 && shared_sun0) ? nullptr : rc);
             st->rays_shadow++;
             if (sh.status == ST_ESCAPED) {
                 const f3 brdf = evaluate_brdf(dir, sun, N, albedo, m.roughness, m.metallic, m.specular);
@@ -1806,7 +1809,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
                 for (uint32_t smp = 0; smp < P->spp; smp++) {
                     PathOut po;
                     trace_path(s, mats, n_mats, *P, h, dir, pix, pix * P->spp + smp, &po, &st, &trc[t],
-                               ems.empty() ? nullptr : &ems[t]);
+                               ems.empty() ? nullptr : &ems[t], ems.empty() && smp > 0);
                     st.paths++;
                     Deposit dp;
                     dp.vid = vid;

@@ -38,7 +38,7 @@ def test_struct_sizes_match_header(ve):
     assert ctypes.sizeof(ve.FrameConfigC) == 160
     assert ctypes.sizeof(ve.ViewC) == 4 + 64 + 160
     assert ctypes.sizeof(ve.FrameOutputsC) == 7 * 8
-    assert ctypes.sizeof(ve.FrameStatsC) == 13 * 8 + 6 * 4 + 2 * 4 + 8 + 5 * 8 + 2 * 4 + 3 * 8
+    assert ctypes.sizeof(ve.FrameStatsC) == 13 * 8 + 6 * 4 + 2 * 4 + 8 + 5 * 8 + 2 * 4 + 4 * 8
     assert ctypes.sizeof(ve.ServerConfigC) == 2 * 8 + 2 * 4 + 8 + 2 * 4
     assert ctypes.sizeof(ve.RequestInfoC) == 8 + 3 * 8 + 2 * 8
     assert ctypes.sizeof(ve.ServerStatsC) == 9 * 8

@@ -123,7 +123,7 @@ class FrameStatsC(ctypes.Structure):
                 ("scheduled_voxels", ctypes.c_uint64), ("scheduled_paths", ctypes.c_uint64),
                 ("ms_learned", ctypes.c_float), ("reserved", ctypes.c_uint32),
                 ("emissive_lights", ctypes.c_uint64), ("nee_emissive", ctypes.c_uint64),
-                ("restir_commits", ctypes.c_uint64)]
+                ("restir_commits", ctypes.c_uint64), ("shadow_shared", ctypes.c_uint64)]
 
 
 class ServerConfigC(ctypes.Structure):

@@ -131,7 +131,8 @@ enum : uint32_t {
     ST_EM_LIGHTS,    // emissive frames: registered lights after the frame
     ST_EM_NEE,       // emissive frames: NEE shadow rays toward lights
     ST_RES_WRITES,   // emissive frames: reservoirs committed
-    ST_TOTAL = 19
+    ST_SHADOW_SHARED,  // sun shadow rays answered by the same pixel's sample-0 traversal
+    ST_TOTAL = 20
 };
 // path flags (meta.z bits 24-31); F_DZERO / F_IZERO: the path's direct /
 // indirect radiance is +0 in every channel and its p_direct / p_indirect slot
@@ -323,11 +324,12 @@ __device__ __forceinline__ void warp_deposit(bool active, uint32_t scene, uint32
 // Per-thread tallies of a shading kernel, added to the frame's counters once
 // at its end.
 struct EmitCounts {
-    uint32_t ext = 0, sh = 0, dep = 0, drop = 0;
+    uint32_t ext = 0, sh = 0, dep = 0, drop = 0, shared = 0;
 };
 __device__ __forceinline__ void flush_counts(const EmitCounts& c, unsigned long long* stats) {
     warp_add_stat(&stats[ST_RAYS_BOUNCE], c.ext);
     warp_add_stat(&stats[ST_RAYS_SHADOW], c.sh);
+    warp_add_stat(&stats[ST_SHADOW_SHARED], c.shared);
     warp_add_stat(&stats[ST_DEPOSITS], c.dep);
     warp_add_stat(&stats[ST_DROPPED], c.drop);
 }
@@ -449,7 +451,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
                 const uint32_t idx = first_idx + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (idx < n) {
                     e = idx < n_ext ? a.rayq[idx] : a.rayq_sh[idx - n_ext];
-                    const uint32_t p = e & 0x7FFFFFFFu;
+                    const uint32_t p = e & 0x3FFFFFFFu;
                     const uint4 meta = a.p_meta[p];
                     const DevView& v = a.views[meta.z & 0xFFFFu];
                     const DevScene S = a.scenes[v.scene];
@@ -486,13 +488,23 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
             if (finished) active = false;
         }
         if (finished) {
-            const uint32_t p = e & 0x7FFFFFFFu;
+            const uint32_t p = e & 0x3FFFFFFFu;
             if (e >> 31) {
                 // the shadow ray's result code: ~0 left the volume, a hit
                 // voxel's vid (emissive batches: the light must be the hit),
-                // else 0 (the record's initial value)
-                if (h.status == kEscaped) reinterpret_cast<uint32_t*>(a.p_pend + p)[3] = 0xFFFFFFFFu;
-                else if (EM && h.status == kHit) reinterpret_cast<uint32_t*>(a.p_pend + p)[3] = voxel_key(h.x, h.y, h.z) + 1u;
+                // else 0 (the record's initial value).  A shared sun shadow
+                // ray (bit 30: a pixel's samples start at the same hit) finds
+                // in its record the count of the records that follow it and
+                // take the same code.
+                uint32_t* rec = reinterpret_cast<uint32_t*>(a.p_pend + p) + 3;
+                if (!EM && (e & 0x40000000u)) {
+                    const uint32_t n = *rec, code = h.status == kEscaped ? 0xFFFFFFFFu : 0u;
+                    for (uint32_t k = 0; k <= n; k++) rec[4u * k] = code;
+                } else if (h.status == kEscaped) {
+                    *rec = 0xFFFFFFFFu;
+                } else if (EM && h.status == kHit) {
+                    *rec = voxel_key(h.x, h.y, h.z) + 1u;
+                }
             } else {
                 // h.id holds the hit leaf's word: the shade pass needs no
                 // dependent load from the node array
@@ -599,6 +611,8 @@ struct ShadeOut {
     // the warp's append), a recorded training sample, a hash-cache ending
     bool want_q = false, sampled = false, hash_term = false;
     bool app_res = false, em_nee = false;  // a reservoir to commit; an emissive NEE shadow ray
+    bool sh_shared = false;  // a sun shadow ray traced by the pixel's sample-0 path instead
+    bool sh_owner = false;   // ... the sample-0 path's ray, whose result the others take
     float dr = 0.0f, dg = 0.0f, db = 0.0f, dl2 = 0.0f;
     float ir = 0.0f, ig = 0.0f, ib = 0.0f;  // lBuffer frames: dr..db direct, ir..ib indirect
     uint32_t dvid = 0, dscene = 0, dview = 0;
@@ -771,7 +785,7 @@ __device__ __forceinline__ void emissive_nee(const FrameArgs& a, const DevView& 
 template <int MODE>
 __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4 meta, f3 tp, f3 direct,
                                            f3 indirect, f3 dir, uint4 hit, ShadeOut& o,
-                                           bool direct_stored = false) {
+                                           bool direct_stored = false, uint32_t share = 0u) {
     constexpr bool EM = (MODE & kModeEm) != 0;
     constexpr bool LB = (MODE & kModeLb) != 0;
     constexpr bool NRC = (MODE & kModeNrc) != 0;
@@ -904,10 +918,18 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
                 const f3 brdf = evaluate_brdf(dir, sun, N, albedo, roughness, metallic, spec);
                 f3 c = muls(brdf, v.sun_intensity);
                 c = mk(gmin(c.x, 20.0f), gmin(c.y, 20.0f), gmin(c.z, 20.0f));
-                a.p_pend[p] = st3(mul(tp, c), 0.0f);
+                // the record's last word is the shadow ray's result; until the
+                // trace writes it, it holds the count of later records (the
+                // pixel's other samples) that take the same result (share)
+                a.p_pend[p] = st3(mul(tp, c), __uint_as_float(share == 0xFFFFFFFFu ? 0u : share));
                 if (EM) a.p_sdir[p] = make_float4(sun.x, sun.y, sun.z, __uint_as_float(0xFFFFFFFFu));
                 nf |= F_PENDING;
-                o.app_sh = true;
+                if (share == 0xFFFFFFFFu) {
+                    o.sh_shared = true;
+                } else {
+                    o.app_sh = true;
+                    o.sh_owner = share != 0u;
+                }
             }
             bool term = false;
             if (ended) {
@@ -1009,9 +1031,10 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
                                   ray_cnt + (CNT_RAYSH - CNT_RAY), q);
     if (o.app_live) live_out[s.x] = p;
     if (o.app_ext) a.rayq[s.y] = p;
-    if (o.app_sh) a.rayq_sh[s.z] = p | 0x80000000u;
+    if (o.app_sh) a.rayq_sh[s.z] = p | (o.sh_owner ? 0xC0000000u : 0x80000000u);
     cnt.ext += o.app_ext ? 1u : 0u;
-    cnt.sh += o.app_sh ? 1u : 0u;
+    cnt.sh += (o.app_sh || o.sh_shared) ? 1u : 0u;
+    cnt.shared += o.sh_shared ? 1u : 0u;
     if (NRC && (a.nq || a.ns)) {
         // learned cache: query records move from the path's ray slots into
         // the query queue (capacity = paths, never full)
@@ -1129,8 +1152,14 @@ __global__ void __launch_bounds__(256, 4) k_primary(FrameArgs a) {
                 // emit.comp:171-174
                 const uint32_t sample_idx = v.frame_index + spix * 2654435761u + list_idx * 1442695040u;
                 const uint32_t rng = (sample_idx << 8) & 0xFFFFFF00u;
+                // the samples of a pixel start at the same hit with the same
+                // direction: one sun shadow ray (sample 0's) serves them all
+                // (share: sample 0 carries the count of the others, each of
+                // which casts none).  Emissive batches keep their own.
+                const uint32_t share = (!(MODE & kModeEm) && spp > 1u) ? (s == 0u ? spp - 1u : 0xFFFFFFFFu) : 0u;
                 shade_step<MODE>(a, p, make_uint4(svid, rng, vi + a.view_offset, spix), mk(1.0f, 1.0f, 1.0f),
-                           mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o);
+                           mk(0.0f, 0.0f, 0.0f), mk(0.0f, 0.0f, 0.0f), sdir, make_uint4(kHit, sword, sxy, szm), o,
+                           false, share);
             }
             shade_emit<MODE>(a, p, o, a.live[1], &a.counters[CNT_LIVE + 1], &a.counters[CNT_RAY + 0],
                            dep + (threadIdx.x & ~31u), bq[it & 1u], cnt);
@@ -2819,7 +2848,8 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
                 return fail(VE_ERR_INVALID,
                             "render: VE_FRAME_ASYNC_OUTPUTS copies voxel_id, hit_node, rgb, mapped and mapped8 only");
     }
-    if (paths >= (1ull << 31)) return fail(VE_ERR_CAPACITY, "render: more than 2^31 paths in one batch");
+    // path slots are 30 bits (queue entries carry two flag bits)
+    if (paths >= (1ull << 30)) return fail(VE_ERR_CAPACITY, "render: more than 2^30 paths in one batch");
     // learned radiance cache: one per batch, attached to the views' scenes
     ve_nrc* nrc = nullptr;
     for (uint32_t i = 0; i < nv; i++) {
@@ -4422,6 +4452,7 @@ static void fill_counters(ve_frame_stats& r, const unsigned long long* h) {
     r.emissive_lights = h[ST_EM_LIGHTS];
     r.nee_emissive = h[ST_EM_NEE];
     r.restir_commits = h[ST_RES_WRITES];
+    r.shadow_shared = h[ST_SHADOW_SHARED];
 }
 
 int ve_get_total_stats(ve_ctx* c, ve_frame_stats* s) {

@@ -374,7 +374,7 @@ int ve_server_create(ve_ctx* c, const ve_server_config* cfg, ve_server** out) {
     if (!c || !cfg || !out) return fail(VE_ERR_INVALID, "server_create: null argument");
     if (cfg->max_requests == 0 || cfg->max_requests > 4096)
         return fail(VE_ERR_INVALID, "server_create: max_requests must be in [1, 4096]");
-    if (cfg->pixel_capacity == 0 || cfg->path_capacity == 0 || cfg->path_capacity >= (1ull << 31) ||
+    if (cfg->pixel_capacity == 0 || cfg->path_capacity == 0 || cfg->path_capacity >= (1ull << 30) ||
         cfg->pixel_capacity >= (1ull << 32))
         return fail(VE_ERR_INVALID, "server_create: bad pool capacities");
     cudaSetDevice(c->device);
