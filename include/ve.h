@@ -434,7 +434,7 @@ int ve_reset_total_stats(ve_ctx* ctx);
 typedef struct ve_server ve_server;
 typedef struct ve_server_config {
     uint64_t pixel_capacity;   /* pooled pixels: GBuffer + outputs, 48 B each */
-    uint64_t path_capacity;    /* pooled path states, 144 B each (below 2^30) */
+    uint64_t path_capacity;    /* pooled path states, 152 B each (below 2^30) */
     uint32_t max_requests;     /* view slots (requests on the GPU at once) */
     uint32_t flags;            /* VE_SERVER_FIFO */
     uint64_t step_path_budget; /* paths whose primary pass one step may start (0: 2^23) */

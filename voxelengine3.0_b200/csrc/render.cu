@@ -176,8 +176,12 @@ struct FrameArgs {
     uint4* p_hit;        // {status, leaf word, x | y<<16, z | material<<16}
     uint4* p_meta;       // {vid, rng, view | bounce<<16 | flags<<24, pixel}
     uint32_t* live[2];
-    uint32_t* rayq;     // per pass: extension rays (path slot)
-    uint32_t* rayq_sh;  // ... and shadow rays (path slot | 1 << 31), a separate region
+    // per pass: extension rays {path slot, view}, and shadow rays {path slot |
+    // 1 << 31 (| 1 << 30: shared by the pixel's samples), view} in a separate
+    // region; the view rides along so a trace refill needs no path-state load
+    // before the ray's own
+    uint2* rayq;
+    uint2* rayq_sh;
     uint32_t* counters;
     unsigned long long* stats;
     uint4* gbuf;
@@ -450,10 +454,10 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
             if (!active) {
                 const uint32_t idx = first_idx + uint32_t(__popc(idle & ((1u << lane) - 1u)));
                 if (idx < n) {
-                    e = idx < n_ext ? a.rayq[idx] : a.rayq_sh[idx - n_ext];
+                    const uint2 en = idx < n_ext ? a.rayq[idx] : a.rayq_sh[idx - n_ext];
+                    e = en.x;
                     const uint32_t p = e & 0x3FFFFFFFu;
-                    const uint4 meta = a.p_meta[p];
-                    const DevView& v = a.views[meta.z & 0xFFFFu];
+                    const DevView& v = a.views[en.y];
                     const DevScene S = a.scenes[v.scene];
                     nodes = S.nodes;
                     n_words = word_bound(S.n_words);
@@ -797,6 +801,7 @@ __device__ __forceinline__ void shade_step(const FrameArgs& a, uint32_t p, uint4
     // vi indexes the whole view table; `a.views` starts view_offset entries
     // into it when the caller passed one view (the serving primary pass)
     const DevView& v = a.views[vi - a.view_offset];
+    o.dview = vi;  // the queue entries of the path's rays carry it
     if (flags & F_TERM) {
         o.do_dep = true;
     } else {
@@ -1030,8 +1035,8 @@ __device__ __forceinline__ void shade_emit(const FrameArgs& a, uint32_t p, const
     const uint3 s = block_append3(o.app_live, o.app_ext, o.app_sh, live_cnt, ray_cnt,
                                   ray_cnt + (CNT_RAYSH - CNT_RAY), q);
     if (o.app_live) live_out[s.x] = p;
-    if (o.app_ext) a.rayq[s.y] = p;
-    if (o.app_sh) a.rayq_sh[s.z] = p | (o.sh_owner ? 0xC0000000u : 0x80000000u);
+    if (o.app_ext) a.rayq[s.y] = make_uint2(p, o.dview);
+    if (o.app_sh) a.rayq_sh[s.z] = make_uint2(p | (o.sh_owner ? 0xC0000000u : 0x80000000u), o.dview);
     cnt.ext += o.app_ext ? 1u : 0u;
     cnt.sh += (o.app_sh || o.sh_shared) ? 1u : 0u;
     cnt.shared += o.sh_shared ? 1u : 0u;
@@ -2040,7 +2045,8 @@ struct FrameSet {
     ve::DevBuf<ve::DevView> d_views;
     ve::DevBuf<float4> p_ray_o, p_ray_d, p_tp, p_direct, p_indirect, p_pend;
     ve::DevBuf<uint4> p_hit, p_meta, gbuf;
-    ve::DevBuf<uint32_t> live0, live1, rayq, counters;
+    ve::DevBuf<uint32_t> live0, live1, counters;
+    ve::DevBuf<uint2> rayq;
     ve::DevBuf<unsigned long long> stats;
     unsigned long long* h_stats = nullptr;  // pinned
 };
@@ -2072,7 +2078,8 @@ struct ve_ctx {
     ve::DevBuf<uint32_t> claim, sched_n;
     ve::DevBuf<uint2> shade_list;
     ve::DevBuf<uint8_t> scan_tmp;
-    ve::DevBuf<uint32_t> live0, live1, rayq;
+    ve::DevBuf<uint32_t> live0, live1;
+    ve::DevBuf<uint2> rayq;
     ve::DevBuf<uint32_t> counters;
     ve::DevBuf<unsigned long long> stats;
     ve::DevBuf<unsigned long long> totals;

@@ -482,7 +482,7 @@ int ve_server_get_stats(ve_server* s, ve_server_stats* out) {
     out->in_flight = s->active.size();
     out->max_in_flight = s->max_inflight;
     out->steps = s->steps_run;
-    out->pool_bytes = s->pix_pool.capacity() * 48ull + s->path_pool.capacity() * 144ull;
+    out->pool_bytes = s->pix_pool.capacity() * 48ull + s->path_pool.capacity() * 152ull;
     uint64_t scene_bytes = 0;
     for (const auto& sc : s->c->scenes)
         if (sc.live)
