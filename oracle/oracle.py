@@ -45,7 +45,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("rays_primary", _U64), ("rays_bounce", _U64), ("rays_shadow", _U64), ("fetch_restart", _U64),
                 ("fetch_min", _U64), ("paths", _U64), ("deposits", _U64), ("steps", _U64),
                 ("scheduled_voxels", _U64), ("scheduled_paths", _U64),
-                ("emissive_lights", _U64), ("nee_emissive", _U64), ("restir_commits", _U64)]
+                ("emissive_lights", _U64), ("nee_emissive", _U64), ("restir_commits", _U64),
+                ("shadow_shared", _U64)]
 
 
 def build_oracle(force: bool = False) -> str:

@@ -1001,6 +1001,7 @@ void trace_path(const Scene& s, const Material* mats, uint32_t n_mats, const ov_
             // counted again (the device traces it once)
             const Hit sh = raycast(s, shading_point, sun, P.bounce_controlchecks, (b == 0 && shared_sun0) ? nullptr : rc);
             st->rays_shadow++;
+            if (b == 0 && shared_sun0) st->shadow_shared++;
             if (sh.status == ST_ESCAPED) {
                 const f3 brdf = evaluate_brdf(dir, sun, N, albedo, m.roughness, m.metallic, m.specular);
                 f3 c = muls(brdf, P.sun_intensity);
@@ -1838,6 +1839,7 @@ int oracle_render_frame(void* rp, const uint32_t* words, uint64_t n_words, uint3
         total.rays_primary += tstats[t].rays_primary;
         total.rays_bounce += tstats[t].rays_bounce;
         total.rays_shadow += tstats[t].rays_shadow;
+        total.shadow_shared += tstats[t].shadow_shared;
         total.paths += tstats[t].paths;
         total.fetch_restart += trc[t].fetch_restart;
         total.fetch_min += trc[t].fetch_min;

@@ -50,6 +50,7 @@ struct ov_stats {
     uint64_t steps;           // DDA outer iterations (all rays)
     uint64_t scheduled_voxels, scheduled_paths;  // scheduled frames
     uint64_t emissive_lights, nee_emissive, restir_commits;  // emissive frames
+    uint64_t shadow_shared;   // first shadow rays of a pixel's later samples (sample 0's walk)
 };
 
 }  // extern "C"

@@ -84,9 +84,34 @@ def test_single_frame_gbuffer_and_paths_exact(ve, renderer, oracle, small):
     assert st["rays_primary"] == s["rays_primary"]
     assert st["rays_bounce"] == s["rays_bounce"]
     assert st["rays_shadow"] == s["rays_shadow"]
+    assert st["shadow_shared"] == s["shadow_shared"]
     assert st["paths"] == s["paths"] == st["deposits"]
     assert st["deposits_dropped"] == 0
     # distinct-node fetches: the device descent reads each node of the walk once
+    assert st["fetch_nodes"] == s["fetch_min"]
+    assert st["dda_steps"] == s["steps"]
+
+
+def test_shared_first_shadow_rays(ve, renderer, oracle, small):
+    """A pixel's samples share their first sun shadow ray (same origin and
+    direction): traced once, its result taken by every sample.  Per-path
+    deposits stay bitwise equal, the walk is counted once on both sides."""
+    sid, words, depth, mats, cam, fc = small
+    renderer.cache_reset(sid)
+    dev_words = renderer.download_scene(sid)
+    fc = ve.FrameConfig(**{**fc.__dict__, "spp": 4, "bounces": 2,
+                           "flags": ve.FRAME_PATH_RGB | ve.FRAME_COUNT_FETCH})
+    _, outs = run_both(ve, oracle, renderer, sid, dev_words, depth, mats, cam, fc, 1,
+                       want=("gbuffer", "path_rgb"))
+    g, st, o = outs[0]
+    assert np.array_equal(g["gbuffer"], o["gbuffer"])
+    hit = np.repeat(o["gbuffer"][..., 3].reshape(-1) != 0, 4)
+    assert np.array_equal(g["path_rgb"][hit].view(np.uint32), o["path_rgb"][hit].view(np.uint32))
+    s = o["stats"]
+    for k in ("rays_primary", "rays_bounce", "rays_shadow", "shadow_shared"):
+        assert st[k] == s[k], k
+    # three of every four first shadow rays of a lit pixel are shared
+    assert s["shadow_shared"] > 0 and s["shadow_shared"] % 3 == 0
     assert st["fetch_nodes"] == s["fetch_min"]
     assert st["dda_steps"] == s["steps"]
 
