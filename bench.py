@@ -21,7 +21,8 @@ radius 600.  A ray is one DDA traversal (primary, bounce or sun shadow).
 * ``roofline``: the trace kernel (bounce + shadow DDA): algorithmic bytes
   (4 B per distinct node word read + 48 B ray state per traversal) over its
   CUDA-event time inside the timed frames, against the measured HBM copy
-  bandwidth.
+  bandwidth; ``roofline.l2`` sets the L2 bytes of the same kernel (ncu) over
+  that time against the L2 byte peak, the yardstick for its L2-resident tree.
 * ``cpu_baseline``: the scalar C++ oracle on the host cores (all threads),
   on a bounded band of rows of frame 0.
 
@@ -73,6 +74,24 @@ def measured_trace_traffic():
         return float(d["dram_bytes_per_launch_1080p"]), d.get("source")
     except (OSError, KeyError, ValueError):
         return None, None
+
+
+def trace_l2_roofline(ms_per_launch):
+    """The trace kernel against L2 instead of HBM (its node words and top
+    table are mostly L2-resident): L2 bytes per launch from the same ncu
+    capture as the DRAM traffic, over the live launch time, against the
+    nominal L2 byte peak recorded with it.  None when the record is absent."""
+    p = os.path.join(ROOT, "profiles", "k_trace_traffic.json")
+    try:
+        d = json.load(open(p))
+        b, peak = float(d["lts_bytes_per_launch_1080p"]), float(d["l2_peak_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+    if not ms_per_launch:
+        return None
+    achieved = b / (ms_per_launch / 1e3) / 1e9
+    return {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "bytes_per_launch": b, "peak_kind": d.get("l2_peak_source")}
 
 
 def peaks():
@@ -1129,7 +1148,8 @@ def main():
                          "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "peak_kind": peak_kind, "traffic": traffic, "traffic_source": traffic_src,
                          "algorithmic_bytes_per_launch": trace_bytes / max(launches, 1),
-                         "ms_per_launch": trace_ms / max(launches, 1)},
+                         "ms_per_launch": trace_ms / max(launches, 1),
+                         "l2": trace_l2_roofline(trace_ms / max(launches, 1))},
             "gpu_launches": int(tot["kernel_launches"]),
             "frame_pipeline": not args.no_pipeline,
             "stage_ms_per_step": {k: ttot[k] / K for k in ("ms_primary", "ms_trace", "ms_shade", "ms_resolve",
