@@ -212,7 +212,7 @@ Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc,
 }
 
 // The box bounce rays are clipped to (a bound of this build, not of the
-// reference).  Levels 0..T0-1 (T0 = min(9, D - 1), none below depth 3) are
+// reference).  Levels 0..T0-1 (T0 = min(10, D), none below depth 3) are
 // the device's top-table levels; a level-(T0-1) cell whose words at those
 // levels are all internal can end a descent on a material voxel, no other
 // in-range cell can (words above level D are never tested for a material).
@@ -222,7 +222,7 @@ Hit raycast(const Scene& s, f3 o, f3 d, uint32_t controlchecks, RayCounters* rc,
 // above 12 where the faces are not searched, no box applies.
 void scene_clip_box(Scene& s) {
     const uint32_t D = s.depth;
-    const uint32_t T0 = D < 3u ? 0u : std::min(9u, D - 1u);
+    const uint32_t T0 = D < 3u ? 0u : std::min(10u, D);
     if (T0 == 0 || D > 12) return;
     const uint32_t L = 1u << D, sh = D - T0 + 1u;
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};

@@ -257,9 +257,10 @@ def test_clip_box(ve, renderer, oracle):
     sid = renderer.upload_scene(scene_from_voxels(ve, 6, cube), 6)
     try:
         lo, hi, bounded = renderer.clip_box(sid)
-        # depth 6: the table resolves 5 levels, cells of 4 voxels
+        # depth 6: the table resolves all 6 levels above the leaves, cells of
+        # 2 voxels (the cube spans x 28-35, y 27-35, z 29-34)
         assert bounded
-        assert lo.tolist() == [27.0, 23.0, 27.0] and hi.tolist() == [37.0, 37.0, 37.0]
+        assert lo.tolist() == [27.0, 25.0, 27.0] and hi.tolist() == [37.0, 37.0, 37.0]
     finally:
         renderer.release_scene(sid)
     depth = 4
@@ -320,8 +321,9 @@ def test_clip_box_follows_edits(ve, renderer, oracle):
                 assert o.capacity == cap  # the blocks freed above are reused: the edit path is taken
                 renderer.apply_edits(sid, slots, o.words()[slots])
             lo, hi, bounded = renderer.clip_box(sid)
-            # depth 6: cells of 4 voxels, widened by one voxel
-            assert bounded and lo[1] == (27.0 if step == 0 else -1.0) and hi[1] == 37.0
+            # depth 6: cells of 2 voxels, widened by one voxel (the floor at
+            # y = 2 lies in the cell of rows 2-3)
+            assert bounded and lo[1] == (27.0 if step == 0 else 1.0) and hi[1] == 37.0
             renderer.cache_reset(sid)
             dev_words = renderer.download_scene(sid)
             assert np.array_equal(dev_words, oracle.fill_normals(o.words(), depth))
