@@ -8,7 +8,11 @@
 # library).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${VE_REFERENCE_ROOT:-/root/reference}"
+# the reference tree: $VE_REFERENCE_ROOT, else BASELINE.json's reference_path
+REF="${VE_REFERENCE_ROOT:-}"
+if [ -z "$REF" ] && [ -f "$HERE/../BASELINE.json" ]; then
+    REF="$(python3 -c 'import json,sys; print(json.load(open(sys.argv[1])).get("reference_path", ""))' "$HERE/../BASELINE.json" 2>/dev/null || true)"
+fi
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/octree_cpu.cpp" ]; then
     echo "build_ref: reference sources not found at $REF; skipping" >&2
