@@ -312,7 +312,9 @@ int ve_scene_download(ve_ctx* ctx, int32_t scene_id, uint32_t* out, uint64_t cap
 #define VE_RAYCAST_FULL_WALK 1u
 int ve_raycast_batch(ve_ctx* ctx, int32_t scene_id, const float* origins, const float* dirs, uint64_t n,
                      uint32_t controlchecks, uint32_t flags, uint32_t* out);
-/* device bytes held by a scene (node array + radiance cache) */
+/* device bytes held by a scene: node array, radiance cache and top table
+ * (4 B per cell of the grid one level above the leaves, for depths up to 10:
+ * 512 MiB at depth 10 and deeper) */
 int ve_scene_footprint(ve_ctx* ctx, int32_t scene_id, uint64_t* bytes);
 /* The box bounce rays are clipped to (no reference counterpart: a bound the
  * trace derives from the top table).  A bounce ray whose escape and timeout
