@@ -420,7 +420,10 @@ __global__ void __launch_bounds__(256) k_decay(CacheEntry* cache, uint32_t n, fl
 // per step: once a refill hands out the queue's last entry the warp stops
 // refilling (a warp-uniform flag) and runs its remaining rays out.
 // EM: the batch has VE_FRAME_EMISSIVE views (shadow rays toward lights).
-template <bool COUNT, bool EM = false>
+// FLAT: every scene of the batch has a top table reaching its leaves
+// (T0 = D): the descent keeps one leaf-block offset instead of the per-level
+// array (dda_step).
+template <bool COUNT, bool EM = false, bool FLAT = false>
 __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
     // the pass's extension rays, then its shadow rays: warps stay mostly of
     // one kind, and the shorter shadow rays form the tail of the pass
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(256, 6) k_trace(FrameArgs a, uint32_t pass) {
             }
         }
         if (active) {
-            finished = dda_step<COUNT, true, true>(s, nodes, n_words, D, top, T0, h, rc);
+            finished = dda_step<COUNT, true, true, FLAT && !COUNT>(s, nodes, n_words, D, top, T0, h, rc);
             if (finished) active = false;
         }
         if (finished) {
@@ -2960,6 +2963,13 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
     }
     // emissive lights: the scenes' registries and reservoir tables, the
     // per-path NEE records and the registry commit's sort buffers
+    // the trace's FLAT instance: every view's scene has a top table reaching
+    // its leaves (depth 3..10)
+    bool flat = true;
+    for (uint32_t i = 0; i < nv; i++) {
+        const SceneSlot& sc = c->scenes[views[i].scene_id];
+        flat = flat && sc.top_level != 0u && sc.top_level == sc.depth;
+    }
     std::vector<int> em_scenes;
     size_t em_sort_bytes = 0;
     if (flags & VE_FRAME_EMISSIVE) {
@@ -3195,6 +3205,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
                     else k_trace<false, true><<<c->grid_trace, 256, 0, st>>>(a, pass);
                 } else {
                     if (count) k_trace<true><<<c->grid_trace_count, 256, 0, st>>>(a, pass);
+                    else if (flat) k_trace<false, false, true><<<c->grid_trace, 256, 0, st>>>(a, pass);
                     else k_trace<false><<<c->grid_trace, 256, 0, st>>>(a, pass);
                 }
                 launches++;
@@ -3286,6 +3297,7 @@ static int render_batch(ve_ctx* c, const ve_view* views, uint32_t nv, ve_frame_o
         }
         for (int sc : em_scenes) key.push_back((1ull << 62) | uint64_t(uint32_t(sc)));
         key.push_back((1ull << 61) | uint64_t(parity));
+        key.push_back((1ull << 59) | uint64_t(flat));
         key.push_back((1ull << 60) | (uint64_t(set) << 8) | uint64_t(part));
         ve_ctx::GraphEntry* ge = nullptr;
         for (auto& g : c->graphs)
