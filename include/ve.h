@@ -389,7 +389,7 @@ int ve_split_resolve(ve_ctx* ctx, const ve_view* view, ve_frame_outputs* out);
 
 /* Launch shape of the persistent bounce kernels: resident blocks per SM of
  * the trace and shade kernels (0 = occupancy maximum) and the number of idle
- * lanes at which a trace warp refills itself with new rays (0 = default, 12). */
+ * lanes at which a trace warp refills itself with new rays (0 = default, 20). */
 typedef struct ve_launch_config {
     uint32_t trace_blocks_per_sm;
     uint32_t shade_blocks_per_sm;

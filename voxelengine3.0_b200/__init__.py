@@ -778,7 +778,8 @@ class Renderer:
         return {k: getattr(c, k) for k, _ in LaunchConfigC._fields_}
 
     def set_launch_config(self, trace_blocks_per_sm: int = 0, shade_blocks_per_sm: int = 0,
-                          refill_threshold: int = 12) -> None:
+                          refill_threshold: int = 0) -> None:
+        """0 for any field keeps the library's default (occupancy maximum; refill at 20 idle lanes)."""
         c = LaunchConfigC(trace_blocks_per_sm, shade_blocks_per_sm, refill_threshold, 0)
         _check(self._lib.ve_set_launch_config(self._h, ctypes.byref(c)))
 

@@ -106,7 +106,7 @@ struct DevView {
 };
 
 enum : uint32_t { kMaxPasses = 18, kMaxControlChecks = 65536 };
-constexpr uint32_t kDefaultRefill = 12;  // trace refill threshold (idle lanes of 32)
+constexpr uint32_t kDefaultRefill = 20;  // trace refill threshold (idle lanes of 32)
 enum : uint32_t {
     CNT_LIVE = 0, CNT_RAY = 20, CNT_CURSOR = 40, CNT_NRC_Q = 60, CNT_NRC_S = 61, CNT_SCHED = 62, CNT_RES = 63,
     CNT_RAYSH = 64,  // shadow rays per pass (extension rays: CNT_RAY)
@@ -2725,10 +2725,10 @@ static void apply_launch(ve_ctx* c) {
     c->grid_trace = c->num_sms * pick(c->launch.trace_blocks_per_sm, c->occ_trace);
     c->grid_trace_count = c->num_sms * pick(c->launch.trace_blocks_per_sm, c->occ_trace_count);
     c->grid_shade = c->num_sms * pick(c->launch.shade_blocks_per_sm, c->occ_shade);
-    // default: refill when 12 of 32 lanes are idle (measured on the depth-10
-    // 1080p workload: 1.335 ms of trace per frame at 12 against 1.36 ms at
-    // 24, 1.37-1.40 ms at 8, 16 and 20, 1.46 ms at 28; each refill is a
-    // dependent chain of loads)
+    // default: refill when 20 of 32 lanes are idle (measured on the depth-10
+    // 1080p workload with the FLAT walk: 0.979 ms of trace per frame at 20
+    // against 0.984 at 16 and 0.994 at 12; each refill is a dependent chain
+    // of loads, and the cheaper the step, the fewer refills pay)
     if (c->launch.refill_threshold == 0 || c->launch.refill_threshold > 32) c->launch.refill_threshold = kDefaultRefill;
 }
 
